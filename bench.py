@@ -1,0 +1,456 @@
+#!/usr/bin/env python
+"""Throughput of the Fourier-slice hot path on B200: extract + insert + backward.
+
+Workload (one "step", the 256^3 differentiation configuration):
+  * volume: 256^3 real Gaussian-blob volume (20 blobs, sigma U(2,6)*4 px,
+    centres uniform in a ball of radius 96, + N(0, 0.01^2)), seeded, as its
+    fftshifted rfft, complex64 (256, 256, 129);
+  * 4096 rotation matrices drawn uniformly on SO(3)
+    (scipy special_ortho_group, random_state=1003);
+  * targets: central slices of a second blob volume plus complex white noise;
+  * step = extract_central_slices_rfft_3d (forward) -> MSE loss against the
+    targets -> backward (d/dvolume via the insert-adjoint scatter and
+    d/drotation, one fused kernel) -> insert_central_slices_rfft_3d of the
+    targets into a fresh (volume, weights) pair.
+  slices/s = 4096 / step time.  Synthetic data stand in for the reference's
+  simulated maps (no network, no dataset).
+
+--impl reference times the reference algorithm on the host CPU cores (the
+oracle's C restatement of it, all threads) on a bounded sample of the same
+workload, with the same metric and unit.
+
+Prints ONE JSON line (rank 0).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "slices/s extract+insert+bwd @256³ fp32 vs plain torch-GPU; % HBM roofline"
+UNIT = "slices/s"
+N_BOX = 256
+N_SLICES = 4096
+ROT_SEED = 1003
+WORKLOAD = ("extract_central_slices_rfft_3d fwd + MSE vs noisy targets + bwd (d/dvolume, "
+            "d/drotation) + insert_central_slices_rfft_3d of the targets; 256^3 complex64 rfft "
+            "volume (256x256x129), 4096 seeded SO(3) rotations")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--box", type=int, default=N_BOX)
+    ap.add_argument("--slices", type=int, default=N_SLICES)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=1024, help="slices per CPU-baseline sample")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------
+# synthetic data
+# ----------------------------------------------------------------------------
+
+def rotations(n: int, seed: int) -> np.ndarray:
+    from scipy.stats import special_ortho_group
+
+    return special_ortho_group.rvs(3, size=n, random_state=seed).reshape(n, 3, 3).astype(np.float32)
+
+
+def blob_volume_torch(n: int, seed: int, device):
+    import torch
+
+    rng = np.random.default_rng(seed)
+    ax = torch.arange(n, device=device, dtype=torch.float32)
+    vol = torch.zeros((n, n, n), device=device, dtype=torch.float32)
+    for _ in range(20):
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        c = n / 2 + u * 0.375 * n * rng.uniform() ** (1.0 / 3.0)
+        s = rng.uniform(2, 6) * n / 64
+        g = [torch.exp(-((ax - float(c[i])) ** 2) / (2 * s * s)) for i in range(3)]
+        vol += g[0][:, None, None] * g[1][None, :, None] * g[2][None, None, :]
+    gen = torch.Generator(device=device).manual_seed(seed)
+    vol += 0.01 * torch.randn(vol.shape, device=device, generator=gen)
+    return vol
+
+
+def rfft_volume_torch(vol):
+    import torch
+
+    f = torch.fft.rfftn(torch.fft.fftshift(vol, dim=(-3, -2, -1)), dim=(-3, -2, -1))
+    return torch.fft.fftshift(f, dim=(-3, -2)).contiguous()
+
+
+# ----------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ----------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# CPU leg (oracle port of the reference algorithm)
+# ----------------------------------------------------------------------------
+
+def cpu_sample_step(O, vol_np, rots_np, targets_np, nthreads):
+    """One bounded CPU sample: extract + grad (dV, dR) + insert of len(rots) slices."""
+    n = vol_np.shape[0]
+    s = O.extract(vol_np, (n, n, n), rots_np, nthreads=nthreads)
+    g = (2.0 / s.size) * (s - targets_np)
+    O.extract_grad(vol_np, (n, n, n), rots_np, g.astype(np.complex64), nthreads=nthreads)
+    O.insert(targets_np, (n, n, n), rots_np, nthreads=nthreads)
+
+
+def cpu_inputs(box, sample, seed=ROT_SEED):
+    rng = np.random.default_rng(seed)
+    real = rng.standard_normal((box, box, box)).astype(np.float32)
+    vol = np.fft.fftshift(np.fft.rfftn(np.fft.fftshift(real)), axes=(0, 1)).astype(np.complex64)
+    rots = rotations(sample, seed)
+    tg = (rng.standard_normal((sample, box, box // 2 + 1)) +
+          1j * rng.standard_normal((sample, box, box // 2 + 1))).astype(np.complex64)
+    return vol, rots, tg
+
+
+def run_cpu_baseline(box, sample, repeats=1):
+    from oracle import oracle as O
+
+    O.lib()
+    threads = os.cpu_count() or 1
+    vol, rots, tg = cpu_inputs(box, sample)
+    cpu_sample_step(O, vol, rots[:4], tg[:4], threads)  # warm
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        cpu_sample_step(O, vol, rots, tg, threads)
+        times.append(time.perf_counter() - t0)
+    t = min(times)
+    return {"value": sample / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sample} slices of the {box}^3 step (extract + dV/dR + insert), oracle C "
+                      f"restatement, OpenMP {threads} threads, best of {repeats}"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    O.lib()
+    threads = os.cpu_count() or 1
+    sample = args.cpu_sample
+    vol, rots, tg = cpu_inputs(args.box, sample)
+    for _ in range(args.warmup):
+        cpu_sample_step(O, vol, rots[:8], tg[:8], threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cpu_sample_step(O, vol, rots, tg, threads)
+    dt = time.perf_counter() - t0
+    value = sample * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "box": args.box, "slices_per_step": sample,
+                   "note": "each step is a bounded sample of the 4096-slice step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sample} slices per step of the {args.box}^3 step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import teamtomo_b200 as tt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n, ns = args.box, args.slices
+    shape = (n, n, n)
+
+    # ---- inputs resident in HBM (targets > L2 per step) ----
+    V0 = rfft_volume_torch(blob_volume_torch(n, ROT_SEED, dev))
+    Vt = rfft_volume_torch(blob_volume_torch(n, ROT_SEED + 1000, dev))
+    R0 = torch.tensor(rotations(ns, ROT_SEED + rank), device=dev)
+    with torch.no_grad():
+        T = tt.extract_central_slices_rfft_3d(Vt, shape, R0)
+        gen = torch.Generator(device=dev).manual_seed(7 + rank)
+        T = T + 0.5 * T.abs().mean() * torch.randn(T.shape, dtype=T.dtype, device=dev, generator=gen)
+    del Vt
+    V = V0.clone().requires_grad_(True)
+    R = R0.clone().requires_grad_(True)
+    stream = torch.cuda.current_stream(dev)
+    marks = {}
+
+    def on_grad(g):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        marks["bwd_start"] = e
+        return g
+
+    class _ResidualMSE(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, s, t):
+            r = s - t
+            ctx.save_for_backward(r)
+            ctx.m = r.numel()
+            return torch.linalg.vector_norm(torch.view_as_real(r)).square() / r.numel()
+
+        @staticmethod
+        def backward(ctx, g):
+            # loss = mean |S - T|^2  ->  PyTorch complex gradient 2 (S - T) / M
+            (r,) = ctx.saved_tensors
+            return r.mul_(g * (2.0 / ctx.m)), None
+
+    def step(with_events=False):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if with_events else None
+        V.grad = None
+        R.grad = None
+        if ev:
+            ev[0].record(stream)
+        S = tt.extract_central_slices_rfft_3d(V, shape, R)
+        if ev:
+            ev[1].record(stream)
+            S.register_hook(on_grad)
+        loss = _ResidualMSE.apply(S, T)
+        loss.backward()
+        if ev:
+            ev[2].record(stream)
+        vol, w = tt.insert_central_slices_rfft_3d(T, shape, R.detach())
+        if ev:
+            ev[3].record(stream)
+        if world > 1:
+            dist.all_reduce(V.grad)
+            dist.all_reduce(vol)
+            dist.all_reduce(w)
+        return loss, ev, (vol, w)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    time.sleep(0.3)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sections = {"extract": [], "backward": [], "insert": []}
+    evs = []
+    start.record(stream)
+    for _ in range(args.steps):
+        loss, ev, _ = step(with_events=True)
+        evs.append((ev, marks["bwd_start"]))
+    end.record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    elapsed = start.elapsed_time(end)  # ms
+    for ev, b in evs:
+        sections["extract"].append(ev[0].elapsed_time(ev[1]))
+        sections["backward"].append(b.elapsed_time(ev[2]))
+        sections["insert"].append(ev[2].elapsed_time(ev[3]))
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    ms_step = elapsed / args.steps
+    value = world * ns * args.steps / (elapsed / 1e3)
+
+    # ---- per-kernel roofline (algorithmic bytes per launch) ----
+    P = n * (n // 2 + 1)
+    vox = n * n * (n // 2 + 1)
+    algo = {
+        "extract": ns * 8 * P + 8 * vox,          # slices written + volume read once
+        "backward": ns * 8 * P + 16 * vox,        # grad read + dV written + volume read once
+        "insert": ns * 8 * P + 12 * vox,          # slices read + volume and weights written
+    }
+    peak, peak_kind = load_peaks()
+    traffic = load_traffic()
+    kernels = {}
+    for k, v in sections.items():
+        ms = statistics.mean(v)
+        gbs = algo[k] / (ms / 1e3) / 1e9
+        kernels[k] = {"ms": round(ms, 4), "algorithmic_bytes": algo[k], "achieved_gbs": round(gbs, 1),
+                      "frac": round(gbs / peak, 4)}
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    roof = {"bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": peak, "unit": "GB/s",
+            "frac": kernels[dom]["frac"], "traffic": traffic.get(dom), "kernel": dom,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6.65 TB/s"}
+
+    # ---- end to end through the public API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        hV = V0.detach().cpu().pin_memory()
+        hR = R0.detach().cpu().pin_memory()
+        hT = T.cpu().pin_memory()
+        h_loss = torch.empty((), dtype=torch.float32).pin_memory()
+        h_dR = torch.empty_like(hR).pin_memory()
+        h2d = hV.numel() * 8 + hR.numel() * 4 + hT.numel() * 8
+        d2h = 4 + h_dR.numel() * 4
+
+        def e2e_step():
+            Vd = hV.to(dev, non_blocking=True).requires_grad_(True)
+            Rd = hR.to(dev, non_blocking=True).requires_grad_(True)
+            Td = hT.to(dev, non_blocking=True)
+            S = tt.extract_central_slices_rfft_3d(Vd, shape, Rd)
+            loss = _ResidualMSE.apply(S, Td)
+            loss.backward()
+            vol, w = tt.insert_central_slices_rfft_3d(Td, shape, Rd.detach())
+            if world > 1:
+                dist.all_reduce(Vd.grad)
+                dist.all_reduce(vol)
+                dist.all_reduce(w)
+            h_loss.copy_(loss.detach(), non_blocking=True)
+            h_dR.copy_(Rd.grad, non_blocking=True)
+
+        e2e_steps = max(3, min(args.steps, 10))
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s2.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        e2.record(stream)
+        torch.cuda.synchronize(dev)
+        el2 = s2.elapsed_time(e2)
+        if world > 1:
+            t = torch.tensor([el2], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el2 = float(t.item())
+        e2e = {"value": world * ns * e2e_steps / (el2 / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = run_cpu_baseline(n, args.cpu_sample)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "box": n, "slices_per_gpu": ns, "global_batch": ns * world,
+                       "rotation_seed": ROT_SEED, "l2": "inputs larger than L2 (1.08 GB of targets per step)",
+                       "parallelism": f"dp{world}" + (" (all_reduce of d/dvolume and inserted volume)"
+                                                      if world > 1 else "")},
+            "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": 5 * args.steps,
+            "loss": float(loss.item()),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,183 @@
+/*
+ * teamtomo_b200 — C ABI of the B200 Fourier-slice kernels.
+ *
+ * Every entry point takes raw device pointers (C-contiguous, CUDA memory of
+ * the current device), sizes in a parameter struct, and a CUDA stream handle
+ * (cudaStream_t passed as void*, NULL = legacy default stream).  Launches are
+ * asynchronous on that stream; no entry point synchronises the host, and none
+ * allocates device memory: scratch space is passed in by the caller
+ * (see the *_workspace_bytes queries).  The return value is a status code
+ * (TT_OK on success); tt_last_error() gives the message of the last failure
+ * on the calling thread.
+ *
+ * Complex arrays are interleaved (re, im): complex64 = 2 x float32,
+ * complex128 = 2 x float64.  "fftshifted rfft" volumes have shape
+ * (d, h, w/2+1) with the zero frequency at (d/2, h/2, 0), the layout the
+ * reference functions consume and produce.
+ *
+ * Reference interfaces replaced (teamtomo monorepo, packages/primitives/…):
+ *   torch-fourier-slice/src/torch_fourier_slice/slice_extraction/_extract_central_slices_rfft_3d.py
+ *   torch-fourier-slice/src/torch_fourier_slice/slice_insertion/_insert_central_slices_rfft_3d.py
+ *   torch-fourier-slice/src/torch_fourier_slice/project.py, backproject.py
+ *   torch-image-interpolation/src/torch_image_interpolation/image_interpolation_3d.py
+ * The reference is pure Python over PyTorch; these entry points are what its
+ * torch ops (grid_sample, index_put_, bmm, boolean indexing) are replaced by.
+ */
+#ifndef TEAMTOMO_B200_H
+#define TEAMTOMO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    TT_OK = 0,
+    TT_ERR_INVALID = 1,   /* bad shape, size, flag or NULL pointer */
+    TT_ERR_CUDA = 2,      /* a CUDA launch or runtime call failed */
+    TT_ERR_WORKSPACE = 3  /* workspace missing or too small */
+};
+
+/* Geometry of one batch of central slices through one rfft volume. */
+typedef struct tt_slice_params {
+    int64_t n;                     /* number of slices (rotation matrices) */
+    int64_t img_d, img_h, img_w;   /* real-space shape defining the slice grid and the
+                                      frequency->array scaling: image_shape for extraction,
+                                      volume_shape for insertion */
+    int64_t vol_d, vol_h, vol_w;   /* dims of the rfft volume array, (d, h, w/2+1) */
+    int32_t has_fftfreq_max;       /* 1: keep only |f| <= fftfreq_max */
+    float fftfreq_max;
+    int32_t zyx_matrices;          /* 0: matrices act on xyz column vectors (default) */
+    float x_tolerance;             /* extraction: conjugate tie-break tolerance (f32) */
+    float x_tolerance10;           /* f32(x_tolerance * 10), computed in double first */
+    int32_t has_rot_tolerance;     /* extraction: zero |R_ij| < rot_tolerance */
+    float rot_tolerance;
+    int32_t rotation_f64;          /* rotation matrices are float64 (else float32) */
+    int32_t volume_unshifted;      /* volume is plain rfftn output (z, y not fftshifted) */
+    int32_t slices_unshifted;      /* slices stored ifftshifted along rows (irfft-ready) */
+    int32_t reserved;
+} tt_slice_params;
+
+/* Library version (major*10000 + minor*100 + patch) and last error text. */
+int tt_version(void);
+const char *tt_last_error(void);
+
+/* Central-slice extraction (trilinear gather with the reference's Hermitian
+ * redirect).  volume_rfft: complex64 (vol_d, vol_h, vol_w); rotation_matrices:
+ * (n, 3, 3) float32 or float64; slices_out: complex64 (n, img_h, img_w/2+1),
+ * fully written (zeros outside fftfreq_max / outside the volume).
+ * Replaces extract_central_slices_rfft_3d,
+ * _extract_central_slices_rfft_3d.py:84-222 (+ :9-81). */
+int tt_extract_central_slices_rfft_3d(const void *volume_rfft, const void *rotation_matrices,
+                                      void *slices_out, const tt_slice_params *p, void *stream);
+
+/* Per-pixel geometry of the slice grid under the extraction (mode 0) or the
+ * insertion (mode 1) rule, for bit-exact checks of the index and mask logic:
+ * flags (n, img_h, img_w/2+1) uint8 — bit0 pixel kept (inside fftfreq_max and,
+ * for insertion, not the Friedel-redundant x==0, y<0 source pixel), bit1
+ * conjugate redirect, bit2 inside the volume; coords (n, img_h, img_w/2+1, 3)
+ * float32 zyx array coordinates after the redirect (0 for dropped pixels).
+ * Exposes the intermediate values of _extract_central_slices_rfft_3d.py:183-209
+ * and _insert_central_slices_rfft_3d.py:30-85, which the reference keeps internal. */
+int tt_slice_geometry(const void *rotation_matrices, int32_t mode, uint8_t *flags, float *coords,
+                      const tt_slice_params *p, void *stream);
+
+/* Bytes of workspace tt_extract_central_slices_rfft_3d_backward needs when a
+ * rotation gradient is requested (0 otherwise is also accepted then). */
+size_t tt_extract_backward_workspace_bytes(const tt_slice_params *p);
+
+/* Backward of the extraction.  grad_slices: complex64 (n, img_h, img_w/2+1),
+ * PyTorch's convention for complex gradients (dL = Re(conj(G) dS)).
+ * grad_volume (nullable): complex64 (vol_d, vol_h, vol_w), ACCUMULATED into.
+ * grad_rotation (nullable): (n, 3, 3) in the rotation dtype, overwritten; the
+ * elements zeroed by rot_tolerance get zero gradient.  The rotation gradient
+ * is reduced deterministically through the caller's workspace.
+ * Replaces the autograd graph of extract_central_slices_rfft_3d
+ * (grid_sampler_3d_backward + the coordinate chain of _dft_utils.py:61-67). */
+int tt_extract_central_slices_rfft_3d_backward(const void *volume_rfft,
+                                               const void *rotation_matrices,
+                                               const void *grad_slices, void *grad_volume,
+                                               void *grad_rotation, void *workspace,
+                                               size_t workspace_bytes,
+                                               const tt_slice_params *p, void *stream);
+
+/* Central-slice insertion, splat stage: trilinear scatter of the slices and of
+ * the interpolation weights into volume_rfft / weights (both ACCUMULATED into),
+ * with the reference's strict x<0 conjugate redirect, the x=0/y<0 source-pixel
+ * exclusion and whole-point bounds rejection.  The Friedel mirror of the x=0
+ * plane is NOT applied here: call tt_friedel_mirror_x0 once after the last
+ * splat into a volume.  complex128 = 1: image/volume complex128 and weights
+ * float64 (coordinates and weights still computed in float32, as the
+ * reference does); else complex64 / float32.
+ * Replaces _insert_central_slices_rfft_3d.py:9-106 and :213-346. */
+int tt_insert_central_slices_rfft_3d(const void *image_rfft, int32_t complex128,
+                                     const void *rotation_matrices, void *volume_rfft,
+                                     void *weights, const tt_slice_params *p, void *stream);
+
+/* Friedel completion of the x=0 plane, equal to the reference's per-corner
+ * mirror insertion (_insert_central_slices_rfft_3d.py:350-404):
+ * out[v] = acc[v] + conj(acc[m(v)]) unless m(v) is the DC voxel, with
+ * m(z, y) = ((d - z) % d, (h - y) % h), and the same for the weights.
+ * channels volumes of (d, h, w_rfft) share one weight volume (weights may be
+ * NULL).  In place. */
+int tt_friedel_mirror_x0(void *volume_rfft, void *weights, int32_t complex128, int64_t channels,
+                         int64_t d, int64_t h, int64_t w_rfft, void *stream);
+
+/* ---- generic 3D interpolation (torch_image_interpolation) -------------
+ * dtype codes: 0 float32, 1 float64, 2 complex64, 3 complex128.  Images are
+ * (channels, d, h, w) of that dtype. */
+
+/* Samples at n zyx coordinates (n, 3) of the image's real dtype into out
+ * (n, channels): trilinear (grid_sample, padding 'border', align_corners) or
+ * nearest (nearbyint); zero where any coordinate is outside [0, dim-1].
+ * Replaces sample_image_3d, image_interpolation_3d.py:11-101. */
+int tt_sample_image_3d(const void *image, int32_t dtype, int64_t channels, int64_t d, int64_t h,
+                       int64_t w, const void *coordinates, int64_t n, void *out, int32_t nearest,
+                       void *stream);
+
+/* Splats values (n, channels) at float32 coordinates (n, 3) into image and
+ * weights (d, h, w; float32, or float64 when weights_f64), ACCUMULATED into:
+ * trilinear (floor/ceil corners, float32 weights) or nearest (rint, weight 1);
+ * points with any coordinate outside [0, dim-1] are dropped.
+ * Replaces insert_into_image_3d, image_interpolation_3d.py:104-275. */
+int tt_insert_into_image_3d(const void *values, int32_t dtype, const float *coordinates, int64_t n,
+                            void *image, int64_t channels, int64_t d, int64_t h, int64_t w,
+                            void *weights, int32_t weights_f64, int32_t nearest, void *stream);
+
+/* ---- elementwise passes around the FFTs of the real-space wrappers ------
+ * is_f64 selects float64 (else float32) real data; complex128 likewise. */
+
+/* out (n^3, n = d + 2*pad) = fftshift(pad(volume, pad) * sinc(|f|)^2), the FFT
+ * input of project_3d_to_2d (project.py:48-69).  volume (d, d, d). */
+int tt_project_prepare(const void *volume, int32_t is_f64, int64_t d, int64_t pad, void *out,
+                       void *stream);
+
+/* out (m, n-2*pad, n-2*pad) = crop(ifftshift(images, (-2, -1)), pad) for
+ * images (m, n, n) (project.py:87-92). */
+int tt_recentre_crop_2d(const void *images, int32_t is_f64, int64_t m, int64_t n, int64_t pad,
+                        void *out, void *stream);
+
+/* out (m, n, n) = fftshift(pad(images, pad), (-2, -1)), images (m, d, d),
+ * n = d + 2*pad (backproject.py:48-59). */
+int tt_pad_fftshift_2d(const void *images, int32_t is_f64, int64_t m, int64_t d, int64_t pad,
+                       void *out, void *stream);
+
+/* Friedel completion + division by max(weights, 1) + ifftshift along (d, h)
+ * of `channels` splatted (not yet mirrored) rfft volumes sharing one weight
+ * volume (backproject.py:66-79).  out must not alias volume_acc. */
+int tt_backproject_normalize(const void *volume_acc, const void *weights, int32_t complex128,
+                             int64_t channels, int64_t d, int64_t h, int64_t w_rfft, void *out,
+                             void *stream);
+
+/* out (channels, c^3), c = n - 2*pad = crop(ifftshift(volume) / sinc(|f|)^2)
+ * of the irfft output volume (channels, n^3) (backproject.py:80-92). */
+int tt_backproject_finish(const void *volume, int32_t is_f64, int64_t channels, int64_t n,
+                          int64_t pad, void *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TEAMTOMO_B200_H */

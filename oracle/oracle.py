@@ -1,0 +1,436 @@
+"""CPU oracle for the Fourier-slice path (TEST INFRASTRUCTURE ONLY).
+
+Nothing in ``teamtomo_b200`` imports this module.  Only ``tests/``, the smoke
+check and the CPU-baseline legs of ``bench.py`` use it, as the checker.
+
+Two layers:
+
+* ``liboracle.so`` (``fourier_slice_oracle.c``): float32 restatement of the
+  reference's central-slice extraction, insertion (with its per-corner Friedel
+  mirror) and the extraction's gradients.  Built by ``oracle/Makefile``.
+* numpy restatements of ``torch_image_interpolation.sample_image_3d`` /
+  ``insert_into_image_3d`` (image_interpolation_3d.py:11-101, 104-275) and of
+  the real-space wrappers ``project_3d_to_2d`` (torch_fourier_slice/project.py:12-93)
+  and ``backproject_2d_to_3d`` (torch_fourier_slice/backproject.py:11-92).
+
+All arrays are numpy; complex arrays are complex64/complex128 C-contiguous.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_f32 = ctypes.c_float
+
+
+def build() -> str:
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(
+            os.path.join(_HERE, "fourier_slice_oracle.c")
+        ):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_extract.argtypes = [_f32p, _i64, _i64, _i64, _f32p, _i64, _i64, _i64, _i64,
+                                  _int, _f32, _int, _f32, _f32, _int, _f32, _f32p, _u8p,
+                                  _f32p, _int]
+        L.orc_extract_grad.argtypes = [_f32p, _i64, _i64, _i64, _f32p, _i64, _i64, _i64, _i64,
+                                       _int, _f32, _int, _f32, _f32, _int, _f32, _f32p, _f32p,
+                                       _f64p, _int]
+        L.orc_slice_geometry.argtypes = [_f32p, _i64, _i64, _i64, _i64, _i64, _i64, _i64,
+                                         _int, _f32, _int, _f32, _f32, _int, _f32, _int, _u8p,
+                                         _f32p]
+        for name, p in (("orc_insert_c64", _f32p), ("orc_insert_c128", _f64p),
+                        ("orc_insert_c64_mt", _f32p)):
+            getattr(L, name).argtypes = [p, _i64, _i64, _i64, _i64, _f32p, _int, _f32, _int,
+                                         p, p, _int, _int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a, t):
+    if a is None:
+        return ctypes.cast(None, t)
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(t)
+
+
+def _rot_f32(rotation_matrices) -> np.ndarray:
+    r = np.asarray(rotation_matrices)
+    return np.ascontiguousarray(r.astype(np.float32).reshape(-1, 9))
+
+
+def _f32_scalar(x: float) -> np.float32:
+    return np.float32(x)
+
+
+def extract(volume_rfft, image_shape, rotation_matrices, fftfreq_max=None, zyx_matrices=False,
+            x_tolerance=1e-8, rot_tolerance=1e-8, return_aux=False, nthreads=1):
+    """Restatement of extract_central_slices_rfft_3d (complex64 volumes)."""
+    vol = np.ascontiguousarray(volume_rfft, dtype=np.complex64)
+    D, H, W = vol.shape
+    R = np.asarray(rotation_matrices)
+    stack = R.shape[:-2]
+    r = _rot_f32(R)
+    n = r.shape[0]
+    d, h, w = (int(s) for s in image_shape)
+    wr = w // 2 + 1
+    out = np.zeros((n, h, wr), np.complex64)
+    conj = np.zeros((n, h, wr), np.uint8) if return_aux else None
+    coords = np.zeros((n, h, wr, 3), np.float32) if return_aux else None
+    lib().orc_extract(
+        _ptr(vol.view(np.float32), _f32p), D, H, W, _ptr(r, _f32p), n, d, h, w,
+        int(fftfreq_max is not None), _f32_scalar(fftfreq_max or 0.0), int(zyx_matrices),
+        _f32_scalar(x_tolerance), _f32_scalar(x_tolerance * 10),
+        int(rot_tolerance is not None), _f32_scalar(rot_tolerance or 0.0),
+        _ptr(out.view(np.float32), _f32p), _ptr(conj, _u8p),
+        _ptr(coords, _f32p), nthreads)
+    out = out.reshape(*stack, h, wr)
+    if return_aux:
+        return out, conj.reshape(*stack, h, wr).astype(bool), coords.reshape(*stack, h, wr, 3)
+    return out
+
+
+def extract_grad(volume_rfft, image_shape, rotation_matrices, grad, fftfreq_max=None,
+                 zyx_matrices=False, x_tolerance=1e-8, rot_tolerance=1e-8, want_dvol=True,
+                 want_drot=True, nthreads=1):
+    """Gradients of the extraction w.r.t. the volume and the rotation matrices."""
+    vol = np.ascontiguousarray(volume_rfft, dtype=np.complex64)
+    D, H, W = vol.shape
+    R = np.asarray(rotation_matrices)
+    r = _rot_f32(R)
+    n = r.shape[0]
+    d, h, w = (int(s) for s in image_shape)
+    g = np.ascontiguousarray(np.asarray(grad, dtype=np.complex64).reshape(n, h, w // 2 + 1))
+    dvol = np.zeros_like(vol) if want_dvol else None
+    drot = np.zeros((n, 9), np.float64) if want_drot else None
+    lib().orc_extract_grad(
+        _ptr(vol.view(np.float32), _f32p), D, H, W, _ptr(r, _f32p), n, d, h, w,
+        int(fftfreq_max is not None), _f32_scalar(fftfreq_max or 0.0), int(zyx_matrices),
+        _f32_scalar(x_tolerance), _f32_scalar(x_tolerance * 10),
+        int(rot_tolerance is not None), _f32_scalar(rot_tolerance or 0.0),
+        _ptr(g.view(np.float32), _f32p),
+        _ptr(dvol.view(np.float32) if dvol is not None else None, _f32p),
+        _ptr(drot, _f64p), nthreads)
+    if drot is not None:
+        drot = drot.reshape(R.shape)
+    return dvol, drot
+
+
+def insert(image_rfft, volume_shape, rotation_matrices, fftfreq_max=None, zyx_matrices=False,
+           nthreads=1, mirror=True):
+    """Restatement of insert_central_slices_rfft_3d -> (volume, weights).
+
+    ``mirror=False`` leaves out the per-corner Friedel mirror insertion (used
+    to check the x=0 plane post-pass form against the reference)."""
+    img = np.asarray(image_rfft)
+    double = img.dtype == np.complex128
+    img = np.ascontiguousarray(img, dtype=np.complex128 if double else np.complex64)
+    vd, vh, vw = (int(s) for s in volume_shape)
+    wr = vw // 2 + 1
+    r = _rot_f32(rotation_matrices)
+    n = r.shape[0]
+    img = img.reshape(n, vh, wr)
+    real = np.float64 if double else np.float32
+    vol = np.zeros((vd, vh, wr), img.dtype)
+    wts = np.zeros((vd, vh, wr), real)
+    if double:
+        fn, p = lib().orc_insert_c128, _f64p
+    else:
+        fn, p = (lib().orc_insert_c64_mt if nthreads != 1 else lib().orc_insert_c64), _f32p
+    fn(_ptr(img.view(real), p), n, vd, vh, vw, _ptr(r, _f32p), int(fftfreq_max is not None),
+       _f32_scalar(fftfreq_max or 0.0), int(zyx_matrices), _ptr(vol.view(real), p),
+       _ptr(wts, p), int(mirror), nthreads)
+    return vol, wts
+
+
+def slice_geometry(rotation_matrices, image_shape, volume_dims, mode, fftfreq_max=None,
+                   zyx_matrices=False, x_tolerance=1e-8, rot_tolerance=1e-8):
+    """Per-pixel (flags, coords) of the extraction (mode 0) / insertion (mode 1)
+    rule: flags bit0 kept, bit1 conjugated, bit2 inside the volume."""
+    r = _rot_f32(rotation_matrices)
+    n = r.shape[0]
+    d, h, w = (int(s) for s in image_shape)
+    D, H, W = (int(s) for s in volume_dims)
+    wr = w // 2 + 1
+    flags = np.zeros((n, h, wr), np.uint8)
+    coords = np.zeros((n, h, wr, 3), np.float32)
+    lib().orc_slice_geometry(
+        _ptr(r, _f32p), n, d, h, w, D, H, W, int(fftfreq_max is not None),
+        _f32_scalar(fftfreq_max or 0.0), int(zyx_matrices), _f32_scalar(x_tolerance),
+        _f32_scalar(x_tolerance * 10), int(rot_tolerance is not None),
+        _f32_scalar(rot_tolerance or 0.0), int(mode), _ptr(flags, _u8p), _ptr(coords, _f32p))
+    return flags, coords
+
+
+def extract_f64(volume_rfft, image_shape, rotation_matrices, zyx_matrices=False):
+    """float64 restatement of the extraction for finite-difference checks.
+
+    Same geometry as the reference (frequency grid, xyz->zyx flip, conjugate
+    redirect, array coordinates, grid_sample trilinear, zero outside) but in
+    float64 with the plain sign rule x' < 0 (no tolerances); finite
+    differences use rotations with no pixel near the x' = 0 boundary."""
+    vol = np.asarray(volume_rfft, np.complex128)
+    D, H, W = vol.shape
+    R = np.asarray(rotation_matrices, np.float64).reshape(-1, 3, 3)
+    M = R if zyx_matrices else R[:, ::-1, ::-1]
+    d, h, w = (int(s) for s in image_shape)
+    k = np.arange(h)
+    fy = np.fft.fftshift(np.where(k < (h + 1) // 2, k, k - h) / h)
+    fx = np.arange(w // 2 + 1) / w
+    q = np.stack(np.broadcast_arrays(np.zeros((h, 1)), fy[:, None], fx[None, :]), -1)  # (h, wr, 3)
+    p = np.einsum("nij,hwj->nhwi", M, q)
+    cj = p[..., 2] < -1e-8
+    # near-zero tie-break of _determine_near_zero_conjugate_mask (:9-81)
+    r11 = M[:, 2, 2][:, None, None]
+    r12 = M[:, 2, 1][:, None, None]
+    near = np.abs(p[..., 2]) < 1e-8
+    cj |= near & np.where(np.abs(r11) <= 1e-7, r12 < 0, r11 < 0)
+    p[cj] *= -1
+    c = np.empty_like(p)
+    c[..., 0] = (p[..., 0] + 0.5) / (1 - 1 / d) * (d - 1)
+    c[..., 1] = (p[..., 1] + 0.5) / (1 - 1 / h) * (h - 1)
+    c[..., 2] = p[..., 2] * 2 * (w // 2)
+    inside = np.all((c >= 0) & (c <= np.array([D, H, W]) - 1), -1)
+    cc = np.clip(c, 0, np.array([D, H, W]) - 1)
+    f = np.floor(cc)
+    t = cc - f
+    f = f.astype(np.int64)
+    out = np.zeros(c.shape[:-1], np.complex128)
+    for bz in (0, 1):
+        for by in (0, 1):
+            for bx in (0, 1):
+                zi, yi, xi = f[..., 0] + bz, f[..., 1] + by, f[..., 2] + bx
+                ok = (zi < D) & (yi < H) & (xi < W)
+                wgt = ((t[..., 0] if bz else 1 - t[..., 0]) * (t[..., 1] if by else 1 - t[..., 1])
+                       * (t[..., 2] if bx else 1 - t[..., 2]))
+                v = vol[np.minimum(zi, D - 1), np.minimum(yi, H - 1), np.minimum(xi, W - 1)]
+                out += np.where(ok, v * wgt, 0)
+    out[~inside] = 0
+    out[cj] = np.conj(out[cj])
+    return out
+
+
+def mirror_x0_post_pass(vol, wts):
+    """Friedel completion of the x=0 plane as one post-pass (numpy):
+    out[v] = acc[v] + conj(acc[m v]) unless m v is the DC voxel,
+    m(z, y) = ((d - z) % d, (h - y) % h); the same for the weights."""
+    vol = np.array(vol, copy=True)
+    wts = np.array(wts, copy=True)
+    d, h = vol.shape[-3:-1]
+    z = np.arange(d)[:, None]
+    y = np.arange(h)[None, :]
+    zm, ym = (d - z) % d, (h - y) % h
+    keep = ~((zm == d // 2) & (ym == h // 2))
+    p, pw = vol[..., 0].copy(), wts[..., 0].copy()
+    vol[..., 0] = p + np.where(keep, np.conj(p[..., zm, ym]), 0)
+    wts[..., 0] = pw + np.where(keep, pw[zm, ym], 0)
+    return vol, wts
+
+
+# ----------------------------------------------------------------------------
+# torch_image_interpolation restatements (numpy)
+# ----------------------------------------------------------------------------
+
+def _roundtrip(c, n, dt):
+    """array coord -> grid_sample coord -> source index (align_corners=True)."""
+    fn = dt.type(n)
+    half = dt.type(0.5) * fn - dt.type(0.5)
+    g = c / half - dt.type(1)
+    ix = ((g + dt.type(1)) / dt.type(2)) * (fn - dt.type(1))
+    return np.clip(ix, dt.type(0), fn - dt.type(1))
+
+
+def sample_image_3d(image, coordinates, interpolation="trilinear"):
+    """Restatement of sample_image_3d (image_interpolation_3d.py:11-101)."""
+    image = np.asarray(image)
+    if image.ndim not in (3, 4):
+        raise ValueError("image should have shape (d, h, w) or (c, d, h, w)")
+    multi = image.ndim == 4
+    img = image if multi else image[None]
+    coords = np.asarray(coordinates)
+    batch = coords.shape[:-1]
+    c = coords.reshape(-1, 3)
+    rdt = np.dtype(np.float64) if img.dtype in (np.float64, np.complex128) else np.dtype(np.float32)
+    c = c.astype(rdt)
+    C, D, H, W = img.shape
+    out = np.zeros((c.shape[0], C), img.dtype)
+    iz, iy, ix = _roundtrip(c[:, 0], D, rdt), _roundtrip(c[:, 1], H, rdt), _roundtrip(c[:, 2], W, rdt)
+    if interpolation == "nearest":
+        z = np.rint(iz).astype(np.int64)
+        y = np.rint(iy).astype(np.int64)
+        x = np.rint(ix).astype(np.int64)
+        ok = (z >= 0) & (z < D) & (y >= 0) & (y < H) & (x >= 0) & (x < W)
+        out[ok] = img[:, z[ok], y[ok], x[ok]].T
+    else:
+        z0, y0, x0 = np.floor(iz), np.floor(iy), np.floor(ix)
+        z1, y1, x1 = z0 + 1, y0 + 1, x0 + 1
+        for bz in (0, 1):
+            for by in (0, 1):
+                for bx in (0, 1):
+                    wz = (iz - z0) if bz else (z1 - iz)
+                    wy = (iy - y0) if by else (y1 - iy)
+                    wx = (ix - x0) if bx else (x1 - ix)
+                    w = wx * wy * wz
+                    zi = (z1 if bz else z0).astype(np.int64)
+                    yi = (y1 if by else y0).astype(np.int64)
+                    xi = (x1 if bx else x0).astype(np.int64)
+                    ok = (zi < D) & (yi < H) & (xi < W)
+                    v = np.zeros_like(out)
+                    v[ok] = img[:, zi[ok], yi[ok], xi[ok]].T
+                    out += v * w[:, None]
+    shape = np.array([D, H, W], rdt)
+    inside = np.all((c >= 0) & (c <= shape - 1), axis=-1)
+    out[~inside] = 0
+    out = out.reshape(*batch, C)
+    return out if multi else out[..., 0]
+
+
+def insert_into_image_3d(values, coordinates, image, weights=None, interpolation="trilinear"):
+    """Restatement of insert_into_image_3d (image_interpolation_3d.py:104-275).
+
+    Accumulates into copies of ``image`` / ``weights`` and returns them."""
+    image = np.array(image, copy=True)
+    multi = image.ndim == 4
+    D, H, W = image.shape[-3:]
+    values = np.asarray(values)
+    coords = np.asarray(coordinates)
+    vshape = values.shape[:-1] if multi else values.shape
+    if vshape != coords.shape[:-1]:
+        raise ValueError("One coordinate triplet is required for each value in data.")
+    if coords.shape[-1] != 3:
+        raise ValueError("Coordinates must be 3D with shape (..., 3).")
+    if image.dtype != values.dtype:
+        raise ValueError("Image and values must have the same dtype.")
+    weights = np.zeros((D, H, W), np.float32) if weights is None else np.array(weights, copy=True)
+    img = image if multi else image[None]
+    vals = values.reshape(-1, img.shape[0]) if multi else values.reshape(-1, 1)
+    c = coords.reshape(-1, 3).astype(np.float32)
+    ub = np.array([D, H, W], np.float32) - 1
+    ok = np.all((c >= 0) & (c <= ub), axis=-1)
+    vals, c = vals[ok], c[ok]
+    if interpolation == "nearest":
+        idx = np.rint(c).astype(np.int64)
+        for ch in range(img.shape[0]):
+            np.add.at(img[ch], (idx[:, 0], idx[:, 1], idx[:, 2]), vals[:, ch])
+        np.add.at(weights, (idx[:, 0], idx[:, 1], idx[:, 2]), np.ones(len(c), weights.dtype))
+    elif interpolation == "trilinear":
+        lo = np.floor(c)
+        hi = np.ceil(c)
+        t = c - lo
+        one = np.float32(1)
+        for bz in (0, 1):
+            for by in (0, 1):
+                for bx in (0, 1):
+                    fz = t[:, 0] if bz else one - t[:, 0]
+                    fy = t[:, 1] if by else one - t[:, 1]
+                    fx = t[:, 2] if bx else one - t[:, 2]
+                    w = ((fz * fy) * fx).astype(weights.dtype)
+                    zi = (hi if bz else lo)[:, 0].astype(np.int64)
+                    yi = (hi if by else lo)[:, 1].astype(np.int64)
+                    xi = (hi if bx else lo)[:, 2].astype(np.int64)
+                    for ch in range(img.shape[0]):
+                        np.add.at(img[ch], (zi, yi, xi), vals[:, ch] * w.astype(vals.dtype))
+                    np.add.at(weights, (zi, yi, xi), w)
+    out = img if multi else img[0]
+    return out, weights
+
+
+# ----------------------------------------------------------------------------
+# real-space wrappers (numpy FFTs around the C oracle)
+# ----------------------------------------------------------------------------
+
+def _fftfreq_norm_grid(shape):
+    """|fftfreq| grid, fftshifted, float32 (torch_grid_utils fftfreq_grid norm=True)."""
+    axes = []
+    for n in shape:
+        k = np.arange(n)
+        kk = np.where(k < (n + 1) // 2, k, k - n).astype(np.float32) * np.float32(1.0 / n)
+        axes.append(np.fft.fftshift(kk))
+    g = np.meshgrid(*axes, indexing="ij")
+    s = np.zeros(shape, np.float32)
+    for a in g:
+        s = s + a * a
+    return np.sqrt(s)
+
+
+def _sinc(x):
+    return np.sinc(x.astype(np.float64)).astype(np.float32)
+
+
+def _crop_pad(pad_factor, n):
+    return int((n * (pad_factor - 1.0)) // 2)
+
+
+def project_3d_to_2d(volume, rotation_matrices, pad_factor=2.0, fftfreq_max=None,
+                     zyx_matrices=False):
+    vol = np.asarray(volume, np.float32)
+    d, h, w = vol.shape
+    if len({d, h, w}) != 1:
+        raise ValueError("all dimensions of volume must be equal.")
+    if pad_factor < 1.0:
+        raise ValueError("pad_factor must be >= 1.0")
+    p = 0
+    if pad_factor > 1.0:
+        p = _crop_pad(pad_factor, w)
+        vol = np.pad(vol, p)
+    shape = vol.shape
+    vol = vol * _sinc(_fftfreq_norm_grid(shape)) ** 2
+    dft = np.fft.rfftn(np.fft.fftshift(vol), axes=(0, 1, 2))
+    dft = np.fft.fftshift(dft, axes=(0, 1)).astype(np.complex64)
+    sl = extract(dft, shape, rotation_matrices, fftfreq_max=fftfreq_max,
+                 zyx_matrices=zyx_matrices)
+    sl = np.fft.ifftshift(sl, axes=(-2,))
+    im = np.fft.irfftn(sl, s=shape[-2:], axes=(-2, -1))
+    im = np.fft.ifftshift(im, axes=(-2, -1)).astype(np.float32)
+    if p:
+        im = im[..., p:-p, p:-p]
+    return im
+
+
+def backproject_2d_to_3d(images, rotation_matrices, pad_factor=2.0, fftfreq_max=None,
+                         zyx_matrices=False):
+    imgs = np.asarray(images)
+    h, w = imgs.shape[-2:]
+    if h != w:
+        raise ValueError("images must be square.")
+    if pad_factor < 1.0:
+        raise ValueError("pad_factor must be >= 1.0")
+    double = imgs.dtype == np.float64
+    p = 0
+    if pad_factor > 1.0:
+        p = _crop_pad(pad_factor, w)
+        imgs = np.pad(imgs, [(0, 0)] * (imgs.ndim - 2) + [(p, p), (p, p)])
+    w = imgs.shape[-1]
+    shape = (w, w, w)
+    f = np.fft.rfftn(np.fft.fftshift(imgs, axes=(-2, -1)), axes=(-2, -1))
+    f = np.fft.fftshift(f, axes=(-2,)).astype(np.complex128 if double else np.complex64)
+    vol, wts = insert(f, shape, rotation_matrices, fftfreq_max=fftfreq_max,
+                      zyx_matrices=zyx_matrices)
+    vol = vol / np.maximum(wts, 1.0)
+    vol = np.fft.ifftshift(vol, axes=(0, 1))
+    real = np.fft.irfftn(vol, s=shape, axes=(0, 1, 2))
+    real = np.fft.ifftshift(real)
+    real = real / _sinc(_fftfreq_norm_grid(shape)).astype(real.dtype) ** 2
+    if p:
+        real = real[p:-p, p:-p, p:-p]
+    return real.astype(np.float64 if double else np.float32)

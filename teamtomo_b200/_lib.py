@@ -1,0 +1,120 @@
+"""ctypes binding of the C ABI declared in ``include/teamtomo_b200.h``.
+
+The CUDA library is required: there is no CPU fallback.  Importing the
+package succeeds without a GPU (so CPU-side checks can run), but every call
+that launches work needs the built ``libteamtomo_b200.so`` and CUDA tensors.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+from . import _build
+
+TT_OK, TT_ERR_INVALID, TT_ERR_CUDA, TT_ERR_WORKSPACE = 0, 1, 2, 3
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_f32 = ctypes.c_float
+_sz = ctypes.c_size_t
+
+
+class SliceParams(ctypes.Structure):
+    """Mirror of ``tt_slice_params``."""
+
+    _fields_ = [
+        ("n", _i64), ("img_d", _i64), ("img_h", _i64), ("img_w", _i64),
+        ("vol_d", _i64), ("vol_h", _i64), ("vol_w", _i64),
+        ("has_fftfreq_max", _i32), ("fftfreq_max", _f32),
+        ("zyx_matrices", _i32),
+        ("x_tolerance", _f32), ("x_tolerance10", _f32),
+        ("has_rot_tolerance", _i32), ("rot_tolerance", _f32),
+        ("rotation_f64", _i32), ("volume_unshifted", _i32), ("slices_unshifted", _i32),
+        ("reserved", _i32),
+    ]
+
+
+# name -> (argtypes, restype); every symbol the header declares
+SIGNATURES = {
+    "tt_version": ([], _i32),
+    "tt_last_error": ([], ctypes.c_char_p),
+    "tt_extract_central_slices_rfft_3d": ([_vp, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_slice_geometry": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_extract_backward_workspace_bytes": ([ctypes.POINTER(SliceParams)], _sz),
+    "tt_extract_central_slices_rfft_3d_backward": (
+        [_vp, _vp, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_insert_central_slices_rfft_3d": (
+        [_vp, _i32, _vp, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_friedel_mirror_x0": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp], _i32),
+    "tt_sample_image_3d": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i32, _vp], _i32),
+    "tt_insert_into_image_3d": (
+        [_vp, _i32, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _i32, _i32, _vp], _i32),
+    "tt_project_prepare": ([_vp, _i32, _i64, _i64, _vp, _vp], _i32),
+    "tt_recentre_crop_2d": ([_vp, _i32, _i64, _i64, _i64, _vp, _vp], _i32),
+    "tt_pad_fftshift_2d": ([_vp, _i32, _i64, _i64, _i64, _vp, _vp], _i32),
+    "tt_backproject_normalize": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp], _i32),
+    "tt_backproject_finish": ([_vp, _i32, _i64, _i64, _i64, _vp, _vp], _i32),
+}
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load() -> ctypes.CDLL:
+    """Load the CUDA library (building it first if the sources are newer)."""
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not os.path.exists(path) or _build.needs_build():
+            try:
+                _build.build()
+            except Exception as exc:  # no nvcc or a compile error: fail loudly
+                if not os.path.exists(path):
+                    raise RuntimeError(
+                        f"teamtomo_b200 CUDA library missing at {path} and could not be built: {exc}"
+                    ) from exc
+        L = ctypes.CDLL(path)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(status: int, what: str) -> None:
+    if status == TT_OK:
+        return
+    msg = load().tt_last_error().decode(errors="replace")
+    if status == TT_ERR_INVALID:
+        raise ValueError(f"{what}: {msg}")
+    raise RuntimeError(f"{what}: {msg}")
+
+
+def ptr(t: torch.Tensor | None):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def stream_of(device: torch.device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def require_cuda(*tensors: torch.Tensor) -> torch.device:
+    dev = None
+    for t in tensors:
+        if t is None:
+            continue
+        if not t.is_cuda:
+            raise RuntimeError(
+                "teamtomo_b200 runs on CUDA tensors only (got a tensor on "
+                f"{t.device}); there is no CPU fallback"
+            )
+        dev = t.device if dev is None else dev
+    return dev

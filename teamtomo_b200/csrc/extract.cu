@@ -1,0 +1,356 @@
+// Central-slice extraction from an fftshifted rfft volume, and its backward.
+//
+// Forward (extract_central_slices_rfft_3d, _extract_central_slices_rfft_3d.py:84-222):
+// one thread per slice pixel.  The pixel's frequency is generated in
+// registers, rotated with the reference's float32 operation order, redirected
+// into the stored half (conjugate rule with the x-tolerance tie-break), scaled
+// to array coordinates and sampled trilinearly with grid_sample's semantics
+// (padding_mode='border', align_corners=True, zero outside [0, n-1]).
+//
+// Backward: the same per-pixel geometry, recomputed rather than stored.
+//   d/dvolume  = trilinear scatter of G' (G conjugated where the sample was)
+//   d/drotation: per pixel Re(conj(G') dV/dc) chained through the coordinate
+//                scale, the conjugate flip and the rotation, reduced per slice.
+// Per-block partial sums of the rotation gradient go to the caller's
+// workspace and are reduced in a fixed order by a second kernel, so the
+// rotation gradient is deterministic.
+#include <cuda_runtime.h>
+
+#include "capi_util.cuh"
+#include "slice_common.cuh"
+
+namespace tt {
+
+constexpr int kExtractThreads = 256;
+
+struct Corners {
+    int z0, y0, x0;
+    float ax0, ax1, ay0, ay1, az0, az1;  // per-axis weights of the low/high corner
+    bool zin, yin, xin;                  // high corner inside the array
+};
+
+// grid_sample trilinear corner set for an inside coordinate c.
+__device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float c[3]) {
+    Corners k;
+    float fz = floorf(c[0]), fy = floorf(c[1]), fx = floorf(c[2]);
+    k.z0 = (int)fz;
+    k.y0 = (int)fy;
+    k.x0 = (int)fx;
+    k.az0 = (fz + 1.0f) - c[0];
+    k.az1 = c[0] - fz;
+    k.ay0 = (fy + 1.0f) - c[1];
+    k.ay1 = c[1] - fy;
+    k.ax0 = (fx + 1.0f) - c[2];
+    k.ax1 = c[2] - fx;
+    k.zin = k.z0 + 1 < g.D;
+    k.yin = k.y0 + 1 < g.H;
+    k.xin = k.x0 + 1 < g.W;
+    return k;
+}
+
+__device__ __forceinline__ void load_rotation(float* sm, const void* rot, int64_t s,
+                                              const SliceGeom& g, bool apply_tol) {
+    if (threadIdx.x < 9) sm[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, apply_tol);
+}
+
+__global__ void __launch_bounds__(kExtractThreads)
+extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
+                   float2* __restrict__ out, SliceGeom g, int tiles) {
+    __shared__ float m[9];
+    const int64_t s = blockIdx.x / tiles;
+    const int tile = blockIdx.x - (int)(s * tiles);
+    load_rotation(m, rot, s, g, true);
+    __syncthreads();
+    const int P = g.img_h * g.wr;
+    const int pix = tile * kExtractThreads + threadIdx.x;
+    if (pix >= P) return;
+    const int iy = pix / g.wr, ix = pix - iy * g.wr;
+    const float qy = shifted_freq(iy, g.img_h, g.inv_h);
+    const float qx = __fmul_rn((float)ix, g.inv_w);
+    float2 r = make_float2(0.0f, 0.0f);
+    if (in_fmax(g, qy, qx)) {
+        float p[3], c[3];
+        rotate_slice_point(m, qy, qx, p);
+        const bool cj = extract_conj(g, m, p[2]);
+        if (cj) {
+            p[0] = -p[0];
+            p[1] = -p[1];
+            p[2] = -p[2];
+        }
+        to_dft_coords(g, p, c);
+        if (inside_volume(g, c)) {
+            Corners k = make_corners(g, c);
+#pragma unroll
+            for (int bz = 0; bz < 2; bz++) {
+                if (bz && !k.zin) continue;
+                const float wz = bz ? k.az1 : k.az0;
+#pragma unroll
+                for (int by = 0; by < 2; by++) {
+                    if (by && !k.yin) continue;
+                    const float wzy = (by ? k.ay1 : k.ay0) * wz;
+                    const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
+                    const float2 v0 = __ldg(vol + base);
+                    const float w0 = k.ax0 * wzy;
+                    r.x = fmaf(v0.x, w0, r.x);
+                    r.y = fmaf(v0.y, w0, r.y);
+                    if (k.xin) {
+                        const float2 v1 = __ldg(vol + base + 1);
+                        const float w1 = k.ax1 * wzy;
+                        r.x = fmaf(v1.x, w1, r.x);
+                        r.y = fmaf(v1.y, w1, r.y);
+                    }
+                }
+            }
+            if (cj) r.y = -r.y;
+        }
+    }
+    out[(s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix] = r;
+}
+
+// Backward.  WANT_DV: scatter into dvol; WANT_DR: per-block partial sums of
+// the 6 non-zero entries of d/dR_zyx (column 0 multiplies the zero z
+// frequency) into part[(s*tiles + tile)*6 + k].
+template <bool WANT_DV, bool WANT_DR>
+__global__ void __launch_bounds__(kExtractThreads)
+extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
+                   const float2* __restrict__ grad, float2* __restrict__ dvol,
+                   float* __restrict__ part, SliceGeom g, int tiles) {
+    __shared__ float m[9];
+    __shared__ float red[kExtractThreads / 32][6];
+    const int64_t s = blockIdx.x / tiles;
+    const int tile = blockIdx.x - (int)(s * tiles);
+    load_rotation(m, rot, s, g, true);
+    __syncthreads();
+    const int P = g.img_h * g.wr;
+    const int pix = tile * kExtractThreads + threadIdx.x;
+    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (pix < P) {
+        const int iy = pix / g.wr, ix = pix - iy * g.wr;
+        const float qy = shifted_freq(iy, g.img_h, g.inv_h);
+        const float qx = __fmul_rn((float)ix, g.inv_w);
+        if (in_fmax(g, qy, qx)) {
+            float p[3], c[3];
+            rotate_slice_point(m, qy, qx, p);
+            const bool cj = extract_conj(g, m, p[2]);
+            if (cj) {
+                p[0] = -p[0];
+                p[1] = -p[1];
+                p[2] = -p[2];
+            }
+            to_dft_coords(g, p, c);
+            if (inside_volume(g, c)) {
+                float2 gv = grad[(s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix];
+                if (cj) gv.y = -gv.y;
+                Corners k = make_corners(g, c);
+                float dz = 0.f, dy = 0.f, dx = 0.f;
+#pragma unroll
+                for (int bz = 0; bz < 2; bz++) {
+                    if (bz && !k.zin) continue;
+                    const float wz = bz ? k.az1 : k.az0;
+                    const float sz = bz ? 1.f : -1.f;
+#pragma unroll
+                    for (int by = 0; by < 2; by++) {
+                        if (by && !k.yin) continue;
+                        const float wy = by ? k.ay1 : k.ay0;
+                        const float sy = by ? 1.f : -1.f;
+                        const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
+#pragma unroll
+                        for (int bx = 0; bx < 2; bx++) {
+                            if (bx && !k.xin) continue;
+                            const float wx = bx ? k.ax1 : k.ax0;
+                            const float sx = bx ? 1.f : -1.f;
+                            if (WANT_DV) {
+                                const float w = wx * wy * wz;
+                                if (w != 0.0f) atomicAdd(dvol + base + bx, make_float2(gv.x * w, gv.y * w));
+                            }
+                            if (WANT_DR) {
+                                const float2 v = __ldg(vol + base + bx);
+                                const float rv = fmaf(gv.x, v.x, gv.y * v.y);
+                                dx = fmaf(rv, sx * wy * wz, dx);
+                                dy = fmaf(rv, sy * wx * wz, dy);
+                                dz = fmaf(rv, sz * wx * wy, dz);
+                            }
+                        }
+                    }
+                }
+                if (WANT_DR) {
+                    const float sg = cj ? -1.f : 1.f;
+                    const float p0 = dz * g.dcdp0 * sg, p1 = dy * g.dcdp1 * sg, p2 = dx * g.dcdp2 * sg;
+                    acc[0] = p0 * qy;
+                    acc[1] = p0 * qx;
+                    acc[2] = p1 * qy;
+                    acc[3] = p1 * qx;
+                    acc[4] = p2 * qy;
+                    acc[5] = p2 * qx;
+                }
+            }
+        }
+    }
+    if (WANT_DR) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            float v = warp_sum(acc[k]);
+            if (lane == 0) red[warp][k] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            float v = 0.f;
+#pragma unroll
+            for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][threadIdx.x];
+            part[((int64_t)s * tiles + tile) * 6 + threadIdx.x] = v;
+        }
+    }
+}
+
+// Sums the per-block partials of each slice in a fixed order and writes the
+// caller-layout gradient: undo the xyz->zyx flip, zero the tolerance-zeroed
+// elements, cast to the rotation dtype.  One thread per (slice, element).
+__global__ void drot_finish_kernel(const float* __restrict__ part, const void* __restrict__ rot,
+                                   void* __restrict__ drot, SliceGeom g, int tiles) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)g.n * 9) return;
+    const int64_t s = idx / 9;
+    const int t = (int)(idx - s * 9);
+    const int a = t / 3, b = t % 3;
+    const int i = g.zyx ? a : 2 - a, j = g.zyx ? b : 2 - b;
+    double v = 0.0;
+    if (j != 0) {
+        const float* ps = part + (int64_t)s * tiles * 6 + i * 2 + (j - 1);
+        for (int k = 0; k < tiles; k++) v += (double)ps[(int64_t)k * 6];
+    }
+    float r = g.rot_f64 ? __double2float_rn(((const double*)rot)[idx]) : ((const float*)rot)[idx];
+    if (g.has_rot_tol && fabsf(r) < g.rot_tol) v = 0.0;
+    if (g.rot_f64)
+        ((double*)drot)[idx] = (double)(float)v;
+    else
+        ((float*)drot)[idx] = (float)v;
+}
+
+// Per-pixel geometry of the extraction (mode 0) or insertion (mode 1) rule,
+// exported for bit-exact checks of the index / mask logic.
+// flags: bit0 inside fftfreq_max (and, for insertion, not the Friedel-
+// redundant x==0,y<0 source pixel), bit1 conjugated, bit2 inside the volume.
+__global__ void slice_geometry_kernel(const void* __restrict__ rot, uint8_t* __restrict__ flags,
+                                      float* __restrict__ coords, SliceGeom g, int tiles, int mode) {
+    __shared__ float m[9];
+    const int64_t s = blockIdx.x / tiles;
+    const int tile = blockIdx.x - (int)(s * tiles);
+    load_rotation(m, rot, s, g, mode == 0);
+    __syncthreads();
+    const int P = g.img_h * g.wr;
+    const int pix = tile * kExtractThreads + threadIdx.x;
+    if (pix >= P) return;
+    const int iy = pix / g.wr, ix = pix - iy * g.wr;
+    const float qy = shifted_freq(iy, g.img_h, g.inv_h);
+    const float qx = __fmul_rn((float)ix, g.inv_w);
+    const int64_t o = s * P + pix;
+    uint8_t f = 0;
+    float c[3] = {0.f, 0.f, 0.f};
+    bool valid = in_fmax(g, qy, qx);
+    if (mode == 1 && qx == 0.0f && qy < 0.0f) valid = false;
+    if (valid) {
+        float p[3];
+        rotate_slice_point(m, qy, qx, p);
+        const bool cj = mode == 0 ? extract_conj(g, m, p[2]) : (p[2] < 0.0f);
+        if (cj) {
+            p[0] = -p[0];
+            p[1] = -p[1];
+            p[2] = -p[2];
+        }
+        to_dft_coords(g, p, c);
+        f = 1 | (cj ? 2 : 0) | (inside_volume(g, c) ? 4 : 0);
+    }
+    flags[o] = f;
+    coords[o * 3 + 0] = c[0];
+    coords[o * 3 + 1] = c[1];
+    coords[o * 3 + 2] = c[2];
+}
+
+static int extract_tiles(const SliceGeom& g) {
+    const int P = g.img_h * g.wr;
+    return (P + kExtractThreads - 1) / kExtractThreads;
+}
+
+}  // namespace tt
+
+using namespace tt;
+
+extern "C" int tt_extract_central_slices_rfft_3d(const void* volume_rfft, const void* rotation_matrices,
+                                                 void* slices_out, const tt_slice_params* p, void* stream) {
+    if (int e = validate_params(p)) return e;
+    if (p->n == 0) return TT_OK;
+    if (!volume_rfft || !rotation_matrices || !slices_out)
+        return fail(TT_ERR_INVALID, "extract: NULL pointer argument");
+    SliceGeom g = make_geom(*p);
+    const int tiles = extract_tiles(g);
+    const int64_t blocks = (int64_t)g.n * tiles;
+    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract: too many blocks");
+    extract_fwd_kernel<<<(unsigned)blocks, kExtractThreads, 0, as_stream(stream)>>>(
+        (const float2*)volume_rfft, rotation_matrices, (float2*)slices_out, g, tiles);
+    return check_launch("extract_fwd_kernel");
+}
+
+extern "C" int tt_slice_geometry(const void* rotation_matrices, int32_t mode, uint8_t* flags, float* coords,
+                                 const tt_slice_params* p, void* stream) {
+    if (int e = validate_params(p)) return e;
+    if (p->n == 0) return TT_OK;
+    if (!rotation_matrices || !flags || !coords) return fail(TT_ERR_INVALID, "slice_geometry: NULL pointer argument");
+    if (mode != 0 && mode != 1) return fail(TT_ERR_INVALID, "slice_geometry: mode must be 0 or 1");
+    SliceGeom g = make_geom(*p);
+    const int tiles = extract_tiles(g);
+    const int64_t blocks = (int64_t)g.n * tiles;
+    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "slice_geometry: too many blocks");
+    slice_geometry_kernel<<<(unsigned)blocks, kExtractThreads, 0, as_stream(stream)>>>(rotation_matrices, flags,
+                                                                                     coords, g, tiles, mode);
+    return check_launch("slice_geometry_kernel");
+}
+
+extern "C" size_t tt_extract_backward_workspace_bytes(const tt_slice_params* p) {
+    if (!p || p->n <= 0 || p->img_h < 1 || p->img_w < 1) return 0;
+    const int64_t P = p->img_h * (p->img_w / 2 + 1);
+    const int64_t tiles = (P + kExtractThreads - 1) / kExtractThreads;
+    return (size_t)(p->n * tiles * 6 * sizeof(float));
+}
+
+extern "C" int tt_extract_central_slices_rfft_3d_backward(
+    const void* volume_rfft, const void* rotation_matrices, const void* grad_slices, void* grad_volume,
+    void* grad_rotation, void* workspace, size_t workspace_bytes, const tt_slice_params* p, void* stream) {
+    if (int e = validate_params(p)) return e;
+    if (p->n == 0) return TT_OK;
+    if (!volume_rfft || !rotation_matrices || !grad_slices)
+        return fail(TT_ERR_INVALID, "extract backward: NULL pointer argument");
+    if (!grad_volume && !grad_rotation) return TT_OK;
+    SliceGeom g = make_geom(*p);
+    const int tiles = extract_tiles(g);
+    const int64_t blocks = (int64_t)g.n * tiles;
+    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract backward: too many blocks");
+    cudaStream_t st = as_stream(stream);
+    if (grad_rotation) {
+        const size_t need = tt_extract_backward_workspace_bytes(p);
+        if (!workspace || workspace_bytes < need)
+            return fail(TT_ERR_WORKSPACE, "extract backward: workspace of %zu bytes needed, got %zu", need,
+                        workspace_bytes);
+    }
+    const float2* v = (const float2*)volume_rfft;
+    const float2* gr = (const float2*)grad_slices;
+    float2* dv = (float2*)grad_volume;
+    float* part = (float*)workspace;
+    if (grad_volume && grad_rotation)
+        extract_bwd_kernel<true, true><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr, dv,
+                                                                                  part, g, tiles);
+    else if (grad_volume)
+        extract_bwd_kernel<true, false><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr,
+                                                                                   dv, part, g, tiles);
+    else
+        extract_bwd_kernel<false, true><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr,
+                                                                                   dv, part, g, tiles);
+    if (int e = check_launch("extract_bwd_kernel")) return e;
+    if (grad_rotation) {
+        const int64_t total = (int64_t)g.n * 9;
+        drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rotation_matrices,
+                                                                          grad_rotation, g, tiles);
+        if (int e = check_launch("drot_finish_kernel")) return e;
+    }
+    return TT_OK;
+}

@@ -1,0 +1,171 @@
+// Generic 3D interpolation primitives of torch_image_interpolation
+// (image_interpolation_3d.py:11-101 sample_image_3d, :104-275 insert_into_image_3d).
+//
+// sample: one thread per coordinate.  Trilinear follows grid_sample with
+//   padding_mode='border', align_corners=True: the 8 corners of the clamped
+//   coordinate, corners past the last index contribute nothing, and samples
+//   whose coordinate is outside [0, n-1] on any axis are zero.  Nearest rounds
+//   half to even (nearbyint).
+// insert: one thread per value.  Coordinates are float32 (the reference casts
+//   with .float()); points outside [0, n-1] on any axis are dropped; trilinear
+//   splats with floor/ceil corners and float32 (1-t)/t weight products cast to
+//   the weight dtype; nearest adds the value and a weight of 1 at rint(c).
+// Element types: float32, float64, complex64, complex128 (dtype codes 0-3).
+#include <cuda_runtime.h>
+
+#include "capi_util.cuh"
+
+namespace tt {
+
+template <typename T>
+__device__ __forceinline__ void atomic_add_real(T* p, T v) {
+    atomicAdd(p, v);
+}
+
+template <typename T, int E>
+__global__ void sample3d_kernel(const T* __restrict__ img, int64_t C, int D, int H, int W,
+                                const T* __restrict__ coords, int64_t n, T* __restrict__ out, int nearest) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T cz = coords[i * 3 + 0], cy = coords[i * 3 + 1], cx = coords[i * 3 + 2];
+    T* o = out + i * C * E;
+    const bool inside = cz >= (T)0 && cz <= (T)(D - 1) && cy >= (T)0 && cy <= (T)(H - 1) && cx >= (T)0 &&
+                        cx <= (T)(W - 1);
+    const int64_t plane = (int64_t)D * H * W;
+    if (!inside) {
+        for (int64_t k = 0; k < C * E; k++) o[k] = (T)0;
+        return;
+    }
+    if (nearest) {
+        const int z = (int)nearbyint((double)cz), y = (int)nearbyint((double)cy), x = (int)nearbyint((double)cx);
+        const int64_t vi = ((int64_t)z * H + y) * W + x;
+        for (int64_t ch = 0; ch < C; ch++)
+#pragma unroll
+            for (int e = 0; e < E; e++) o[ch * E + e] = img[(ch * plane + vi) * E + e];
+        return;
+    }
+    const T fz = floor(cz), fy = floor(cy), fx = floor(cx);
+    const int z0 = (int)fz, y0 = (int)fy, x0 = (int)fx;
+    const T az[2] = {(fz + (T)1) - cz, cz - fz};
+    const T ay[2] = {(fy + (T)1) - cy, cy - fy};
+    const T ax[2] = {(fx + (T)1) - cx, cx - fx};
+    for (int64_t ch = 0; ch < C; ch++) {
+        T acc[E];
+#pragma unroll
+        for (int e = 0; e < E; e++) acc[e] = (T)0;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int bz = (k >> 2) & 1, by = (k >> 1) & 1, bx = k & 1;
+            const int z = z0 + bz, y = y0 + by, x = x0 + bx;
+            if (z >= D || y >= H || x >= W) continue;
+            const T wgt = ax[bx] * ay[by] * az[bz];
+            const int64_t vi = ch * plane + ((int64_t)z * H + y) * W + x;
+#pragma unroll
+            for (int e = 0; e < E; e++) acc[e] += img[vi * E + e] * wgt;
+        }
+#pragma unroll
+        for (int e = 0; e < E; e++) o[ch * E + e] = acc[e];
+    }
+}
+
+template <typename T, int E, typename WT>
+__global__ void insert3d_kernel(const T* __restrict__ vals, const float* __restrict__ coords, int64_t n,
+                                T* __restrict__ img, int64_t C, int D, int H, int W, WT* __restrict__ wts,
+                                int nearest) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float cz = coords[i * 3 + 0], cy = coords[i * 3 + 1], cx = coords[i * 3 + 2];
+    if (!(cz >= 0.0f && cz <= (float)D - 1.0f && cy >= 0.0f && cy <= (float)H - 1.0f && cx >= 0.0f &&
+          cx <= (float)W - 1.0f))
+        return;
+    const int64_t plane = (int64_t)D * H * W;
+    const T* v = vals + i * C * E;
+    if (nearest) {
+        const int64_t vi = ((int64_t)rintf(cz) * H + (int64_t)rintf(cy)) * W + (int64_t)rintf(cx);
+        for (int64_t ch = 0; ch < C; ch++)
+#pragma unroll
+            for (int e = 0; e < E; e++) atomic_add_real(img + (ch * plane + vi) * E + e, v[ch * E + e]);
+        atomic_add_real(wts + vi, (WT)1);
+        return;
+    }
+    const float z0 = floorf(cz), y0 = floorf(cy), x0 = floorf(cx);
+    const int iz[2] = {(int)z0, (int)ceilf(cz)}, iy[2] = {(int)y0, (int)ceilf(cy)}, ix[2] = {(int)x0, (int)ceilf(cx)};
+    const float tz = cz - z0, ty = cy - y0, tx = cx - x0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int bz = (k >> 2) & 1, by = (k >> 1) & 1, bx = k & 1;
+        const float w = ((bz ? tz : 1.0f - tz) * (by ? ty : 1.0f - ty)) * (bx ? tx : 1.0f - tx);
+        if (w == 0.0f) continue;
+        const int64_t vi = ((int64_t)iz[bz] * H + iy[by]) * W + ix[bx];
+        const WT ww = (WT)w;
+        const T wv = (T)ww;
+        for (int64_t ch = 0; ch < C; ch++)
+#pragma unroll
+            for (int e = 0; e < E; e++) atomic_add_real(img + (ch * plane + vi) * E + e, v[ch * E + e] * wv);
+        atomic_add_real(wts + vi, ww);
+    }
+}
+
+inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace tt
+
+using namespace tt;
+
+extern "C" int tt_sample_image_3d(const void* image, int32_t dtype, int64_t channels, int64_t d, int64_t h,
+                                  int64_t w, const void* coordinates, int64_t n, void* out, int32_t nearest,
+                                  void* stream) {
+    if (n == 0) return TT_OK;
+    if (!image || !coordinates || !out || channels < 1 || d < 1 || h < 1 || w < 1 || n < 0)
+        return fail(TT_ERR_INVALID, "sample_image_3d: bad arguments");
+    cudaStream_t st = as_stream(stream);
+    const unsigned b = nblocks(n, 256);
+    switch (dtype) {
+        case 0:
+            sample3d_kernel<float, 1><<<b, 256, 0, st>>>((const float*)image, channels, (int)d, (int)h, (int)w,
+                                                          (const float*)coordinates, n, (float*)out, nearest);
+            break;
+        case 1:
+            sample3d_kernel<double, 1><<<b, 256, 0, st>>>((const double*)image, channels, (int)d, (int)h, (int)w,
+                                                           (const double*)coordinates, n, (double*)out, nearest);
+            break;
+        case 2:
+            sample3d_kernel<float, 2><<<b, 256, 0, st>>>((const float*)image, channels, (int)d, (int)h, (int)w,
+                                                          (const float*)coordinates, n, (float*)out, nearest);
+            break;
+        case 3:
+            sample3d_kernel<double, 2><<<b, 256, 0, st>>>((const double*)image, channels, (int)d, (int)h, (int)w,
+                                                           (const double*)coordinates, n, (double*)out, nearest);
+            break;
+        default:
+            return fail(TT_ERR_INVALID, "sample_image_3d: unknown dtype code %d", dtype);
+    }
+    return check_launch("sample3d_kernel");
+}
+
+extern "C" int tt_insert_into_image_3d(const void* values, int32_t dtype, const float* coordinates, int64_t n,
+                                       void* image, int64_t channels, int64_t d, int64_t h, int64_t w,
+                                       void* weights, int32_t weights_f64, int32_t nearest, void* stream) {
+    if (n == 0) return TT_OK;
+    if (!values || !coordinates || !image || !weights || channels < 1 || d < 1 || h < 1 || w < 1 || n < 0)
+        return fail(TT_ERR_INVALID, "insert_into_image_3d: bad arguments");
+    cudaStream_t st = as_stream(stream);
+    const unsigned b = nblocks(n, 256);
+#define TT_INSERT_CASE(T, E)                                                                                  \
+    if (weights_f64)                                                                                          \
+        insert3d_kernel<T, E, double><<<b, 256, 0, st>>>((const T*)values, coordinates, n, (T*)image, channels, \
+                                                         (int)d, (int)h, (int)w, (double*)weights, nearest);  \
+    else                                                                                                      \
+        insert3d_kernel<T, E, float><<<b, 256, 0, st>>>((const T*)values, coordinates, n, (T*)image, channels,  \
+                                                        (int)d, (int)h, (int)w, (float*)weights, nearest);
+    switch (dtype) {
+        case 0: TT_INSERT_CASE(float, 1) break;
+        case 1: TT_INSERT_CASE(double, 1) break;
+        case 2: TT_INSERT_CASE(float, 2) break;
+        case 3: TT_INSERT_CASE(double, 2) break;
+        default:
+            return fail(TT_ERR_INVALID, "insert_into_image_3d: unknown dtype code %d", dtype);
+    }
+#undef TT_INSERT_CASE
+    return check_launch("insert3d_kernel");
+}

@@ -1,0 +1,217 @@
+// Elementwise kernels around the FFTs of the real-space wrappers
+// project_3d_to_2d (torch_fourier_slice/project.py:48-92) and
+// backproject_2d_to_3d (torch_fourier_slice/backproject.py:48-92).
+// Each replaces a chain of pad / multiply / fftshift / divide / crop passes by
+// one read and one write, folding every shift into the index arithmetic.
+//
+// Shift conventions (torch.fft): fftshift(x)[i] = x[(i - n/2) mod n],
+// ifftshift(x)[i] = x[(i + n/2) mod n], n/2 rounded down.
+#include <cuda_runtime.h>
+
+#include "capi_util.cuh"
+
+namespace tt {
+
+__device__ __forceinline__ int64_t wrap(int64_t i, int64_t n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// f32(k) * f32(1/n) for unshifted index k of an axis of length n.
+__device__ __forceinline__ float fftfreq_at(int64_t k, int64_t n, float inv_n) {
+    int64_t kk = (k < (n + 1) / 2) ? k : k - n;
+    return __fmul_rn((float)kk, inv_n);
+}
+
+// sinc(|f|)^2 at position a of the fftshifted norm grid of an n^3 array
+// (fftfreq_grid(rfft=False, fftshift=True, norm=True)).
+__device__ __forceinline__ float sinc2_at(int64_t a0, int64_t a1, int64_t a2, int64_t n, float inv_n) {
+    const float f0 = fftfreq_at(wrap(a0 - n / 2, n), n, inv_n);
+    const float f1 = fftfreq_at(wrap(a1 - n / 2, n), n, inv_n);
+    const float f2 = fftfreq_at(wrap(a2 - n / 2, n), n, inv_n);
+    const float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(f0, f0), __fmul_rn(f1, f1)), __fmul_rn(f2, f2)));
+    if (r == 0.0f) return 1.0f;
+    const float px = __fmul_rn(3.14159265358979323846f, r);
+    const float s = __fdiv_rn(sinpif(r), px);
+    return s * s;
+}
+
+// out (n^3, FFT order) = fftshift(pad(vol, p) * sinc^2)
+template <typename T>
+__global__ void project_prepare_kernel(const T* __restrict__ vol, T* __restrict__ out, int64_t d, int64_t p,
+                                       int64_t n, float inv_n) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * n * n) return;
+    const int64_t i = idx / (n * n), j = (idx / n) % n, k = idx % n;
+    const int64_t a0 = wrap(i - n / 2, n), a1 = wrap(j - n / 2, n), a2 = wrap(k - n / 2, n);
+    const int64_t v0 = a0 - p, v1 = a1 - p, v2 = a2 - p;
+    T v = 0;
+    if (v0 >= 0 && v0 < d && v1 >= 0 && v1 < d && v2 >= 0 && v2 < d)
+        v = vol[(v0 * d + v1) * d + v2] * (T)sinc2_at(a0, a1, a2, n, inv_n);
+    out[idx] = v;
+}
+
+// out (m, n-2p, n-2p) = crop(ifftshift(images, (-2,-1)), p)
+template <typename T>
+__global__ void recentre_crop_2d_kernel(const T* __restrict__ img, T* __restrict__ out, int64_t m, int64_t n,
+                                        int64_t p) {
+    const int64_t c = n - 2 * p;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= m * c * c) return;
+    const int64_t b = idx / (c * c), i = (idx / c) % c, j = idx % c;
+    const int64_t si = wrap(i + p + n / 2, n), sj = wrap(j + p + n / 2, n);
+    out[idx] = img[(b * n + si) * n + sj];
+}
+
+// out (m, n, n) = fftshift(pad(images, p), (-2,-1)), images (m, d, d)
+template <typename T>
+__global__ void pad_fftshift_2d_kernel(const T* __restrict__ img, T* __restrict__ out, int64_t m, int64_t d,
+                                       int64_t p, int64_t n) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= m * n * n) return;
+    const int64_t b = idx / (n * n), i = (idx / n) % n, j = idx % n;
+    const int64_t a0 = wrap(i - n / 2, n) - p, a1 = wrap(j - n / 2, n) - p;
+    T v = 0;
+    if (a0 >= 0 && a0 < d && a1 >= 0 && a1 < d) v = img[(b * d + a0) * d + a1];
+    out[idx] = v;
+}
+
+template <typename R>
+struct C2;
+template <>
+struct C2<float> {
+    using T = float2;
+};
+template <>
+struct C2<double> {
+    using T = double2;
+};
+
+// Backprojection normalisation of `channels` accumulated (pre-mirror)
+// fftshifted rfft volumes (d, h, w) sharing one weight volume:
+// Friedel completion of the x=0 plane, division by max(weights, 1), written
+// ifftshifted along (d, h) for the 3D irfft.
+template <typename R>
+__global__ void normalize_unshift_kernel(const typename C2<R>::T* __restrict__ acc, const R* __restrict__ wts,
+                                         typename C2<R>::T* __restrict__ out, int64_t channels, int64_t d,
+                                         int64_t h, int64_t w) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t per = d * h * w;
+    if (idx >= channels * per) return;
+    const int64_t ch = idx / per, r = idx % per;
+    const int64_t i = r / (h * w), j = (r / w) % h, k = r % w;
+    const int64_t z = wrap(i + d / 2, d), y = wrap(j + h / 2, h);  // source (shifted) voxel
+    const int64_t src = (z * h + y) * w + k;
+    typename C2<R>::T v = acc[ch * per + src];
+    R wt = wts[src];
+    if (k == 0) {
+        const int64_t zm = (d - z) % d, ym = (h - y) % h;
+        const bool m_dc = (zm == d / 2) && (ym == h / 2);
+        if (!m_dc) {
+            const int64_t ms = (zm * h + ym) * w;
+            const typename C2<R>::T u = acc[ch * per + ms];
+            v.x += u.x;
+            v.y -= u.y;
+            wt += wts[ms];
+        }
+    }
+    const R den = wt < (R)1 ? (R)1 : wt;
+    v.x /= den;
+    v.y /= den;
+    out[idx] = v;
+}
+
+// out (c^3) = crop(ifftshift(vol) / sinc^2, p), vol (n^3) real
+template <typename T>
+__global__ void backproject_finish_kernel(const T* __restrict__ vol, T* __restrict__ out, int64_t n, int64_t p,
+                                          float inv_n) {
+    const int64_t c = n - 2 * p;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= c * c * c) return;
+    const int64_t i = idx / (c * c) + p, j = (idx / c) % c + p, k = idx % c + p;
+    const int64_t s = (wrap(i + n / 2, n) * n + wrap(j + n / 2, n)) * n + wrap(k + n / 2, n);
+    out[idx] = vol[s] / (T)sinc2_at(i, j, k, n, inv_n);
+}
+
+inline unsigned blocks_for(int64_t total, int threads) { return (unsigned)((total + threads - 1) / threads); }
+
+}  // namespace tt
+
+using namespace tt;
+
+extern "C" int tt_project_prepare(const void* volume, int32_t is_f64, int64_t d, int64_t pad, void* out,
+                                  void* stream) {
+    if (!volume || !out || d < 1 || pad < 0) return fail(TT_ERR_INVALID, "project_prepare: bad arguments");
+    const int64_t n = d + 2 * pad, total = n * n * n;
+    const float inv_n = (float)(1.0 / (double)n);
+    if (is_f64)
+        project_prepare_kernel<double><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
+            (const double*)volume, (double*)out, d, pad, n, inv_n);
+    else
+        project_prepare_kernel<float><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
+            (const float*)volume, (float*)out, d, pad, n, inv_n);
+    return check_launch("project_prepare_kernel");
+}
+
+extern "C" int tt_recentre_crop_2d(const void* images, int32_t is_f64, int64_t m, int64_t n, int64_t pad, void* out,
+                                   void* stream) {
+    if (!images || !out || m < 0 || n < 1 || pad < 0 || 2 * pad >= n)
+        return fail(TT_ERR_INVALID, "recentre_crop_2d: bad arguments");
+    if (m == 0) return TT_OK;
+    const int64_t c = n - 2 * pad, total = m * c * c;
+    if (is_f64)
+        recentre_crop_2d_kernel<double><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
+            (const double*)images, (double*)out, m, n, pad);
+    else
+        recentre_crop_2d_kernel<float><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
+            (const float*)images, (float*)out, m, n, pad);
+    return check_launch("recentre_crop_2d_kernel");
+}
+
+extern "C" int tt_pad_fftshift_2d(const void* images, int32_t is_f64, int64_t m, int64_t d, int64_t pad, void* out,
+                                  void* stream) {
+    if (!images || !out || m < 0 || d < 1 || pad < 0) return fail(TT_ERR_INVALID, "pad_fftshift_2d: bad arguments");
+    if (m == 0) return TT_OK;
+    const int64_t n = d + 2 * pad, total = m * n * n;
+    if (is_f64)
+        pad_fftshift_2d_kernel<double><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
+            (const double*)images, (double*)out, m, d, pad, n);
+    else
+        pad_fftshift_2d_kernel<float><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
+            (const float*)images, (float*)out, m, d, pad, n);
+    return check_launch("pad_fftshift_2d_kernel");
+}
+
+extern "C" int tt_backproject_normalize(const void* volume_acc, const void* weights, int32_t complex128,
+                                        int64_t channels, int64_t d, int64_t h, int64_t w_rfft, void* out,
+                                        void* stream) {
+    if (!volume_acc || !weights || !out || channels < 1 || d < 1 || h < 1 || w_rfft < 1)
+        return fail(TT_ERR_INVALID, "backproject_normalize: bad arguments");
+    if (volume_acc == out) return fail(TT_ERR_INVALID, "backproject_normalize: out must not alias the input");
+    const int64_t total = channels * d * h * w_rfft;
+    if (complex128)
+        normalize_unshift_kernel<double><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
+            (const double2*)volume_acc, (const double*)weights, (double2*)out, channels, d, h, w_rfft);
+    else
+        normalize_unshift_kernel<float><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
+            (const float2*)volume_acc, (const float*)weights, (float2*)out, channels, d, h, w_rfft);
+    return check_launch("normalize_unshift_kernel");
+}
+
+extern "C" int tt_backproject_finish(const void* volume, int32_t is_f64, int64_t channels, int64_t n, int64_t pad,
+                                     void* out, void* stream) {
+    if (!volume || !out || channels < 1 || n < 1 || pad < 0 || 2 * pad >= n)
+        return fail(TT_ERR_INVALID, "backproject_finish: bad arguments");
+    const int64_t c = n - 2 * pad, per = c * c * c;
+    const float inv_n = (float)(1.0 / (double)n);
+    for (int64_t ch = 0; ch < channels; ch++) {
+        if (is_f64)
+            backproject_finish_kernel<double><<<blocks_for(per, 256), 256, 0, as_stream(stream)>>>(
+                (const double*)volume + ch * n * n * n, (double*)out + ch * per, n, pad, inv_n);
+        else
+            backproject_finish_kernel<float><<<blocks_for(per, 256), 256, 0, as_stream(stream)>>>(
+                (const float*)volume + ch * n * n * n, (float*)out + ch * per, n, pad, inv_n);
+        if (int e = check_launch("backproject_finish_kernel")) return e;
+    }
+    return TT_OK;
+}

@@ -1,0 +1,123 @@
+"""Host side of the elementwise passes around the FFTs of project / backproject.
+
+Each forward runs one fused CUDA kernel (see ``csrc/wrappers.cu``).  The
+projection passes are differentiable; their backward passes are the exact
+adjoints (a permutation, a crop or zero-pad and a fixed sinc^2 weight),
+written with torch ops because they are off the hot path.
+"""
+
+from __future__ import annotations
+
+import torch
+import torch.nn.functional as F
+
+from .. import _lib
+
+
+def _is_f64(t: torch.Tensor) -> int:
+    return int(t.dtype == torch.float64)
+
+
+def sinc2_grid(n: int, device, dtype=torch.float32) -> torch.Tensor:
+    """sinc(|f|)^2 on the fftshifted n^3 frequency grid."""
+    k = torch.arange(n, device=device)
+    f = torch.where(k < (n + 1) // 2, k, k - n).to(torch.float32) * torch.tensor(
+        1.0 / n, dtype=torch.float32)
+    f = torch.fft.fftshift(f)
+    r = torch.sqrt(f[:, None, None] ** 2 + f[None, :, None] ** 2 + f[None, None, :] ** 2)
+    return (torch.sinc(r) ** 2).to(dtype)
+
+
+class _ProjectPrepare(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, volume, pad):
+        d = volume.shape[-1]
+        n = d + 2 * pad
+        out = torch.empty((n, n, n), dtype=volume.dtype, device=volume.device)
+        L = _lib.load()
+        _lib.check(L.tt_project_prepare(_lib.ptr(volume), _is_f64(volume), d, pad, _lib.ptr(out),
+                                        _lib.stream_of(volume.device)), "project_prepare")
+        ctx.pad = pad
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        p = ctx.pad
+        n = g.shape[-1]
+        g = torch.fft.ifftshift(g, dim=(-3, -2, -1)) * sinc2_grid(n, g.device, g.dtype)
+        if p:
+            g = g[p:-p, p:-p, p:-p]
+        return g, None
+
+
+class _RecentreCrop2d(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, images, pad):
+        m, n = images.shape[0], images.shape[-1]
+        c = n - 2 * pad
+        out = torch.empty((m, c, c), dtype=images.dtype, device=images.device)
+        L = _lib.load()
+        _lib.check(L.tt_recentre_crop_2d(_lib.ptr(images), _is_f64(images), m, n, pad,
+                                         _lib.ptr(out), _lib.stream_of(images.device)),
+                   "recentre_crop_2d")
+        ctx.pad = pad
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        p = ctx.pad
+        if p:
+            g = F.pad(g, [p] * 4)
+        return torch.fft.fftshift(g, dim=(-2, -1)), None
+
+
+def project_prepare(volume: torch.Tensor, pad: int) -> torch.Tensor:
+    _lib.require_cuda(volume)
+    if volume.dtype not in (torch.float32, torch.float64):
+        volume = volume.to(torch.float32)
+    return _ProjectPrepare.apply(volume.contiguous(), int(pad))
+
+
+def recentre_crop_2d(images: torch.Tensor, pad: int) -> torch.Tensor:
+    n = images.shape[-1]
+    flat = images.reshape(-1, n, n).contiguous()
+    return _RecentreCrop2d.apply(flat, int(pad))
+
+
+def pad_fftshift_2d(images: torch.Tensor, pad: int) -> torch.Tensor:
+    """(m, d, d) real -> fftshift(pad(images)) (m, n, n)."""
+    m, d = images.shape[0], images.shape[-1]
+    n = d + 2 * pad
+    out = torch.empty((m, n, n), dtype=images.dtype, device=images.device)
+    L = _lib.load()
+    _lib.check(L.tt_pad_fftshift_2d(_lib.ptr(images), _is_f64(images), m, d, pad, _lib.ptr(out),
+                                    _lib.stream_of(images.device)), "pad_fftshift_2d")
+    return out
+
+
+def backproject_normalize(volume_acc: torch.Tensor, weights: torch.Tensor) -> torch.Tensor:
+    """Mirror + divide by max(w, 1) + ifftshift(d, h) of (c?, d, h, w) volumes."""
+    d, h, w = volume_acc.shape[-3:]
+    channels = volume_acc.numel() // (d * h * w)
+    out = torch.empty_like(volume_acc)
+    L = _lib.load()
+    _lib.check(L.tt_backproject_normalize(_lib.ptr(volume_acc), _lib.ptr(weights),
+                                          int(volume_acc.dtype == torch.complex128), channels,
+                                          d, h, w, _lib.ptr(out),
+                                          _lib.stream_of(volume_acc.device)),
+               "backproject_normalize")
+    return out
+
+
+def backproject_finish(volume: torch.Tensor, pad: int) -> torch.Tensor:
+    """(c?, n, n, n) irfft output -> crop(ifftshift(v) / sinc^2)."""
+    n = volume.shape[-1]
+    lead = volume.shape[:-3]
+    channels = volume.numel() // (n ** 3)
+    c = n - 2 * pad
+    out = torch.empty((*lead, c, c, c), dtype=volume.dtype, device=volume.device)
+    L = _lib.load()
+    _lib.check(L.tt_backproject_finish(_lib.ptr(volume), _is_f64(volume), channels, n, pad,
+                                       _lib.ptr(out), _lib.stream_of(volume.device)),
+               "backproject_finish")
+    return out

@@ -1,0 +1,158 @@
+"""Central-slice extraction (drop-in for torch_fourier_slice.slice_extraction).
+
+``extract_central_slices_rfft_3d`` keeps the reference signature, defaults and
+semantics (torch_fourier_slice/slice_extraction/_extract_central_slices_rfft_3d.py:84-222)
+and runs on the sm_100a gather kernel.  It is differentiable w.r.t. the volume
+and the rotation matrices through one fused backward kernel; interpolation
+weights are recomputed in the backward pass, not stored.
+
+Deliberate difference: the reference zeroes near-zero rotation elements IN
+PLACE on the caller's float32 tensor (:147-151), which also raises for a leaf
+that requires grad.  Here the caller's tensor is never modified; the zeroing
+is applied to a private copy inside the kernel and the zeroed elements get a
+zero gradient, as in the reference.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from .. import _lib
+from ._params import rotation_arg, slice_params
+
+
+class _ExtractCentralSlices(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, volume_rfft, rotation_matrices, params, out_shape):
+        dev = volume_rfft.device
+        out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
+        L = _lib.load()
+        _lib.check(
+            L.tt_extract_central_slices_rfft_3d(_lib.ptr(volume_rfft), _lib.ptr(rotation_matrices),
+                                                _lib.ptr(out), params, _lib.stream_of(dev)),
+            "extract_central_slices_rfft_3d",
+        )
+        ctx.params = params
+        ctx.save_for_backward(volume_rfft, rotation_matrices)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        volume_rfft, rotation_matrices = ctx.saved_tensors
+        want_v, want_r = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        dvol = drot = None
+        if want_v or want_r:
+            dvol, drot = extract_backward(volume_rfft, rotation_matrices, grad, ctx.params,
+                                          want_v, want_r)
+        return dvol, drot, None, None
+
+
+def extract_backward(volume_rfft, rotation_matrices, grad, params, want_volume=True,
+                     want_rotation=True):
+    """Fused backward: (d/dvolume, d/drotation) for upstream slice gradient ``grad``."""
+    dev = volume_rfft.device
+    grad = grad.to(torch.complex64).contiguous()
+    L = _lib.load()
+    dvol = torch.zeros_like(volume_rfft) if want_volume else None
+    drot = torch.empty_like(rotation_matrices) if want_rotation else None
+    ws = None
+    nbytes = 0
+    if want_rotation:
+        nbytes = int(L.tt_extract_backward_workspace_bytes(params))
+        ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
+    _lib.check(
+        L.tt_extract_central_slices_rfft_3d_backward(
+            _lib.ptr(volume_rfft), _lib.ptr(rotation_matrices), _lib.ptr(grad), _lib.ptr(dvol),
+            _lib.ptr(drot), _lib.ptr(ws), nbytes, params, _lib.stream_of(dev)),
+        "extract_central_slices_rfft_3d backward",
+    )
+    return dvol, drot
+
+
+def extract_central_slices_rfft_3d(
+    volume_rfft: torch.Tensor,
+    image_shape: tuple[int, int, int],
+    rotation_matrices: torch.Tensor,  # (..., 3, 3)
+    fftfreq_max: float | None = None,
+    zyx_matrices: bool = False,
+    x_tolerance: float = 1e-8,
+    rot_tolerance: float | None = 1e-8,
+) -> torch.Tensor:
+    """Extract central slices from an fftshifted rfft volume.
+
+    Parameters and return value as in the reference: ``volume_rfft`` is
+    ``(d, d, d//2+1)`` complex64 (fftshifted in the first two dims),
+    ``image_shape`` the real-space shape defining the slice grid,
+    ``rotation_matrices`` ``(..., 3, 3)``; returns ``(..., h, w//2+1)``
+    complex64 slices (zero outside ``fftfreq_max``).
+    """
+    assert volume_rfft.ndim == 3, "Input volume_rfft must be 3D tensor."
+    _lib.require_cuda(volume_rfft)
+    if volume_rfft.dtype != torch.complex64:
+        raise RuntimeError(
+            f"extract_central_slices_rfft_3d supports complex64 volumes (got {volume_rfft.dtype})"
+        )
+    volume_rfft = volume_rfft.contiguous()
+    R, stack = rotation_arg(rotation_matrices, volume_rfft.device)
+    h, w = int(image_shape[-2]), int(image_shape[-1])
+    params = slice_params(n=R.shape[0], image_shape=image_shape, volume=volume_rfft,
+                          rotation=R, fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                          x_tolerance=x_tolerance, rot_tolerance=rot_tolerance)
+    out = _ExtractCentralSlices.apply(volume_rfft, R, params, (R.shape[0], h, w // 2 + 1))
+    return out.reshape(*stack, h, w // 2 + 1)
+
+
+def central_slice_geometry(
+    rotation_matrices: torch.Tensor,
+    image_shape: tuple[int, int, int],
+    volume_dims: tuple[int, int, int],
+    mode: str = "extract",
+    fftfreq_max: float | None = None,
+    zyx_matrices: bool = False,
+    x_tolerance: float = 1e-8,
+    rot_tolerance: float | None = 1e-8,
+) -> tuple[torch.Tensor, torch.Tensor]:
+    """Per-pixel geometry of the slice grid, computed by the CUDA kernels.
+
+    Returns ``(flags, coords)``: flags (n, h, w//2+1) uint8 with bit0 = pixel
+    kept, bit1 = conjugate redirect, bit2 = inside the volume; coords
+    (n, h, w//2+1, 3) float32 redirected zyx array coordinates.  ``mode`` is
+    'extract' (tolerance rules of the extraction) or 'insert' (strict x<0 rule,
+    Friedel-redundant source pixels dropped, no rot_tolerance)."""
+    R, _ = rotation_arg(rotation_matrices, rotation_matrices.device)
+    _lib.require_cuda(R)
+    h, w = int(image_shape[-2]), int(image_shape[-1])
+    n = R.shape[0]
+    params = slice_params(n=n, image_shape=image_shape, volume=None, rotation=R,
+                          fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                          x_tolerance=x_tolerance, rot_tolerance=rot_tolerance,
+                          vol_dims=tuple(int(v) for v in volume_dims))
+    flags = torch.empty((n, h, w // 2 + 1), dtype=torch.uint8, device=R.device)
+    coords = torch.empty((n, h, w // 2 + 1, 3), dtype=torch.float32, device=R.device)
+    L = _lib.load()
+    _lib.check(L.tt_slice_geometry(_lib.ptr(R), 0 if mode == "extract" else 1, _lib.ptr(flags),
+                                   _lib.ptr(coords), params, _lib.stream_of(R.device)),
+               "central_slice_geometry")
+    return flags, coords
+
+
+def extract_central_slices_rfft_3d_multichannel(
+    volume_rfft: torch.Tensor,  # (c, d, d, d)
+    image_shape: tuple[int, int, int],
+    rotation_matrices: torch.Tensor,  # (..., 3, 3)
+    fftfreq_max: float | None = None,
+    zyx_matrices: bool = False,
+    x_tolerance: float = 1e-8,
+    rot_tolerance: float | None = 1e-8,
+) -> torch.Tensor:  # (..., c, h, w)
+    """Multichannel extraction (_extract_central_slices_rfft_3d.py:225-367):
+    ``(c, d, d, d//2+1)`` -> ``(..., c, h, w//2+1)``, the same rotations for
+    every channel."""
+    assert volume_rfft.ndim == 4, "Input volume_rfft must be 4D tensor."
+    slices = [
+        extract_central_slices_rfft_3d(volume_rfft[c], image_shape, rotation_matrices,
+                                       fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                                       x_tolerance=x_tolerance, rot_tolerance=rot_tolerance)
+        for c in range(volume_rfft.shape[0])
+    ]
+    return torch.stack(slices, dim=-3)

@@ -1,0 +1,117 @@
+"""Central-slice insertion (drop-in for torch_fourier_slice.slice_insertion).
+
+``insert_central_slices_rfft_3d`` keeps the reference signature and returns
+``(volume, weights)`` like
+torch_fourier_slice/slice_insertion/_insert_central_slices_rfft_3d.py:9-106:
+complex64 slices give a complex64 volume with float32 weights, complex128
+slices a complex128 volume with float64 weights.  The splat runs on the
+sm_100a scatter kernel; the Friedel completion of the x=0 plane is one
+post-pass over that plane.
+"""
+
+from __future__ import annotations
+
+import math
+
+import torch
+
+from .. import _lib
+from ._params import rfft_shape, rotation_arg, slice_params
+
+
+def _check_image(image_rfft: torch.Tensor, volume_shape):
+    if image_rfft.dtype not in (torch.complex64, torch.complex128):
+        raise ValueError(f"image_rfft must be complex64 or complex128, got {image_rfft.dtype}")
+    h, w = int(volume_shape[-2]), int(volume_shape[-1])
+    if tuple(image_rfft.shape[-2:]) != (h, w // 2 + 1):
+        raise ValueError(
+            f"image_rfft has rfft shape {tuple(image_rfft.shape[-2:])}, expected {(h, w // 2 + 1)} "
+            f"for volume_shape {tuple(volume_shape)}"
+        )
+
+
+def insert_splat(image_rfft, R, volume_shape, volume, weights, fftfreq_max=None,
+                 zyx_matrices=False, images_unshifted=False):
+    """Accumulate the trilinear splat of (n, h, w//2+1) slices into ``volume``
+    / ``weights`` (no Friedel completion)."""
+    dev = volume.device
+    params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=volume, rotation=R,
+                          fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                          slices_unshifted=images_unshifted)
+    L = _lib.load()
+    _lib.check(
+        L.tt_insert_central_slices_rfft_3d(_lib.ptr(image_rfft),
+                                           int(image_rfft.dtype == torch.complex128),
+                                           _lib.ptr(R), _lib.ptr(volume), _lib.ptr(weights),
+                                           params, _lib.stream_of(dev)),
+        "insert_central_slices_rfft_3d",
+    )
+
+
+def friedel_mirror_x0(volume, weights):
+    """In-place Friedel completion of the x=0 plane of (c?, d, h, w) volumes."""
+    dev = volume.device
+    d, h, w = volume.shape[-3:]
+    channels = volume.numel() // (d * h * w)
+    L = _lib.load()
+    _lib.check(
+        L.tt_friedel_mirror_x0(_lib.ptr(volume), _lib.ptr(weights),
+                               int(volume.dtype == torch.complex128), channels, d, h, w,
+                               _lib.stream_of(dev)),
+        "friedel_mirror_x0",
+    )
+
+
+def insert_central_slices_rfft_3d(
+    image_rfft: torch.Tensor,  # fftshifted rfft of (..., h, w) 2d image
+    volume_shape: tuple[int, int, int],
+    rotation_matrices: torch.Tensor,
+    fftfreq_max: float | None = None,
+    zyx_matrices: bool = False,
+) -> tuple[torch.Tensor, torch.Tensor]:
+    _lib.require_cuda(image_rfft)
+    _check_image(image_rfft, volume_shape)
+    dev = image_rfft.device
+    R, stack = rotation_arg(rotation_matrices, dev)
+    n = R.shape[0]
+    lead = image_rfft.shape[:-2]
+    if math.prod(lead) != n:
+        raise ValueError(
+            f"{n} rotation matrices for image stack of shape {tuple(lead)}")
+    img = image_rfft.reshape(n, *image_rfft.shape[-2:]).contiguous()
+    shape3 = rfft_shape(volume_shape)
+    volume = torch.zeros(shape3, dtype=image_rfft.dtype, device=dev)
+    wdt = torch.float64 if image_rfft.dtype == torch.complex128 else torch.float32
+    weights = torch.zeros(shape3, dtype=wdt, device=dev)
+    insert_splat(img, R, volume_shape, volume, weights, fftfreq_max, zyx_matrices)
+    friedel_mirror_x0(volume, weights)
+    return volume, weights
+
+
+def insert_central_slices_rfft_3d_multichannel(
+    image_rfft: torch.Tensor,  # fftshifted rfft of (..., c, h, w) 2d images
+    volume_shape: tuple[int, int, int],
+    rotation_matrices: torch.Tensor,  # (..., 3, 3)
+    fftfreq_max: float | None = None,
+    zyx_matrices: bool = False,
+) -> tuple[torch.Tensor, torch.Tensor]:
+    """Multichannel insertion (_insert_central_slices_rfft_3d.py:109-210):
+    returns ``(c, d, h, w//2+1)`` volumes and ONE ``(d, h, w//2+1)`` weight
+    volume shared by the channels."""
+    _lib.require_cuda(image_rfft)
+    _check_image(image_rfft, volume_shape)
+    dev = image_rfft.device
+    c = image_rfft.shape[-3]
+    R, stack = rotation_arg(rotation_matrices, dev)
+    shape3 = rfft_shape(volume_shape)
+    volume = torch.zeros((c, *shape3), dtype=image_rfft.dtype, device=dev)
+    wdt = torch.float64 if image_rfft.dtype == torch.complex128 else torch.float32
+    weights = torch.zeros(shape3, dtype=wdt, device=dev)
+    scratch_w = torch.zeros(shape3, dtype=wdt, device=dev)
+    n = R.shape[0]
+    for ch in range(c):
+        img = image_rfft[..., ch, :, :].reshape(n, *image_rfft.shape[-2:]).contiguous()
+        insert_splat(img, R, volume_shape, volume[ch], weights if ch == 0 else scratch_w,
+                     fftfreq_max, zyx_matrices)
+    friedel_mirror_x0(volume, weights)
+    return volume, weights

@@ -1,0 +1,106 @@
+"""3D interpolation primitives (drop-in for torch_image_interpolation's 3D API).
+
+``sample_image_3d`` and ``insert_into_image_3d`` keep the reference
+signatures and semantics (torch_image_interpolation/image_interpolation_3d.py:11-101
+and :104-275) and run on sm_100a gather / scatter kernels.
+"""
+
+from __future__ import annotations
+
+from typing import Literal
+
+import torch
+
+from .. import _lib
+
+_DTYPE_CODES = {torch.float32: 0, torch.float64: 1, torch.complex64: 2, torch.complex128: 3}
+_REAL = {torch.float32: torch.float32, torch.float64: torch.float64,
+         torch.complex64: torch.float32, torch.complex128: torch.float64}
+
+
+def _code(dtype: torch.dtype) -> int:
+    if dtype not in _DTYPE_CODES:
+        raise ValueError(f"unsupported dtype {dtype}; expected float32/64 or complex64/128")
+    return _DTYPE_CODES[dtype]
+
+
+def sample_image_3d(
+    image: torch.Tensor,
+    coordinates: torch.Tensor,
+    interpolation: Literal["nearest", "trilinear"] = "trilinear",
+) -> torch.Tensor:
+    """Sample a (d, h, w) or (c, d, h, w) image at (..., 3) zyx array coordinates.
+
+    Returns (...) or (..., c) samples; zero where a coordinate is outside
+    [0, N-1]."""
+    if image.ndim not in (3, 4):
+        raise ValueError(f"image should have shape (d, h, w) or (c, d, h, w), got {image.shape}")
+    if interpolation not in ("nearest", "trilinear"):
+        raise ValueError(f"interpolation must be 'nearest' or 'trilinear', got {interpolation!r}")
+    _lib.require_cuda(image)
+    code = _code(image.dtype)
+    multi = image.ndim == 4
+    img = (image if multi else image[None]).contiguous()
+    C, D, H, W = img.shape
+    coords = torch.as_tensor(coordinates).to(image.device)
+    batch = coords.shape[:-1]
+    c = coords.reshape(-1, 3).to(_REAL[image.dtype]).contiguous()
+    n = c.shape[0]
+    out = torch.empty((n, C), dtype=image.dtype, device=image.device)
+    L = _lib.load()
+    _lib.check(L.tt_sample_image_3d(_lib.ptr(img), code, C, D, H, W, _lib.ptr(c), n,
+                                    _lib.ptr(out), int(interpolation == "nearest"),
+                                    _lib.stream_of(image.device)), "sample_image_3d")
+    out = out.reshape(*batch, C)
+    return out if multi else out[..., 0]
+
+
+def insert_into_image_3d(
+    values: torch.Tensor,
+    coordinates: torch.Tensor,
+    image: torch.Tensor,
+    weights: torch.Tensor | None = None,
+    interpolation: Literal["nearest", "trilinear"] = "trilinear",
+) -> tuple[torch.Tensor, torch.Tensor]:
+    """Insert values into a (d, h, w) or (c, d, h, w) image (in place).
+
+    Returns ``(image, weights)``; ``weights`` (d, h, w) keeps its dtype and
+    defaults to a new float32 zero volume.  As in the reference, an
+    ``interpolation`` other than 'nearest' / 'trilinear' inserts nothing."""
+    multi = image.ndim == 4
+    d, h, w = image.shape[-3:]
+    values_shape = values.shape[:-1] if multi else values.shape
+    coordinates_shape, coordinates_ndim = coordinates.shape[:-1], coordinates.shape[-1]
+    if values_shape != coordinates_shape:
+        raise ValueError("One coordinate triplet is required for each value in data.")
+    if coordinates_ndim != 3:
+        raise ValueError("Coordinates must be 3D with shape (..., 3).")
+    if image.dtype != values.dtype:
+        raise ValueError("Image and values must have the same dtype.")
+    _lib.require_cuda(image)
+    if weights is None:
+        weights = torch.zeros(size=(d, h, w), dtype=torch.float32, device=image.device)
+    if interpolation not in ("nearest", "trilinear"):
+        return image, weights
+    if weights.dtype not in (torch.float32, torch.float64):
+        raise ValueError(f"weights must be float32 or float64, got {weights.dtype}")
+    code = _code(image.dtype)
+    C = image.shape[0] if multi else 1
+    vals = values.to(image.device).reshape(-1, C).contiguous()
+    c = coordinates.to(image.device).reshape(-1, 3).float().contiguous()
+    img = image if image.is_contiguous() else image.contiguous()
+    wts = weights if weights.is_contiguous() else weights.contiguous()
+    L = _lib.load()
+    _lib.check(L.tt_insert_into_image_3d(_lib.ptr(vals), code, _lib.ptr(c), c.shape[0],
+                                         _lib.ptr(img), C, d, h, w, _lib.ptr(wts),
+                                         int(wts.dtype == torch.float64),
+                                         int(interpolation == "nearest"),
+                                         _lib.stream_of(image.device)), "insert_into_image_3d")
+    if img is not image:
+        image.copy_(img)
+    if wts is not weights:
+        weights.copy_(wts)
+    return image, weights
+
+
+__all__ = ["sample_image_3d", "insert_into_image_3d"]

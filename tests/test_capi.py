@@ -1,0 +1,155 @@
+"""CPU checks of the C ABI and the host layer (no GPU, no kernel launches).
+
+* the library loads and exports every function include/teamtomo_b200.h declares,
+  and the ctypes layer binds exactly those;
+* argument validation fails with TT_ERR_INVALID before anything is launched;
+* the workspace query and the parameter struct layout;
+* host-side errors of the Python API raise the reference's exception types;
+* the product refuses CPU tensors (no CPU fallback).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "teamtomo_b200.h")
+
+
+def declared_functions() -> set[str]:
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return set(re.findall(r"\b(tt_[a-z0-9_]+)\s*\(", src))
+
+
+def test_library_exports_every_declared_symbol():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    declared = declared_functions()
+    assert len(declared) >= 10
+    for name in declared:
+        assert hasattr(L, name), name
+    assert set(_lib.SIGNATURES) == declared
+    assert L.tt_version() >= 100
+
+
+def _params(**kw):
+    from teamtomo_b200 import _lib
+
+    p = _lib.SliceParams()
+    p.n, p.img_d, p.img_h, p.img_w = 4, 16, 16, 16
+    p.vol_d, p.vol_h, p.vol_w = 16, 16, 9
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def test_param_struct_layout():
+    from teamtomo_b200 import _lib
+
+    # 7 int64 + 11 four-byte fields, padded to the 8-byte alignment of the struct
+    assert ctypes.sizeof(_lib.SliceParams) == 104
+    assert _lib.SliceParams.fftfreq_max.offset == 60 and _lib.SliceParams.reserved.offset == 96
+
+
+def test_validation_rejects_before_launch():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    fake = ctypes.c_void_p(16)  # never dereferenced: validation fails first
+    p = _params(n=-1)
+    assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert b"n must be" in L.tt_last_error()
+    p = _params(img_h=0)
+    assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    p = _params()
+    assert L.tt_extract_central_slices_rfft_3d(None, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert b"NULL" in L.tt_last_error()
+    p = _params(vol_w=8)  # insertion needs the rfft of volume_shape
+    assert L.tt_insert_central_slices_rfft_3d(fake, 0, fake, fake, fake, ctypes.byref(p), None) == \
+        _lib.TT_ERR_INVALID
+    p = _params()
+    assert L.tt_extract_central_slices_rfft_3d_backward(fake, fake, fake, None, fake, None, 0,
+                                                        ctypes.byref(p), None) == _lib.TT_ERR_WORKSPACE
+    assert L.tt_friedel_mirror_x0(None, None, 0, 1, 4, 4, 3, None) == _lib.TT_ERR_INVALID
+    assert L.tt_slice_geometry(fake, 7, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert L.tt_sample_image_3d(fake, 9, 1, 4, 4, 4, fake, 1, fake, 0, None) == _lib.TT_ERR_INVALID
+    assert L.tt_backproject_finish(fake, 0, 1, 8, 4, fake, None) == _lib.TT_ERR_INVALID
+    # n == 0 is a successful no-op that touches nothing
+    p = _params(n=0)
+    assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_OK
+
+
+def test_workspace_query():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    p = _params(n=4096, img_d=256, img_h=256, img_w=256, vol_d=256, vol_h=256, vol_w=129)
+    tiles = (256 * 129 + 255) // 256
+    assert L.tt_extract_backward_workspace_bytes(ctypes.byref(p)) == 4096 * tiles * 6 * 4
+    p = _params(n=0)
+    assert L.tt_extract_backward_workspace_bytes(ctypes.byref(p)) == 0
+
+
+def test_slice_params_rounding():
+    from teamtomo_b200.torch_fourier_slice._params import slice_params
+
+    p = slice_params(n=3, image_shape=(16, 16, 16), volume=None, rotation=torch.zeros(3, 3, 3),
+                     fftfreq_max=0.3, x_tolerance=1e-8, rot_tolerance=1e-8, vol_dims=(16, 16, 9))
+    assert p.x_tolerance == float(np.float32(1e-8))
+    assert p.x_tolerance10 == float(np.float32(1e-8 * 10))
+    assert p.fftfreq_max == float(np.float32(0.3))
+    assert p.has_rot_tolerance == 1 and p.rotation_f64 == 0
+    p = slice_params(n=1, image_shape=(8, 8, 8), volume=None, rotation=torch.zeros(1, 3, 3, dtype=torch.float64),
+                     rot_tolerance=None, vol_dims=(8, 8, 5))
+    assert p.has_rot_tolerance == 0 and p.rotation_f64 == 1 and p.has_fftfreq_max == 0
+
+
+def test_rotation_arg():
+    from teamtomo_b200.torch_fourier_slice._params import rotation_arg
+
+    R, stack = rotation_arg(torch.zeros(4, 5, 3, 3, dtype=torch.float16), torch.device("cpu"))
+    assert R.shape == (20, 3, 3) and R.dtype == torch.float32 and stack == (4, 5)
+    R, stack = rotation_arg(torch.zeros(3, 3, dtype=torch.float64), torch.device("cpu"))
+    assert R.shape == (1, 3, 3) and R.dtype == torch.float64 and stack == ()
+    with pytest.raises(ValueError):
+        rotation_arg(torch.zeros(4, 3, 2), torch.device("cpu"))
+
+
+def test_no_cpu_fallback():
+    import teamtomo_b200 as tt
+
+    vol = torch.zeros((8, 8, 5), dtype=torch.complex64)
+    with pytest.raises(RuntimeError, match="CUDA tensors only"):
+        tt.extract_central_slices_rfft_3d(vol, (8, 8, 8), torch.eye(3))
+    with pytest.raises(RuntimeError, match="CUDA tensors only"):
+        tt.insert_central_slices_rfft_3d(torch.zeros((1, 8, 5), dtype=torch.complex64), (8, 8, 8),
+                                         torch.eye(3)[None])
+    with pytest.raises(RuntimeError, match="CUDA tensors only"):
+        tt.sample_image_3d(torch.zeros((4, 4, 4)), torch.zeros((2, 3)))
+
+
+def test_reference_exceptions_on_host():
+    import teamtomo_b200 as tt
+
+    with pytest.raises(ValueError, match="all dimensions of volume must be equal"):
+        tt.project_3d_to_2d(torch.zeros((8, 8, 9)), torch.eye(3))
+    with pytest.raises(ValueError, match="pad_factor"):
+        tt.project_3d_to_2d(torch.zeros((8, 8, 8)), torch.eye(3), pad_factor=0.5)
+    with pytest.raises(ValueError, match="images must be square"):
+        tt.backproject_2d_to_3d(torch.zeros((2, 8, 9)), torch.eye(3)[None])
+    with pytest.raises(AssertionError):
+        tt.extract_central_slices_rfft_3d(torch.zeros((8, 8)), (8, 8, 8), torch.eye(3))
+    with pytest.raises(ValueError, match="One coordinate triplet"):
+        tt.insert_into_image_3d(torch.zeros(3), torch.zeros((4, 3)), torch.zeros((4, 4, 4)))
+    with pytest.raises(ValueError, match="same dtype"):
+        tt.insert_into_image_3d(torch.zeros(4, dtype=torch.float64), torch.zeros((4, 3)), torch.zeros((4, 4, 4)))
+    with pytest.raises(ValueError, match="shape \\(d, h, w\\)"):
+        tt.sample_image_3d(torch.zeros((4, 4)), torch.zeros((2, 3)))

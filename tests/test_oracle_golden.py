@@ -1,0 +1,143 @@
+"""The CPU oracle pinned against golden vectors produced by the reference itself.
+
+These run without a GPU.  They are what makes the oracle trustworthy as the
+checker of the CUDA path: extraction must match the reference bit for bit,
+everything accumulated (insertion, gradients) within float32 summation-order
+noise.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+
+
+def _extract_kwargs(g, name):
+    fmax = float(g[f"extract_{name}_fmax"])
+    rtol = float(g[f"extract_{name}_rtol"])
+    return dict(
+        fftfreq_max=None if fmax < 0 else fmax,
+        zyx_matrices=bool(int(g[f"extract_{name}_zyx"])),
+        rot_tolerance=None if rtol < 0 else rtol,
+        x_tolerance=float(g[f"extract_{name}_xtol"]),
+    )
+
+
+def _insert_kwargs(g, name):
+    fmax = float(g[f"insert_{name}_fmax"])
+    return dict(fftfreq_max=None if fmax < 0 else fmax,
+                zyx_matrices=bool(int(g[f"insert_{name}_zyx"])))
+
+
+def test_extract_bit_exact(golden, oracle):
+    for name in golden["extract_cases"]:
+        name = str(name)
+        out = oracle.extract(golden[f"extract_{name}_volume"], tuple(golden[f"extract_{name}_shape"]),
+                             golden[f"extract_{name}_rot"], **_extract_kwargs(golden, name))
+        ref = golden[f"extract_{name}_out"]
+        assert out.shape == ref.shape, name
+        assert np.array_equal(out, ref), f"{name}: max |diff| {np.abs(out - ref).max()}"
+
+
+def test_insert_matches_reference(golden, oracle):
+    for name in golden["insert_cases"]:
+        name = str(name)
+        imgs = golden[f"insert_{name}_images"]
+        n = imgs.shape[-2]
+        vol, w = oracle.insert(imgs, (n, n, n), golden[f"insert_{name}_rot"],
+                               **_insert_kwargs(golden, name))
+        assert vol.dtype == golden[f"insert_{name}_volume"].dtype
+        assert w.dtype == golden[f"insert_{name}_weights"].dtype
+        tol = 1e-12 if vol.dtype == np.complex128 else 1e-6
+        assert rel_l2(vol, golden[f"insert_{name}_volume"]) < tol, name
+        assert rel_l2(w, golden[f"insert_{name}_weights"]) < tol, name
+        # whole-volume support is identical: no voxel touched by one and not the other
+        assert np.array_equal(w != 0, golden[f"insert_{name}_weights"] != 0), name
+
+
+def test_gradients_match_reference_autograd(golden, oracle):
+    vol = golden["grad_drot_volume"]
+    n = vol.shape[0]
+    _, drot = oracle.extract_grad(vol, (n, n, n), golden["grad_drot_rot"], golden["grad_drot_G"],
+                                  want_dvol=False)
+    assert rel_l2(drot, golden["grad_drot_out"]) < 1e-5
+    vol = golden["grad_dvol_volume"]
+    n = vol.shape[0]
+    dvol, _ = oracle.extract_grad(vol, (n, n, n), golden["grad_dvol_rot"], golden["grad_dvol_G"],
+                                  want_drot=False)
+    assert rel_l2(dvol, golden["grad_dvol_out"]) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["real", "complex", "multi", "f64"])
+@pytest.mark.parametrize("mode", ["trilinear", "nearest"])
+def test_sample_image_3d(golden, oracle, name, mode):
+    out = oracle.sample_image_3d(golden[f"sample_{name}_image"], golden[f"sample_{name}_coords"], mode)
+    ref = golden[f"sample_{name}_{mode}_out"]
+    assert out.shape == ref.shape and out.dtype == ref.dtype
+    tol = 1e-12 if ref.dtype in (np.float64, np.complex128) else 1e-6
+    assert rel_l2(out, ref) < tol
+
+
+@pytest.mark.parametrize("name", ["f32", "c64", "f32w64"])
+@pytest.mark.parametrize("mode", ["trilinear", "nearest"])
+def test_insert_into_image_3d(golden, oracle, name, mode):
+    img_ref = golden[f"insimg_{name}_{mode}_image"]
+    w_ref = golden[f"insimg_{name}_{mode}_weights"]
+    img, w = oracle.insert_into_image_3d(golden[f"insimg_{name}_values"], golden[f"insimg_{name}_coords"],
+                                         np.zeros_like(img_ref), np.zeros_like(w_ref), mode)
+    assert rel_l2(img, img_ref) < 1e-6 and rel_l2(w, w_ref) < 1e-6
+    assert w.dtype == w_ref.dtype
+
+
+def test_insert_into_image_3d_multichannel(golden, oracle):
+    ref = golden["insimg_multi_trilinear_image"]
+    img, w = oracle.insert_into_image_3d(golden["insimg_multi_values"], golden["insimg_multi_coords"],
+                                         np.zeros_like(ref))
+    assert rel_l2(img, ref) < 1e-6
+    assert rel_l2(w, golden["insimg_multi_trilinear_weights"]) < 1e-6
+
+
+def test_insert_into_image_3d_known_answers(oracle):
+    # test_image_interpolation_3d.py:66-81: 5 at (10.5, 14.5, 18.5) -> 5/8 on 8 voxels
+    img, _ = oracle.insert_into_image_3d(np.array([5.0], np.float32),
+                                         np.array([[10.5, 14.5, 18.5]], np.float32),
+                                         np.zeros((28, 28, 28), np.float32))
+    assert np.allclose(img[10:12, 14:16, 18:20], 5 / 8)
+    assert img.sum() == pytest.approx(5.0)
+    # :100-113: nearest at (10.7, 14.3, 18.9) -> 5 at [11, 14, 19]
+    img, _ = oracle.insert_into_image_3d(np.array([5.0], np.float32),
+                                         np.array([[10.7, 14.3, 18.9]], np.float32),
+                                         np.zeros((28, 28, 28), np.float32), interpolation="nearest")
+    exp = np.zeros((28, 28, 28), np.float32)
+    exp[11, 14, 19] = 5
+    assert np.array_equal(img, exp)
+
+
+def test_project_backproject(golden, oracle):
+    vol, rot = golden["project_volume"], golden["project_rot"]
+    assert rel_l2(oracle.project_3d_to_2d(vol, rot), golden["project_out"]) < 1e-5
+    assert rel_l2(oracle.project_3d_to_2d(vol, rot, fftfreq_max=0.25), golden["project_fmax_out"]) < 1e-5
+    assert rel_l2(oracle.project_3d_to_2d(vol, rot, pad_factor=1.0), golden["project_pad1_out"]) < 1e-5
+    imgs = golden["backproject_images"]
+    rec = oracle.backproject_2d_to_3d(imgs, golden["backproject_rot"])
+    assert rel_l2(rec, golden["backproject_out"]) < 1e-5
+    rec64 = oracle.backproject_2d_to_3d(imgs.astype(np.float64), golden["backproject_rot"])
+    assert rec64.dtype == np.float64
+    assert rel_l2(rec64, golden["backproject_f64_out"]) < 1e-5
+
+
+def test_insert_mirror_is_plane_post_pass(golden, oracle):
+    """The reference's per-corner Friedel mirror equals a splat without it
+    followed by one post-pass over the x=0 plane (the form the CUDA path uses)."""
+    for name in golden["insert_cases"]:
+        name = str(name)
+        imgs = golden[f"insert_{name}_images"]
+        n = imgs.shape[-2]
+        acc, accw = oracle.insert(imgs, (n, n, n), golden[f"insert_{name}_rot"], mirror=False,
+                                  **_insert_kwargs(golden, name))
+        vol, w = oracle.mirror_x0_post_pass(acc, accw)
+        tol = 1e-12 if vol.dtype == np.complex128 else 1e-6
+        assert rel_l2(vol, golden[f"insert_{name}_volume"]) < tol, name
+        assert rel_l2(w, golden[f"insert_{name}_weights"]) < tol, name
