@@ -154,10 +154,11 @@ int tt_insert_into_image_3d(const void *values, int32_t dtype, const float *coor
 int tt_project_prepare(const void *volume, int32_t is_f64, int64_t d, int64_t pad, void *out,
                        void *stream);
 
-/* out (m, n-2*pad, n-2*pad) = crop(ifftshift(images, (-2, -1)), pad) for
- * images (m, n, n) (project.py:87-92). */
-int tt_recentre_crop_2d(const void *images, int32_t is_f64, int64_t m, int64_t n, int64_t pad,
-                        void *out, void *stream);
+/* out (m, h-2*pad, w-2*pad) = crop(ifftshift(images, (-2, -1)), pad) for
+ * images (m, h, w) (project.py:87-92; w = h-1 for odd padded sizes, because
+ * the reference's irfftn runs without an output size). */
+int tt_recentre_crop_2d(const void *images, int32_t is_f64, int64_t m, int64_t h, int64_t w,
+                        int64_t pad, void *out, void *stream);
 
 /* out (m, n, n) = fftshift(pad(images, pad), (-2, -1)), images (m, d, d),
  * n = d + 2*pad (backproject.py:48-59). */
@@ -171,10 +172,11 @@ int tt_backproject_normalize(const void *volume_acc, const void *weights, int32_
                              int64_t channels, int64_t d, int64_t h, int64_t w_rfft, void *out,
                              void *stream);
 
-/* out (channels, c^3), c = n - 2*pad = crop(ifftshift(volume) / sinc(|f|)^2)
- * of the irfft output volume (channels, n^3) (backproject.py:80-92). */
-int tt_backproject_finish(const void *volume, int32_t is_f64, int64_t channels, int64_t n,
-                          int64_t pad, void *out, void *stream);
+/* out (channels, n0-2*pad, n1-2*pad, n2-2*pad) = crop(ifftshift(volume) /
+ * sinc(|f|)^2) of the irfft output volumes (channels, n0, n1, n2), the sinc
+ * grid being that of the (n0, n1, n2) array (backproject.py:80-92). */
+int tt_backproject_finish(const void *volume, int32_t is_f64, int64_t channels, int64_t n0,
+                          int64_t n1, int64_t n2, int64_t pad, void *out, void *stream);
 
 #ifdef __cplusplus
 }

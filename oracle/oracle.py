@@ -400,7 +400,7 @@ def project_3d_to_2d(volume, rotation_matrices, pad_factor=2.0, fftfreq_max=None
     sl = extract(dft, shape, rotation_matrices, fftfreq_max=fftfreq_max,
                  zyx_matrices=zyx_matrices)
     sl = np.fft.ifftshift(sl, axes=(-2,))
-    im = np.fft.irfftn(sl, s=shape[-2:], axes=(-2, -1))
+    im = np.fft.irfftn(sl, axes=(-2, -1))  # no output size, as the reference (odd: n-1 wide)
     im = np.fft.ifftshift(im, axes=(-2, -1)).astype(np.float32)
     if p:
         im = im[..., p:-p, p:-p]
@@ -428,9 +428,9 @@ def backproject_2d_to_3d(images, rotation_matrices, pad_factor=2.0, fftfreq_max=
                       zyx_matrices=zyx_matrices)
     vol = vol / np.maximum(wts, 1.0)
     vol = np.fft.ifftshift(vol, axes=(0, 1))
-    real = np.fft.irfftn(vol, s=shape, axes=(0, 1, 2))
+    real = np.fft.irfftn(vol, axes=(0, 1, 2))  # no output size, as the reference
     real = np.fft.ifftshift(real)
-    real = real / _sinc(_fftfreq_norm_grid(shape)).astype(real.dtype) ** 2
+    real = real / _sinc(_fftfreq_norm_grid(real.shape)).astype(real.dtype) ** 2
     if p:
         real = real[p:-p, p:-p, p:-p]
     return real.astype(np.float64 if double else np.float32)

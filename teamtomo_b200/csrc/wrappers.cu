@@ -23,12 +23,13 @@ __device__ __forceinline__ float fftfreq_at(int64_t k, int64_t n, float inv_n) {
     return __fmul_rn((float)kk, inv_n);
 }
 
-// sinc(|f|)^2 at position a of the fftshifted norm grid of an n^3 array
-// (fftfreq_grid(rfft=False, fftshift=True, norm=True)).
-__device__ __forceinline__ float sinc2_at(int64_t a0, int64_t a1, int64_t a2, int64_t n, float inv_n) {
-    const float f0 = fftfreq_at(wrap(a0 - n / 2, n), n, inv_n);
-    const float f1 = fftfreq_at(wrap(a1 - n / 2, n), n, inv_n);
-    const float f2 = fftfreq_at(wrap(a2 - n / 2, n), n, inv_n);
+// sinc(|f|)^2 at position a of the fftshifted norm grid of an (n0, n1, n2)
+// array (fftfreq_grid(rfft=False, fftshift=True, norm=True)).
+__device__ __forceinline__ float sinc2_at(int64_t a0, int64_t a1, int64_t a2, int64_t n0, int64_t n1, int64_t n2,
+                                          float i0, float i1, float i2) {
+    const float f0 = fftfreq_at(wrap(a0 - n0 / 2, n0), n0, i0);
+    const float f1 = fftfreq_at(wrap(a1 - n1 / 2, n1), n1, i1);
+    const float f2 = fftfreq_at(wrap(a2 - n2 / 2, n2), n2, i2);
     const float r = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(f0, f0), __fmul_rn(f1, f1)), __fmul_rn(f2, f2)));
     if (r == 0.0f) return 1.0f;
     const float px = __fmul_rn(3.14159265358979323846f, r);
@@ -47,20 +48,20 @@ __global__ void project_prepare_kernel(const T* __restrict__ vol, T* __restrict_
     const int64_t v0 = a0 - p, v1 = a1 - p, v2 = a2 - p;
     T v = 0;
     if (v0 >= 0 && v0 < d && v1 >= 0 && v1 < d && v2 >= 0 && v2 < d)
-        v = vol[(v0 * d + v1) * d + v2] * (T)sinc2_at(a0, a1, a2, n, inv_n);
+        v = vol[(v0 * d + v1) * d + v2] * (T)sinc2_at(a0, a1, a2, n, n, n, inv_n, inv_n, inv_n);
     out[idx] = v;
 }
 
-// out (m, n-2p, n-2p) = crop(ifftshift(images, (-2,-1)), p)
+// out (m, h-2p, w-2p) = crop(ifftshift(images, (-2,-1)), p), images (m, h, w)
 template <typename T>
-__global__ void recentre_crop_2d_kernel(const T* __restrict__ img, T* __restrict__ out, int64_t m, int64_t n,
-                                        int64_t p) {
-    const int64_t c = n - 2 * p;
+__global__ void recentre_crop_2d_kernel(const T* __restrict__ img, T* __restrict__ out, int64_t m, int64_t h,
+                                        int64_t w, int64_t p) {
+    const int64_t ch = h - 2 * p, cw = w - 2 * p;
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= m * c * c) return;
-    const int64_t b = idx / (c * c), i = (idx / c) % c, j = idx % c;
-    const int64_t si = wrap(i + p + n / 2, n), sj = wrap(j + p + n / 2, n);
-    out[idx] = img[(b * n + si) * n + sj];
+    if (idx >= m * ch * cw) return;
+    const int64_t b = idx / (ch * cw), i = (idx / cw) % ch, j = idx % cw;
+    const int64_t si = wrap(i + p + h / 2, h), sj = wrap(j + p + w / 2, w);
+    out[idx] = img[(b * h + si) * w + sj];
 }
 
 // out (m, n, n) = fftshift(pad(images, p), (-2,-1)), images (m, d, d)
@@ -121,16 +122,18 @@ __global__ void normalize_unshift_kernel(const typename C2<R>::T* __restrict__ a
     out[idx] = v;
 }
 
-// out (c^3) = crop(ifftshift(vol) / sinc^2, p), vol (n^3) real
+// out (n0-2p, n1-2p, n2-2p) = crop(ifftshift(vol) / sinc^2, p), vol (n0, n1, n2)
+// real; the sinc^2 grid is that of the (n0, n1, n2) array.
 template <typename T>
-__global__ void backproject_finish_kernel(const T* __restrict__ vol, T* __restrict__ out, int64_t n, int64_t p,
-                                          float inv_n) {
-    const int64_t c = n - 2 * p;
+__global__ void backproject_finish_kernel(const T* __restrict__ vol, T* __restrict__ out, int64_t n0, int64_t n1,
+                                          int64_t n2, int64_t p) {
+    const int64_t c0 = n0 - 2 * p, c1 = n1 - 2 * p, c2 = n2 - 2 * p;
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= c * c * c) return;
-    const int64_t i = idx / (c * c) + p, j = (idx / c) % c + p, k = idx % c + p;
-    const int64_t s = (wrap(i + n / 2, n) * n + wrap(j + n / 2, n)) * n + wrap(k + n / 2, n);
-    out[idx] = vol[s] / (T)sinc2_at(i, j, k, n, inv_n);
+    if (idx >= c0 * c1 * c2) return;
+    const int64_t i = idx / (c1 * c2) + p, j = (idx / c2) % c1 + p, k = idx % c2 + p;
+    const int64_t s = (wrap(i + n0 / 2, n0) * n1 + wrap(j + n1 / 2, n1)) * n2 + wrap(k + n2 / 2, n2);
+    const float i0 = (float)(1.0 / (double)n0), i1 = (float)(1.0 / (double)n1), i2 = (float)(1.0 / (double)n2);
+    out[idx] = vol[s] / (T)sinc2_at(i, j, k, n0, n1, n2, i0, i1, i2);
 }
 
 inline unsigned blocks_for(int64_t total, int threads) { return (unsigned)((total + threads - 1) / threads); }
@@ -153,18 +156,18 @@ extern "C" int tt_project_prepare(const void* volume, int32_t is_f64, int64_t d,
     return check_launch("project_prepare_kernel");
 }
 
-extern "C" int tt_recentre_crop_2d(const void* images, int32_t is_f64, int64_t m, int64_t n, int64_t pad, void* out,
-                                   void* stream) {
-    if (!images || !out || m < 0 || n < 1 || pad < 0 || 2 * pad >= n)
+extern "C" int tt_recentre_crop_2d(const void* images, int32_t is_f64, int64_t m, int64_t h, int64_t w, int64_t pad,
+                                   void* out, void* stream) {
+    if (!images || !out || m < 0 || h < 1 || w < 1 || pad < 0 || 2 * pad >= h || 2 * pad >= w)
         return fail(TT_ERR_INVALID, "recentre_crop_2d: bad arguments");
     if (m == 0) return TT_OK;
-    const int64_t c = n - 2 * pad, total = m * c * c;
+    const int64_t total = m * (h - 2 * pad) * (w - 2 * pad);
     if (is_f64)
         recentre_crop_2d_kernel<double><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
-            (const double*)images, (double*)out, m, n, pad);
+            (const double*)images, (double*)out, m, h, w, pad);
     else
         recentre_crop_2d_kernel<float><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
-            (const float*)images, (float*)out, m, n, pad);
+            (const float*)images, (float*)out, m, h, w, pad);
     return check_launch("recentre_crop_2d_kernel");
 }
 
@@ -198,19 +201,19 @@ extern "C" int tt_backproject_normalize(const void* volume_acc, const void* weig
     return check_launch("normalize_unshift_kernel");
 }
 
-extern "C" int tt_backproject_finish(const void* volume, int32_t is_f64, int64_t channels, int64_t n, int64_t pad,
-                                     void* out, void* stream) {
-    if (!volume || !out || channels < 1 || n < 1 || pad < 0 || 2 * pad >= n)
+extern "C" int tt_backproject_finish(const void* volume, int32_t is_f64, int64_t channels, int64_t n0, int64_t n1,
+                                     int64_t n2, int64_t pad, void* out, void* stream) {
+    if (!volume || !out || channels < 1 || n0 < 1 || n1 < 1 || n2 < 1 || pad < 0 || 2 * pad >= n0 ||
+        2 * pad >= n1 || 2 * pad >= n2)
         return fail(TT_ERR_INVALID, "backproject_finish: bad arguments");
-    const int64_t c = n - 2 * pad, per = c * c * c;
-    const float inv_n = (float)(1.0 / (double)n);
+    const int64_t per = (n0 - 2 * pad) * (n1 - 2 * pad) * (n2 - 2 * pad), in = n0 * n1 * n2;
     for (int64_t ch = 0; ch < channels; ch++) {
         if (is_f64)
             backproject_finish_kernel<double><<<blocks_for(per, 256), 256, 0, as_stream(stream)>>>(
-                (const double*)volume + ch * n * n * n, (double*)out + ch * per, n, pad, inv_n);
+                (const double*)volume + ch * in, (double*)out + ch * per, n0, n1, n2, pad);
         else
             backproject_finish_kernel<float><<<blocks_for(per, 256), 256, 0, as_stream(stream)>>>(
-                (const float*)volume + ch * n * n * n, (float*)out + ch * per, n, pad, inv_n);
+                (const float*)volume + ch * in, (float*)out + ch * per, n0, n1, n2, pad);
         if (int e = check_launch("backproject_finish_kernel")) return e;
     }
     return TT_OK;

@@ -53,11 +53,10 @@ class _ProjectPrepare(torch.autograd.Function):
 class _RecentreCrop2d(torch.autograd.Function):
     @staticmethod
     def forward(ctx, images, pad):
-        m, n = images.shape[0], images.shape[-1]
-        c = n - 2 * pad
-        out = torch.empty((m, c, c), dtype=images.dtype, device=images.device)
+        m, h, w = images.shape
+        out = torch.empty((m, h - 2 * pad, w - 2 * pad), dtype=images.dtype, device=images.device)
         L = _lib.load()
-        _lib.check(L.tt_recentre_crop_2d(_lib.ptr(images), _is_f64(images), m, n, pad,
+        _lib.check(L.tt_recentre_crop_2d(_lib.ptr(images), _is_f64(images), m, h, w, pad,
                                          _lib.ptr(out), _lib.stream_of(images.device)),
                    "recentre_crop_2d")
         ctx.pad = pad
@@ -79,8 +78,8 @@ def project_prepare(volume: torch.Tensor, pad: int) -> torch.Tensor:
 
 
 def recentre_crop_2d(images: torch.Tensor, pad: int) -> torch.Tensor:
-    n = images.shape[-1]
-    flat = images.reshape(-1, n, n).contiguous()
+    h, w = images.shape[-2:]
+    flat = images.reshape(-1, h, w).contiguous()
     return _RecentreCrop2d.apply(flat, int(pad))
 
 
@@ -110,14 +109,15 @@ def backproject_normalize(volume_acc: torch.Tensor, weights: torch.Tensor) -> to
 
 
 def backproject_finish(volume: torch.Tensor, pad: int) -> torch.Tensor:
-    """(c?, n, n, n) irfft output -> crop(ifftshift(v) / sinc^2)."""
-    n = volume.shape[-1]
+    """(c?, n0, n1, n2) irfft output -> crop(ifftshift(v) / sinc^2)."""
+    n0, n1, n2 = volume.shape[-3:]
     lead = volume.shape[:-3]
-    channels = volume.numel() // (n ** 3)
-    c = n - 2 * pad
-    out = torch.empty((*lead, c, c, c), dtype=volume.dtype, device=volume.device)
+    channels = volume.numel() // (n0 * n1 * n2)
+    volume = volume.contiguous()
+    out = torch.empty((*lead, n0 - 2 * pad, n1 - 2 * pad, n2 - 2 * pad), dtype=volume.dtype,
+                      device=volume.device)
     L = _lib.load()
-    _lib.check(L.tt_backproject_finish(_lib.ptr(volume), _is_f64(volume), channels, n, pad,
-                                       _lib.ptr(out), _lib.stream_of(volume.device)),
+    _lib.check(L.tt_backproject_finish(_lib.ptr(volume), _is_f64(volume), channels, n0, n1, n2,
+                                       pad, _lib.ptr(out), _lib.stream_of(volume.device)),
                "backproject_finish")
     return out

@@ -55,7 +55,8 @@ def _backproject(images, rotation_matrices, pad_factor, fftfreq_max, zyx_matrice
                      weights if ch == 0 else scratch_w, fftfreq_max, zyx_matrices,
                      images_unshifted=True)
     dft = _wrappers.backproject_normalize(acc, weights)
-    real = torch.fft.irfftn(dft, s=shape, dim=(-3, -2, -1))
+    # irfftn without an output size, as the reference (odd boxes lose one x column)
+    real = torch.fft.irfftn(dft, dim=(-3, -2, -1))
     out = _wrappers.backproject_finish(real, p)
     return out if channels else out[0]
 

@@ -41,15 +41,18 @@ def project_3d_to_2d(
     n_pad = d + 2 * p
     shape = (n_pad, n_pad, n_pad)
     fft_in = _wrappers.project_prepare(volume, p)  # padded * sinc^2, fftshifted
-    dft = torch.fft.rfftn(fft_in, dim=(-3, -2, -1))  # unshifted rfft
+    # unshifted rfft; cuFFT may hand back a non-contiguous layout
+    dft = torch.fft.rfftn(fft_in, dim=(-3, -2, -1)).contiguous()
     R, stack = rotation_arg(rotation_matrices, volume.device)
     params = slice_params(n=R.shape[0], image_shape=shape, volume=dft, rotation=R,
                           fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
                           rot_tolerance=1e-8, volume_unshifted=True, slices_unshifted=True)
     slices = _ExtractCentralSlices.apply(dft, R, params, (R.shape[0], n_pad, n_pad // 2 + 1))
-    images = torch.fft.irfftn(slices, s=(n_pad, n_pad), dim=(-2, -1))
+    # irfftn without an output size, as the reference: an odd padded box
+    # gives images one column narrower (2 * (n_pad // 2) wide)
+    images = torch.fft.irfftn(slices, dim=(-2, -1))
     out = _wrappers.recentre_crop_2d(images, p)
-    return out.reshape(*stack, d, d)
+    return out.reshape(*stack, *out.shape[-2:])
 
 
 def project_3d_to_2d_multichannel(

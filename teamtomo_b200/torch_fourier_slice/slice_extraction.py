@@ -24,6 +24,9 @@ from ._params import rotation_arg, slice_params
 class _ExtractCentralSlices(torch.autograd.Function):
     @staticmethod
     def forward(ctx, volume_rfft, rotation_matrices, params, out_shape):
+        # the kernels index raw memory in C order
+        if not (volume_rfft.is_contiguous() and rotation_matrices.is_contiguous()):
+            raise ValueError("extraction needs C-contiguous volume and rotation tensors")
         dev = volume_rfft.device
         out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
         L = _lib.load()

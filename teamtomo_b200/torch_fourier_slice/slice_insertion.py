@@ -35,6 +35,10 @@ def insert_splat(image_rfft, R, volume_shape, volume, weights, fftfreq_max=None,
     """Accumulate the trilinear splat of (n, h, w//2+1) slices into ``volume``
     / ``weights`` (no Friedel completion)."""
     dev = volume.device
+    # the kernels index raw memory in C order
+    if not (image_rfft.is_contiguous() and R.is_contiguous() and volume.is_contiguous()
+            and weights.is_contiguous()):
+        raise ValueError("insertion needs C-contiguous slices, rotations, volume and weights")
     params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=volume, rotation=R,
                           fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
                           slices_unshifted=images_unshifted)

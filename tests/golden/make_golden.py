@@ -209,6 +209,13 @@ def main():
     g["backproject_images"], g["backproject_rot"], g["backproject_out"] = proj.numpy(), rots, rec.numpy()
     rec64 = backproject_2d_to_3d(proj.double(), torch.tensor(rots))
     g["backproject_f64_out"] = rec64.numpy()
+    # odd padded box: the reference's irfftn has no output size -> (d, d-1) images
+    odd = torch.tensor(blob_volume(33, 33))
+    proj_odd = project_3d_to_2d(odd, torch.tensor(rots), pad_factor=1.5)
+    g["project_odd_volume"], g["project_odd_out"] = odd.numpy(), proj_odd.numpy()
+    imgs_odd = torch.tensor(np.random.default_rng(4).standard_normal((6, 33, 33)).astype(np.float32))
+    g["backproject_odd_images"] = imgs_odd.numpy()
+    g["backproject_odd_out"] = backproject_2d_to_3d(imgs_odd, torch.tensor(rots), pad_factor=1.5).numpy()
 
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {os.path.getsize(OUT) / 1e6:.2f} MB, {len(g)} arrays")

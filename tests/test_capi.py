@@ -81,7 +81,8 @@ def test_validation_rejects_before_launch():
     assert L.tt_friedel_mirror_x0(None, None, 0, 1, 4, 4, 3, None) == _lib.TT_ERR_INVALID
     assert L.tt_slice_geometry(fake, 7, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
     assert L.tt_sample_image_3d(fake, 9, 1, 4, 4, 4, fake, 1, fake, 0, None) == _lib.TT_ERR_INVALID
-    assert L.tt_backproject_finish(fake, 0, 1, 8, 4, fake, None) == _lib.TT_ERR_INVALID
+    assert L.tt_backproject_finish(fake, 0, 1, 8, 8, 8, 4, fake, None) == _lib.TT_ERR_INVALID
+    assert L.tt_recentre_crop_2d(fake, 0, 1, 8, 7, 4, fake, None) == _lib.TT_ERR_INVALID
     # n == 0 is a successful no-op that touches nothing
     p = _params(n=0)
     assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_OK

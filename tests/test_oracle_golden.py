@@ -126,6 +126,13 @@ def test_project_backproject(golden, oracle):
     rec64 = oracle.backproject_2d_to_3d(imgs.astype(np.float64), golden["backproject_rot"])
     assert rec64.dtype == np.float64
     assert rel_l2(rec64, golden["backproject_f64_out"]) < 1e-5
+    # odd padded box: (d, d-1) outputs, as the reference
+    po = oracle.project_3d_to_2d(golden["project_odd_volume"], rot, pad_factor=1.5)
+    assert po.shape == golden["project_odd_out"].shape == (6, 33, 32)
+    assert rel_l2(po, golden["project_odd_out"]) < 1e-5
+    bo = oracle.backproject_2d_to_3d(golden["backproject_odd_images"], rot, pad_factor=1.5)
+    assert bo.shape == golden["backproject_odd_out"].shape == (33, 33, 32)
+    assert rel_l2(bo, golden["backproject_odd_out"]) < 1e-5
 
 
 def test_insert_mirror_is_plane_post_pass(golden, oracle):
