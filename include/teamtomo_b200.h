@@ -103,6 +103,32 @@ int tt_extract_central_slices_rfft_3d_backward(const void *volume_rfft,
                                                size_t workspace_bytes,
                                                const tt_slice_params *p, void *stream);
 
+/* Size of the built-in scratch array used by
+ * tt_extract_central_slices_rfft_3d_backward_noalloc (per GPU, for the life of
+ * the process). */
+#define TT_NOALLOC_SCRATCH_BYTES (4u << 20)
+
+/* Same computation as tt_extract_central_slices_rfft_3d_backward, for callers
+ * that cannot allocate device memory (a host or plugin framework that owns
+ * all device allocations and only hands over the buffers of the call, or a
+ * fixed memory budget that must not grow): it takes no workspace and calls no
+ * allocator; the rotation-gradient partial sums go to a 4 MiB array built
+ * into the library instead.
+ *  - Limit: when grad_rotation is requested, n * ceil(img_h * (img_w/2+1) / 256)
+ *    * 24 bytes must not exceed TT_NOALLOC_SCRATCH_BYTES (at a 256^3 box that is
+ *    1354 slices per call); larger calls fail with TT_ERR_INVALID and a message.
+ *  - The first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make it before any
+ *    stream capture.
+ *  - All calls share the array: calls that overlap on the GPU race and must be
+ *    serialised by the caller.  Nothing needs clearing between calls.
+ * This entry point has no counterpart in the reference. */
+int tt_extract_central_slices_rfft_3d_backward_noalloc(const void *volume_rfft,
+                                                       const void *rotation_matrices,
+                                                       const void *grad_slices,
+                                                       void *grad_volume, void *grad_rotation,
+                                                       const tt_slice_params *p, void *stream);
+
 /* Central-slice insertion, splat stage: trilinear scatter of the slices and of
  * the interpolation weights into volume_rfft / weights (both ACCUMULATED into),
  * with the reference's strict x<0 conjugate redirect, the x=0/y<0 source-pixel

@@ -47,6 +47,8 @@ SIGNATURES = {
     "tt_extract_backward_workspace_bytes": ([ctypes.POINTER(SliceParams)], _sz),
     "tt_extract_central_slices_rfft_3d_backward": (
         [_vp, _vp, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_extract_central_slices_rfft_3d_backward_noalloc": (
+        [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_central_slices_rfft_3d": (
         [_vp, _i32, _vp, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_friedel_mirror_x0": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp], _i32),

@@ -16,6 +16,8 @@
 // rotation gradient is deterministic.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "capi_util.cuh"
 #include "slice_common.cuh"
 
@@ -353,4 +355,100 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward(
         if (int e = check_launch("drot_finish_kernel")) return e;
     }
     return TT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the extraction backward.
+//
+// Some callers cannot allocate device memory at the time they run this
+// backward: a host application or plugin framework that owns every device
+// allocation and only lends the library the buffers of one call, or a caller
+// working inside a fixed, pre-reserved memory budget that must never grow.
+// For them the rotation-gradient partial sums live in a fixed scratch array
+// compiled into this library instead of a caller-provided workspace.
+//
+// * The array is TT_NOALLOC_SCRATCH_BYTES (4 MiB) of device memory per GPU that
+//   loads the library, held until the process exits.
+// * Host code cannot pass the array's name to a kernel (it is only a host-side
+//   stand-in for the device symbol), so the first call on each device looks up
+//   its device address with cudaGetSymbolAddress while that device is current
+//   and keeps it.  Make that first call before any stream capture.
+// * Every call shares the one array.  Calls whose kernels overlap on the GPU
+//   (different streams, or different host threads on the same device) race on
+//   it and must be serialised by the caller.  Each call fully overwrites the
+//   part it reads, so nothing has to be cleared between calls.
+// * No cudaMalloc, cudaFree or allocating library routine is called.
+// ---------------------------------------------------------------------------
+
+static __device__ __align__(256) float g_noalloc_scratch[TT_NOALLOC_SCRATCH_BYTES / sizeof(float)];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+float* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_scratch on the current device (looked up once).
+int noalloc_scratch(float** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return tt::fail(TT_ERR_CUDA, "noalloc backward: cudaGetDevice: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices) return tt::fail(TT_ERR_INVALID, "noalloc backward: device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        float* ptr = nullptr;
+        e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return tt::fail(TT_ERR_CUDA, "noalloc backward: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = ptr;
+    }
+    *out = g_noalloc_ptr[dev];
+    return TT_OK;
+}
+}  // namespace
+
+extern "C" int tt_extract_central_slices_rfft_3d_backward_noalloc(const void* volume_rfft,
+                                                                  const void* rotation_matrices,
+                                                                  const void* grad_slices, void* grad_volume,
+                                                                  void* grad_rotation, const tt_slice_params* p,
+                                                                  void* stream) {
+    if (int e = validate_params(p)) return e;
+    if (p->n == 0) return TT_OK;
+    if (!volume_rfft || !rotation_matrices || !grad_slices)
+        return fail(TT_ERR_INVALID, "noalloc backward: NULL pointer argument");
+    if (!grad_volume && !grad_rotation) return TT_OK;
+    SliceGeom g = make_geom(*p);
+    const int tiles = extract_tiles(g);
+    const int64_t blocks = (int64_t)g.n * tiles;
+    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "noalloc backward: too many blocks");
+    cudaStream_t st = as_stream(stream);
+    const float2* v = (const float2*)volume_rfft;
+    const float2* gr = (const float2*)grad_slices;
+    float2* dv = (float2*)grad_volume;
+    if (!grad_rotation) {
+        // the volume gradient alone needs no scratch
+        extract_bwd_kernel<true, false><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr, dv,
+                                                                                   nullptr, g, tiles);
+        return check_launch("extract_bwd_kernel");
+    }
+    const size_t need = tt_extract_backward_workspace_bytes(p);
+    if (need > (size_t)TT_NOALLOC_SCRATCH_BYTES)
+        return fail(TT_ERR_INVALID,
+                    "noalloc backward: %lld slices of %lld x %lld need %zu bytes of scratch, more than the "
+                    "%u-byte built-in array; split the slices into smaller calls or use "
+                    "tt_extract_central_slices_rfft_3d_backward with a workspace",
+                    (long long)p->n, (long long)p->img_h, (long long)(p->img_w / 2 + 1), need,
+                    (unsigned)TT_NOALLOC_SCRATCH_BYTES);
+    float* part = nullptr;
+    if (int e = noalloc_scratch(&part)) return e;
+    if (grad_volume)
+        extract_bwd_kernel<true, true><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr, dv,
+                                                                                  part, g, tiles);
+    else
+        extract_bwd_kernel<false, true><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr,
+                                                                                   dv, part, g, tiles);
+    if (int e = check_launch("extract_bwd_kernel")) return e;
+    const int64_t total = (int64_t)g.n * 9;
+    drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rotation_matrices, grad_rotation, g,
+                                                                      tiles);
+    return check_launch("drot_finish_kernel");
 }
