@@ -114,9 +114,10 @@ int tt_extract_central_slices_rfft_3d_backward(const void *volume_rfft,
  * fixed memory budget that must not grow): it takes no workspace and calls no
  * allocator; the rotation-gradient partial sums go to a 4 MiB array built
  * into the library instead.
- *  - Limit: when grad_rotation is requested, n * ceil(img_h * (img_w/2+1) / 256)
- *    * 24 bytes must not exceed TT_NOALLOC_SCRATCH_BYTES (at a 256^3 box that is
- *    1354 slices per call); larger calls fail with TT_ERR_INVALID and a message.
+ *  - Limit: when grad_rotation is requested, n * ceil((img_w/2+1) / 8) *
+ *    ceil(img_h / 32) * 24 bytes (the per-tile partial sums) must not exceed
+ *    TT_NOALLOC_SCRATCH_BYTES (at a 256^3 box that is 1285 slices per call);
+ *    larger calls fail with TT_ERR_INVALID and a message.
  *  - The first call on each device looks up the array's device address
  *    (cudaGetSymbolAddress) with that device current; make it before any
  *    stream capture.
@@ -129,18 +130,34 @@ int tt_extract_central_slices_rfft_3d_backward_noalloc(const void *volume_rfft,
                                                        void *grad_volume, void *grad_rotation,
                                                        const tt_slice_params *p, void *stream);
 
-/* Central-slice insertion, splat stage: trilinear scatter of the slices and of
- * the interpolation weights into volume_rfft / weights (both ACCUMULATED into),
- * with the reference's strict x<0 conjugate redirect, the x=0/y<0 source-pixel
- * exclusion and whole-point bounds rejection.  The Friedel mirror of the x=0
- * plane is NOT applied here: call tt_friedel_mirror_x0 once after the last
- * splat into a volume.  complex128 = 1: image/volume complex128 and weights
- * float64 (coordinates and weights still computed in float32, as the
- * reference does); else complex64 / float32.
- * Replaces _insert_central_slices_rfft_3d.py:9-106 and :213-346. */
+/* Central-slice insertion: trilinear scatter of the slices and of the
+ * interpolation weights with the reference's strict x<0 conjugate redirect,
+ * the x=0/y<0 source-pixel exclusion and whole-point bounds rejection, then
+ * the Friedel completion of the x=0 plane.  volume_rfft (vol_d, vol_h, vol_w)
+ * and weights (same dims) are OVERWRITTEN.  complex128 = 1: image/volume
+ * complex128 and weights float64 (coordinates and weights still computed in
+ * float32, as the reference does); else complex64 / float32.  The workspace
+ * holds the accumulator (tt_insert_accumulator_bytes(complex128, 1, ...)).
+ * Replaces insert_central_slices_rfft_3d, _insert_central_slices_rfft_3d.py:9-106, :213-406. */
 int tt_insert_central_slices_rfft_3d(const void *image_rfft, int32_t complex128,
                                      const void *rotation_matrices, void *volume_rfft,
-                                     void *weights, const tt_slice_params *p, void *stream);
+                                     void *weights, void *workspace, size_t workspace_bytes,
+                                     const tt_slice_params *p, void *stream);
+
+/* Bytes of an insertion accumulator for `channels` volumes of (d, h, w_rfft):
+ * one (re, im, w, pad) slot per voxel, 16 bytes (complex64) or 32 (complex128). */
+size_t tt_insert_accumulator_bytes(int32_t complex128, int64_t channels, int64_t d, int64_t h,
+                                   int64_t w_rfft);
+
+/* Two-stage insertion for accumulating many batches into one volume:
+ * tt_insert_accumulate adds the splat of n slices into a caller-zeroed
+ * accumulator (no Friedel completion); call it any number of times, then
+ * tt_insert_finalize once to write volume (channels, d, h, w_rfft) and
+ * weights (d, h, w_rfft, may be NULL) with the x=0 plane completed. */
+int tt_insert_accumulate(const void *image_rfft, int32_t complex128, const void *rotation_matrices,
+                         void *accumulator, const tt_slice_params *p, void *stream);
+int tt_insert_finalize(const void *accumulator, int32_t complex128, int64_t channels, int64_t d,
+                       int64_t h, int64_t w_rfft, void *volume_rfft, void *weights, void *stream);
 
 /* Friedel completion of the x=0 plane, equal to the reference's per-corner
  * mirror insertion (_insert_central_slices_rfft_3d.py:350-404):
@@ -192,11 +209,10 @@ int tt_pad_fftshift_2d(const void *images, int32_t is_f64, int64_t m, int64_t d,
                        void *out, void *stream);
 
 /* Friedel completion + division by max(weights, 1) + ifftshift along (d, h)
- * of `channels` splatted (not yet mirrored) rfft volumes sharing one weight
- * volume (backproject.py:66-79).  out must not alias volume_acc. */
-int tt_backproject_normalize(const void *volume_acc, const void *weights, int32_t complex128,
-                             int64_t channels, int64_t d, int64_t h, int64_t w_rfft, void *out,
-                             void *stream);
+ * of `channels` insertion accumulators (tt_insert_accumulate, not finalized)
+ * into complex volumes out (channels, d, h, w_rfft) (backproject.py:66-79). */
+int tt_backproject_normalize(const void *accumulator, int32_t complex128, int64_t channels,
+                             int64_t d, int64_t h, int64_t w_rfft, void *out, void *stream);
 
 /* out (channels, n0-2*pad, n1-2*pad, n2-2*pad) = crop(ifftshift(volume) /
  * sinc(|f|)^2) of the irfft output volumes (channels, n0, n1, n2), the sinc

@@ -50,7 +50,10 @@ SIGNATURES = {
     "tt_extract_central_slices_rfft_3d_backward_noalloc": (
         [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_central_slices_rfft_3d": (
-        [_vp, _i32, _vp, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+        [_vp, _i32, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_insert_accumulator_bytes": ([_i32, _i64, _i64, _i64, _i64], _sz),
+    "tt_insert_accumulate": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_insert_finalize": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp, _vp], _i32),
     "tt_friedel_mirror_x0": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp], _i32),
     "tt_sample_image_3d": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i32, _vp], _i32),
     "tt_insert_into_image_3d": (
@@ -58,7 +61,7 @@ SIGNATURES = {
     "tt_project_prepare": ([_vp, _i32, _i64, _i64, _vp, _vp], _i32),
     "tt_recentre_crop_2d": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp], _i32),
     "tt_pad_fftshift_2d": ([_vp, _i32, _i64, _i64, _i64, _vp, _vp], _i32),
-    "tt_backproject_normalize": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp], _i32),
+    "tt_backproject_normalize": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp], _i32),
     "tt_backproject_finish": ([_vp, _i32, _i64, _i64, _i64, _i64, _i64, _vp, _vp], _i32),
 }
 

@@ -23,7 +23,7 @@
 
 namespace tt {
 
-constexpr int kExtractThreads = 256;
+constexpr int kExtractThreads = kTileThreads;
 
 struct Corners {
     int z0, y0, x0;
@@ -63,10 +63,8 @@ extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     const int tile = blockIdx.x - (int)(s * tiles);
     load_rotation(m, rot, s, g, true);
     __syncthreads();
-    const int P = g.img_h * g.wr;
-    const int pix = tile * kExtractThreads + threadIdx.x;
-    if (pix >= P) return;
-    const int iy = pix / g.wr, ix = pix - iy * g.wr;
+    int iy, ix;
+    if (!tile_pixel(g, tile, iy, ix)) return;
     const float qy = shifted_freq(iy, g.img_h, g.inv_h);
     const float qx = __fmul_rn((float)ix, g.inv_w);
     float2 r = make_float2(0.0f, 0.0f);
@@ -106,7 +104,8 @@ extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
             if (cj) r.y = -r.y;
         }
     }
-    out[(s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix] = r;
+    // streaming store: the slices are written once and must not evict the volume from L2
+    __stcs(out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, r);
 }
 
 // Backward.  WANT_DV: scatter into dvol; WANT_DR: per-block partial sums of
@@ -123,11 +122,10 @@ extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     const int tile = blockIdx.x - (int)(s * tiles);
     load_rotation(m, rot, s, g, true);
     __syncthreads();
-    const int P = g.img_h * g.wr;
-    const int pix = tile * kExtractThreads + threadIdx.x;
+    int iy, ix;
+    const bool have = tile_pixel(g, tile, iy, ix);
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (pix < P) {
-        const int iy = pix / g.wr, ix = pix - iy * g.wr;
+    if (have) {
         const float qy = shifted_freq(iy, g.img_h, g.inv_h);
         const float qx = __fmul_rn((float)ix, g.inv_w);
         if (in_fmax(g, qy, qx)) {
@@ -141,7 +139,7 @@ extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
             }
             to_dft_coords(g, p, c);
             if (inside_volume(g, c)) {
-                float2 gv = grad[(s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix];
+                float2 gv = __ldcs(grad + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
                 if (cj) gv.y = -gv.y;
                 Corners k = make_corners(g, c);
                 float dz = 0.f, dy = 0.f, dx = 0.f;
@@ -240,13 +238,11 @@ __global__ void slice_geometry_kernel(const void* __restrict__ rot, uint8_t* __r
     const int tile = blockIdx.x - (int)(s * tiles);
     load_rotation(m, rot, s, g, mode == 0);
     __syncthreads();
-    const int P = g.img_h * g.wr;
-    const int pix = tile * kExtractThreads + threadIdx.x;
-    if (pix >= P) return;
-    const int iy = pix / g.wr, ix = pix - iy * g.wr;
+    int iy, ix;
+    if (!tile_pixel(g, tile, iy, ix)) return;
     const float qy = shifted_freq(iy, g.img_h, g.inv_h);
     const float qx = __fmul_rn((float)ix, g.inv_w);
-    const int64_t o = s * P + pix;
+    const int64_t o = (s * g.img_h + iy) * (int64_t)g.wr + ix;
     uint8_t f = 0;
     float c[3] = {0.f, 0.f, 0.f};
     bool valid = in_fmax(g, qy, qx);
@@ -270,8 +266,7 @@ __global__ void slice_geometry_kernel(const void* __restrict__ rot, uint8_t* __r
 }
 
 static int extract_tiles(const SliceGeom& g) {
-    const int P = g.img_h * g.wr;
-    return (P + kExtractThreads - 1) / kExtractThreads;
+    return tiles_per_slice(g.img_h, g.wr);
 }
 
 }  // namespace tt
@@ -310,8 +305,7 @@ extern "C" int tt_slice_geometry(const void* rotation_matrices, int32_t mode, ui
 
 extern "C" size_t tt_extract_backward_workspace_bytes(const tt_slice_params* p) {
     if (!p || p->n <= 0 || p->img_h < 1 || p->img_w < 1) return 0;
-    const int64_t P = p->img_h * (p->img_w / 2 + 1);
-    const int64_t tiles = (P + kExtractThreads - 1) / kExtractThreads;
+    const int64_t tiles = tiles_per_slice((int)p->img_h, (int)(p->img_w / 2 + 1));
     return (size_t)(p->n * tiles * 6 * sizeof(float));
 }
 

@@ -2,19 +2,22 @@
 // volume (insert_central_slices_rfft_3d, _insert_central_slices_rfft_3d.py:9-106,
 // _insert_into_3d_dft :213-286, _insert_into_3d_dft_linear :289-406).
 //
-// Splat stage: one thread per source pixel.  Pixels outside fftfreq_max and
-// the Friedel-redundant half of the x=0 column (x == 0 and y < 0) are skipped;
-// the rotated frequency is redirected (conjugating the data) when x' < 0;
-// points with any array coordinate outside [0, n-1] are dropped whole; the
-// eight floor/ceil corners receive data*w and w with the reference's float32
-// weights ((1-t) and t products, left to right).
+// Accumulate stage: one thread per source pixel, 8 x 32 pixel tiles per block
+// (warp = 8 x 4 patch, so a warp's corners stay close in the volume).  Pixels
+// outside fftfreq_max and the Friedel-redundant half of the x=0 column
+// (x == 0 and y < 0) are skipped; the rotated frequency is redirected
+// (conjugating the data) when x' < 0; points with any array coordinate outside
+// [0, n-1] are dropped whole; the eight floor/ceil corners receive data*w and w
+// with the reference's float32 weights ((1-t) and t products, left to right).
+// Data and weight of a voxel share one 16-byte accumulator slot
+// (re, im, w, 0) so each corner costs one vector reduction in L2 instead of
+// two; complex128 uses a 32-byte (re, im, w, 0) double slot.
 //
-// Mirror stage: the reference also inserts conj(data)*w at ((d-z)%d, (h-y)%h, 0)
+// Finalize stage: the reference also inserts conj(data)*w at ((d-z)%d, (h-y)%h, 0)
 // for every corner that lands on the x=0 plane except the DC voxel.  Summed
 // over all points that equals, per plane voxel v with partner m(v),
 //   out[v] = acc[v] + conj(acc[m(v)])   unless m(v) is the DC voxel,
-// which one pass over the plane applies after the last splat (m is an
-// involution, so each thread owns the pair {v, m(v)}).
+// applied while splitting the accumulator into the volume and weight arrays.
 #include <cuda_runtime.h>
 
 #include "capi_util.cuh"
@@ -22,49 +25,49 @@
 
 namespace tt {
 
-constexpr int kInsertThreads = 256;
-
 template <typename R>
-struct cplx;
+struct Acc;
 template <>
-struct cplx<float> {
-    using T = float2;
+struct Acc<float> {
+    using T = float4;
+    using C = float2;
 };
 template <>
-struct cplx<double> {
-    using T = double2;
+struct Acc<double> {
+    using T = double4;
+    using C = double2;
 };
 
-__device__ __forceinline__ void accumulate(float2* vol, float* w, int64_t i, float re, float im, float wt) {
-    atomicAdd(vol + i, make_float2(re, im));
-    atomicAdd(w + i, wt);
+__device__ __forceinline__ void acc_add(float4* a, float re, float im, float w) {
+    atomicAdd(a, make_float4(re, im, w, 0.0f));
 }
-__device__ __forceinline__ void accumulate(double2* vol, double* w, int64_t i, double re, double im, double wt) {
-    atomicAdd(&vol[i].x, re);
-    atomicAdd(&vol[i].y, im);
-    atomicAdd(w + i, wt);
+__device__ __forceinline__ void acc_add(double4* a, double re, double im, double w) {
+    atomicAdd(&a->x, re);
+    atomicAdd(&a->y, im);
+    atomicAdd(&a->z, w);
 }
 
+__device__ __forceinline__ float2 load_slice(const float2* p) { return __ldcs(p); }
+__device__ __forceinline__ double2 load_slice(const double2* p) { return __ldcs(p); }
+
 template <typename R>
-__global__ void __launch_bounds__(kInsertThreads)
-insert_splat_kernel(const typename cplx<R>::T* __restrict__ img, const void* __restrict__ rot,
-                    typename cplx<R>::T* __restrict__ vol, R* __restrict__ wts, SliceGeom g, int tiles) {
+__global__ void __launch_bounds__(kTileThreads)
+insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void* __restrict__ rot,
+                         typename Acc<R>::T* __restrict__ acc, SliceGeom g, int tiles) {
     __shared__ float m[9];
     const int64_t s = blockIdx.x / tiles;
     const int tile = blockIdx.x - (int)(s * tiles);
     if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
     __syncthreads();
-    const int P = g.img_h * g.wr;
-    const int pix = tile * kInsertThreads + threadIdx.x;
-    if (pix >= P) return;
-    const int iy = pix / g.wr, ix = pix - iy * g.wr;
+    int iy, ix;
+    if (!tile_pixel(g, tile, iy, ix)) return;
     const float qy = shifted_freq(iy, g.img_h, g.inv_h);
     const float qx = __fmul_rn((float)ix, g.inv_w);
     if (!in_fmax(g, qy, qx)) return;
     if (qx == 0.0f && qy < 0.0f) return;  // Friedel-redundant source pixel
     float p[3], c[3];
     rotate_slice_point(m, qy, qx, p);
-    const typename cplx<R>::T d = img[(s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix];
+    const typename Acc<R>::C d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
     R dre = d.x, dim = d.y;
     if (p[2] < 0.0f) {
         p[0] = -p[0];
@@ -88,14 +91,46 @@ insert_splat_kernel(const typename cplx<R>::T* __restrict__ img, const void* __r
         if (w == 0.0f) continue;  // adds nothing (ceil == floor or zero fraction)
         const int64_t vi = vox_index(g, bz ? iz1 : iz0, by ? iy1 : iy0, bx ? ix1 : ix0);
         const R rw = (R)w;
-        accumulate(vol, wts, vi, dre * rw, dim * rw, rw);
+        acc_add(acc + vi, dre * rw, dim * rw, rw);
     }
 }
 
-// Friedel completion of the x=0 plane (see file comment).  `vol` holds
-// `channels` volumes of (d, h, w) complex; `wts` one (d, h, w) weight volume.
+// Accumulator -> (volume, weights) with the Friedel completion of the x=0
+// plane.  `channels` accumulators of (d, h, w); the weights come from channel 0
+// (every channel carries the same weights).
 template <typename R>
-__global__ void mirror_x0_kernel(typename cplx<R>::T* __restrict__ vol, R* __restrict__ wts, int64_t channels,
+__global__ void insert_finalize_kernel(const typename Acc<R>::T* __restrict__ acc,
+                                       typename Acc<R>::C* __restrict__ vol, R* __restrict__ wts, int64_t channels,
+                                       int d, int h, int w) {
+    const int64_t per = (int64_t)d * h * w;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= channels * per) return;
+    const int64_t ch = idx / per, r = idx - ch * per;
+    const typename Acc<R>::T a = acc[idx];
+    R re = a.x, im = a.y, wt = a.z;
+    const int x = (int)(r % w);
+    if (x == 0) {
+        const int64_t zy = r / w;
+        const int z = (int)(zy / h), y = (int)(zy % h);
+        const int zm = (d - z) % d, ym = (h - y) % h;
+        if (!(zm == d / 2 && ym == h / 2)) {
+            const typename Acc<R>::T b = acc[ch * per + ((int64_t)zm * h + ym) * w];
+            re += b.x;
+            im -= b.y;
+            wt += b.z;
+        }
+    }
+    typename Acc<R>::C o;
+    o.x = re;
+    o.y = im;
+    vol[idx] = o;
+    if (ch == 0 && wts) wts[r] = wt;
+}
+
+// Friedel completion of the x=0 plane of already split volumes, in place
+// (kept for callers that accumulate into (volume, weights) themselves).
+template <typename R>
+__global__ void mirror_x0_kernel(typename Acc<R>::C* __restrict__ vol, R* __restrict__ wts, int64_t channels,
                                  int d, int h, int w) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)d * h) return;
@@ -107,18 +142,18 @@ __global__ void mirror_x0_kernel(typename cplx<R>::T* __restrict__ vol, R* __res
     const bool u_dc = (zm == d / 2) && (ym == h / 2);
     const int64_t plane = (int64_t)d * h * w;
     for (int64_t ch = 0; ch < channels; ch++) {
-        typename cplx<R>::T* base = vol + ch * plane;
-        const typename cplx<R>::T a = base[idx * w];
+        typename Acc<R>::C* base = vol + ch * plane;
+        const typename Acc<R>::C a = base[idx * w];
         if (u == idx) {
             if (!u_dc) {
-                typename cplx<R>::T o;
+                typename Acc<R>::C o;
                 o.x = a.x + a.x;
                 o.y = a.y - a.y;
                 base[idx * w] = o;
             }
         } else {
-            const typename cplx<R>::T b = base[u * w];
-            typename cplx<R>::T oa = a, ob = b;
+            const typename Acc<R>::C b = base[u * w];
+            typename Acc<R>::C oa = a, ob = b;
             if (!u_dc) {
                 oa.x = a.x + b.x;
                 oa.y = a.y - b.y;
@@ -143,33 +178,85 @@ __global__ void mirror_x0_kernel(typename cplx<R>::T* __restrict__ vol, R* __res
     }
 }
 
+static int check_insert_params(const tt_slice_params* p) {
+    if (int e = validate_params(p)) return e;
+    if (p->vol_d != p->img_d || p->vol_h != p->img_h || p->vol_w != p->img_w / 2 + 1)
+        return fail(TT_ERR_INVALID, "insert: volume dims (%lld, %lld, %lld) are not the rfft of volume_shape",
+                    (long long)p->vol_d, (long long)p->vol_h, (long long)p->vol_w);
+    return TT_OK;
+}
+
+int launch_insert_accumulate(const void* image_rfft, int32_t complex128, const void* rot, void* acc,
+                             const tt_slice_params* p, cudaStream_t st) {
+    SliceGeom g = make_geom(*p);
+    const int tiles = tiles_per_slice(g.img_h, g.wr);
+    const int64_t blocks = (int64_t)g.n * tiles;
+    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert: too many blocks");
+    if (complex128)
+        insert_accumulate_kernel<double><<<(unsigned)blocks, kTileThreads, 0, st>>>(
+            (const double2*)image_rfft, rot, (double4*)acc, g, tiles);
+    else
+        insert_accumulate_kernel<float><<<(unsigned)blocks, kTileThreads, 0, st>>>(
+            (const float2*)image_rfft, rot, (float4*)acc, g, tiles);
+    return check_launch("insert_accumulate_kernel");
+}
+
+int launch_insert_finalize(const void* acc, int32_t complex128, int64_t channels, int64_t d, int64_t h, int64_t w,
+                           void* volume, void* weights, cudaStream_t st) {
+    const int64_t total = channels * d * h * w;
+    const unsigned blocks = (unsigned)((total + 255) / 256);
+    if (complex128)
+        insert_finalize_kernel<double><<<blocks, 256, 0, st>>>((const double4*)acc, (double2*)volume,
+                                                               (double*)weights, channels, (int)d, (int)h, (int)w);
+    else
+        insert_finalize_kernel<float><<<blocks, 256, 0, st>>>((const float4*)acc, (float2*)volume, (float*)weights,
+                                                              channels, (int)d, (int)h, (int)w);
+    return check_launch("insert_finalize_kernel");
+}
+
 }  // namespace tt
 
 using namespace tt;
 
+extern "C" size_t tt_insert_accumulator_bytes(int32_t complex128, int64_t channels, int64_t d, int64_t h,
+                                              int64_t w_rfft) {
+    if (channels < 1 || d < 1 || h < 1 || w_rfft < 1) return 0;
+    return (size_t)(channels * d * h * w_rfft) * (complex128 ? sizeof(double4) : sizeof(float4));
+}
+
+extern "C" int tt_insert_accumulate(const void* image_rfft, int32_t complex128, const void* rotation_matrices,
+                                    void* accumulator, const tt_slice_params* p, void* stream) {
+    if (int e = check_insert_params(p)) return e;
+    if (p->n == 0) return TT_OK;
+    if (!image_rfft || !rotation_matrices || !accumulator)
+        return fail(TT_ERR_INVALID, "insert_accumulate: NULL pointer argument");
+    return launch_insert_accumulate(image_rfft, complex128, rotation_matrices, accumulator, p, as_stream(stream));
+}
+
+extern "C" int tt_insert_finalize(const void* accumulator, int32_t complex128, int64_t channels, int64_t d, int64_t h,
+                                  int64_t w_rfft, void* volume_rfft, void* weights, void* stream) {
+    if (!accumulator || !volume_rfft) return fail(TT_ERR_INVALID, "insert_finalize: NULL pointer argument");
+    if (channels < 1 || d < 1 || h < 1 || w_rfft < 1) return fail(TT_ERR_INVALID, "insert_finalize: bad dims");
+    return launch_insert_finalize(accumulator, complex128, channels, d, h, w_rfft, volume_rfft, weights,
+                                  as_stream(stream));
+}
+
 extern "C" int tt_insert_central_slices_rfft_3d(const void* image_rfft, int32_t complex128,
                                                 const void* rotation_matrices, void* volume_rfft, void* weights,
-                                                const tt_slice_params* p, void* stream) {
-    if (int e = validate_params(p)) return e;
-    if (p->n == 0) return TT_OK;
-    if (!image_rfft || !rotation_matrices || !volume_rfft || !weights)
+                                                void* workspace, size_t workspace_bytes, const tt_slice_params* p,
+                                                void* stream) {
+    if (int e = check_insert_params(p)) return e;
+    if (!volume_rfft || !weights || (p->n > 0 && (!image_rfft || !rotation_matrices)))
         return fail(TT_ERR_INVALID, "insert: NULL pointer argument");
-    if (p->vol_d != p->img_d || p->vol_h != p->img_h || p->vol_w != p->img_w / 2 + 1)
-        return fail(TT_ERR_INVALID, "insert: volume dims (%lld, %lld, %lld) are not the rfft of volume_shape",
-                    (long long)p->vol_d, (long long)p->vol_h, (long long)p->vol_w);
-    SliceGeom g = make_geom(*p);
-    const int P = g.img_h * g.wr;
-    const int tiles = (P + kInsertThreads - 1) / kInsertThreads;
-    const int64_t blocks = (int64_t)g.n * tiles;
-    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert: too many blocks");
+    const size_t need = tt_insert_accumulator_bytes(complex128, 1, p->vol_d, p->vol_h, p->vol_w);
+    if (!workspace || workspace_bytes < need)
+        return fail(TT_ERR_WORKSPACE, "insert: workspace of %zu bytes needed, got %zu", need, workspace_bytes);
     cudaStream_t st = as_stream(stream);
-    if (complex128)
-        insert_splat_kernel<double><<<(unsigned)blocks, kInsertThreads, 0, st>>>(
-            (const double2*)image_rfft, rotation_matrices, (double2*)volume_rfft, (double*)weights, g, tiles);
-    else
-        insert_splat_kernel<float><<<(unsigned)blocks, kInsertThreads, 0, st>>>(
-            (const float2*)image_rfft, rotation_matrices, (float2*)volume_rfft, (float*)weights, g, tiles);
-    return check_launch("insert_splat_kernel");
+    cudaError_t e = cudaMemsetAsync(workspace, 0, need, st);
+    if (e != cudaSuccess) return fail(TT_ERR_CUDA, "insert: memset: %s", cudaGetErrorString(e));
+    if (p->n > 0)
+        if (int r = launch_insert_accumulate(image_rfft, complex128, rotation_matrices, workspace, p, st)) return r;
+    return launch_insert_finalize(workspace, complex128, 1, p->vol_d, p->vol_h, p->vol_w, volume_rfft, weights, st);
 }
 
 extern "C" int tt_friedel_mirror_x0(void* volume_rfft, void* weights, int32_t complex128, int64_t channels,

@@ -149,6 +149,27 @@ __device__ __forceinline__ int slice_row(const SliceGeom& g, int iy) {
     return r < 0 ? r + g.img_h : r;
 }
 
+// Slice pixels are processed in 8 (x) x 32 (y) tiles of 256 threads; each warp
+// takes an 8 x 4 patch so that its 32 points, and their volume corners, stay
+// close together (fewer cache lines per warp-wide gather or reduction).
+constexpr int kTileX = 8, kTileY = 32, kTileThreads = kTileX * kTileY;
+
+__host__ __device__ inline int tiles_x_of(int wr) { return (wr + kTileX - 1) / kTileX; }
+__host__ __device__ inline int tiles_per_slice(int img_h, int wr) {
+    return tiles_x_of(wr) * ((img_h + kTileY - 1) / kTileY);
+}
+
+// Pixel (iy, ix) of this thread in tile `tile` of a slice; false when the
+// tile overhangs the slice.
+__device__ __forceinline__ bool tile_pixel(const SliceGeom& g, int tile, int& iy, int& ix) {
+    const int tx_tiles = tiles_x_of(g.wr);
+    const int ty = tile / tx_tiles, tx = tile - ty * tx_tiles;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    ix = tx * kTileX + (lane & 7);
+    iy = ty * kTileY + warp * 4 + (lane >> 3);
+    return ix < g.wr && iy < g.img_h;
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -82,18 +82,20 @@ struct C2;
 template <>
 struct C2<float> {
     using T = float2;
+    using A = float4;
 };
 template <>
 struct C2<double> {
     using T = double2;
+    using A = double4;
 };
 
-// Backprojection normalisation of `channels` accumulated (pre-mirror)
-// fftshifted rfft volumes (d, h, w) sharing one weight volume:
-// Friedel completion of the x=0 plane, division by max(weights, 1), written
-// ifftshifted along (d, h) for the 3D irfft.
+// Backprojection normalisation of `channels` insertion accumulators
+// ((re, im, w, 0) slots of fftshifted rfft volumes (d, h, w); every channel
+// carries the same weights): Friedel completion of the x=0 plane, division by
+// max(weights, 1), written ifftshifted along (d, h) for the 3D irfft.
 template <typename R>
-__global__ void normalize_unshift_kernel(const typename C2<R>::T* __restrict__ acc, const R* __restrict__ wts,
+__global__ void normalize_unshift_kernel(const typename C2<R>::A* __restrict__ acc,
                                          typename C2<R>::T* __restrict__ out, int64_t channels, int64_t d,
                                          int64_t h, int64_t w) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -103,22 +105,22 @@ __global__ void normalize_unshift_kernel(const typename C2<R>::T* __restrict__ a
     const int64_t i = r / (h * w), j = (r / w) % h, k = r % w;
     const int64_t z = wrap(i + d / 2, d), y = wrap(j + h / 2, h);  // source (shifted) voxel
     const int64_t src = (z * h + y) * w + k;
-    typename C2<R>::T v = acc[ch * per + src];
-    R wt = wts[src];
+    const typename C2<R>::A a = acc[ch * per + src];
+    R re = a.x, im = a.y, wt = a.z;
     if (k == 0) {
         const int64_t zm = (d - z) % d, ym = (h - y) % h;
         const bool m_dc = (zm == d / 2) && (ym == h / 2);
         if (!m_dc) {
-            const int64_t ms = (zm * h + ym) * w;
-            const typename C2<R>::T u = acc[ch * per + ms];
-            v.x += u.x;
-            v.y -= u.y;
-            wt += wts[ms];
+            const typename C2<R>::A u = acc[ch * per + (zm * h + ym) * w];
+            re += u.x;
+            im -= u.y;
+            wt += u.z;
         }
     }
     const R den = wt < (R)1 ? (R)1 : wt;
-    v.x /= den;
-    v.y /= den;
+    typename C2<R>::T v;
+    v.x = re / den;
+    v.y = im / den;
     out[idx] = v;
 }
 
@@ -185,19 +187,18 @@ extern "C" int tt_pad_fftshift_2d(const void* images, int32_t is_f64, int64_t m,
     return check_launch("pad_fftshift_2d_kernel");
 }
 
-extern "C" int tt_backproject_normalize(const void* volume_acc, const void* weights, int32_t complex128,
-                                        int64_t channels, int64_t d, int64_t h, int64_t w_rfft, void* out,
-                                        void* stream) {
-    if (!volume_acc || !weights || !out || channels < 1 || d < 1 || h < 1 || w_rfft < 1)
+extern "C" int tt_backproject_normalize(const void* accumulator, int32_t complex128, int64_t channels, int64_t d,
+                                        int64_t h, int64_t w_rfft, void* out, void* stream) {
+    if (!accumulator || !out || channels < 1 || d < 1 || h < 1 || w_rfft < 1)
         return fail(TT_ERR_INVALID, "backproject_normalize: bad arguments");
-    if (volume_acc == out) return fail(TT_ERR_INVALID, "backproject_normalize: out must not alias the input");
+    if (accumulator == out) return fail(TT_ERR_INVALID, "backproject_normalize: out must not alias the input");
     const int64_t total = channels * d * h * w_rfft;
     if (complex128)
         normalize_unshift_kernel<double><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
-            (const double2*)volume_acc, (const double*)weights, (double2*)out, channels, d, h, w_rfft);
+            (const double4*)accumulator, (double2*)out, channels, d, h, w_rfft);
     else
         normalize_unshift_kernel<float><<<blocks_for(total, 256), 256, 0, as_stream(stream)>>>(
-            (const float2*)volume_acc, (const float*)weights, (float2*)out, channels, d, h, w_rfft);
+            (const float4*)accumulator, (float2*)out, channels, d, h, w_rfft);
     return check_launch("normalize_unshift_kernel");
 }
 

@@ -94,16 +94,16 @@ def pad_fftshift_2d(images: torch.Tensor, pad: int) -> torch.Tensor:
     return out
 
 
-def backproject_normalize(volume_acc: torch.Tensor, weights: torch.Tensor) -> torch.Tensor:
-    """Mirror + divide by max(w, 1) + ifftshift(d, h) of (c?, d, h, w) volumes."""
-    d, h, w = volume_acc.shape[-3:]
-    channels = volume_acc.numel() // (d * h * w)
-    out = torch.empty_like(volume_acc)
+def backproject_normalize(acc: torch.Tensor) -> torch.Tensor:
+    """Insertion accumulator (c, d, h, w, 4) -> Friedel completion, division by
+    max(w, 1) and ifftshift(d, h): complex volumes (c, d, h, w)."""
+    c, d, h, w = acc.shape[:4]
+    c128 = acc.dtype == torch.float64
+    out = torch.empty((c, d, h, w), dtype=torch.complex128 if c128 else torch.complex64,
+                      device=acc.device)
     L = _lib.load()
-    _lib.check(L.tt_backproject_normalize(_lib.ptr(volume_acc), _lib.ptr(weights),
-                                          int(volume_acc.dtype == torch.complex128), channels,
-                                          d, h, w, _lib.ptr(out),
-                                          _lib.stream_of(volume_acc.device)),
+    _lib.check(L.tt_backproject_normalize(_lib.ptr(acc), int(c128), c, d, h, w, _lib.ptr(out),
+                                          _lib.stream_of(acc.device)),
                "backproject_normalize")
     return out
 

@@ -14,8 +14,8 @@ import torch
 
 from .. import _lib
 from . import _wrappers
-from ._params import rfft_shape, rotation_arg
-from .slice_insertion import insert_splat
+from ._params import rotation_arg
+from .slice_insertion import insert_accumulate, new_accumulator
 
 
 def _pad_amount(n: int, pad_factor: float) -> int:
@@ -44,17 +44,11 @@ def _backproject(images, rotation_matrices, pad_factor, fftfreq_max, zyx_matrice
     fft_in = _wrappers.pad_fftshift_2d(flat, p)
     spec = torch.fft.rfftn(fft_in, dim=(-2, -1)).reshape(*lead, c, n, n // 2 + 1)
     spec = spec.reshape(nrot, c, n, n // 2 + 1)
-    shape3 = rfft_shape(shape)
-    cdt = spec.dtype
-    wdt = torch.float64 if cdt == torch.complex128 else torch.float32
-    acc = torch.zeros((c, *shape3), dtype=cdt, device=dev)
-    weights = torch.zeros(shape3, dtype=wdt, device=dev)
-    scratch_w = torch.zeros(shape3, dtype=wdt, device=dev) if c > 1 else None
+    acc = new_accumulator(shape, spec.dtype == torch.complex128, dev, channels=c)
     for ch in range(c):
-        insert_splat(spec[:, ch].contiguous(), R, shape, acc[ch],
-                     weights if ch == 0 else scratch_w, fftfreq_max, zyx_matrices,
-                     images_unshifted=True)
-    dft = _wrappers.backproject_normalize(acc, weights)
+        insert_accumulate(spec[:, ch].contiguous(), R, shape, acc[ch], fftfreq_max, zyx_matrices,
+                          images_unshifted=True)
+    dft = _wrappers.backproject_normalize(acc)
     # irfftn without an output size, as the reference (odd boxes lose one x column)
     real = torch.fft.irfftn(dft, dim=(-3, -2, -1))
     out = _wrappers.backproject_finish(real, p)

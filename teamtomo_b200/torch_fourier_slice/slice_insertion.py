@@ -5,8 +5,8 @@
 torch_fourier_slice/slice_insertion/_insert_central_slices_rfft_3d.py:9-106:
 complex64 slices give a complex64 volume with float32 weights, complex128
 slices a complex128 volume with float64 weights.  The splat runs on the
-sm_100a scatter kernel; the Friedel completion of the x=0 plane is one
-post-pass over that plane.
+sm_100a scatter kernel into an (re, im, w) accumulator; one finalize pass
+applies the Friedel completion of the x=0 plane and writes the two outputs.
 """
 
 from __future__ import annotations
@@ -30,26 +30,45 @@ def _check_image(image_rfft: torch.Tensor, volume_shape):
         )
 
 
-def insert_splat(image_rfft, R, volume_shape, volume, weights, fftfreq_max=None,
-                 zyx_matrices=False, images_unshifted=False):
-    """Accumulate the trilinear splat of (n, h, w//2+1) slices into ``volume``
-    / ``weights`` (no Friedel completion)."""
-    dev = volume.device
+def new_accumulator(volume_shape, complex128: bool, device, channels: int = 1) -> torch.Tensor:
+    """Zeroed insertion accumulator: (channels, d, h, w//2+1) slots of
+    (re, im, w, pad) in float32 (complex64 data) or float64 (complex128)."""
+    d, h, w = rfft_shape(volume_shape)
+    dt = torch.float64 if complex128 else torch.float32
+    return torch.zeros((channels, d, h, w, 4), dtype=dt, device=device)
+
+
+def insert_accumulate(image_rfft, R, volume_shape, acc, fftfreq_max=None, zyx_matrices=False,
+                      images_unshifted=False):
+    """Add the trilinear splat of (n, h, w//2+1) slices into one accumulator
+    (no Friedel completion)."""
+    dev = acc.device
     # the kernels index raw memory in C order
-    if not (image_rfft.is_contiguous() and R.is_contiguous() and volume.is_contiguous()
-            and weights.is_contiguous()):
-        raise ValueError("insertion needs C-contiguous slices, rotations, volume and weights")
-    params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=volume, rotation=R,
+    if not (image_rfft.is_contiguous() and R.is_contiguous() and acc.is_contiguous()):
+        raise ValueError("insertion needs C-contiguous slices, rotations and accumulator")
+    params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=None, rotation=R,
                           fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
-                          slices_unshifted=images_unshifted)
+                          slices_unshifted=images_unshifted, vol_dims=rfft_shape(volume_shape))
     L = _lib.load()
     _lib.check(
-        L.tt_insert_central_slices_rfft_3d(_lib.ptr(image_rfft),
-                                           int(image_rfft.dtype == torch.complex128),
-                                           _lib.ptr(R), _lib.ptr(volume), _lib.ptr(weights),
-                                           params, _lib.stream_of(dev)),
+        L.tt_insert_accumulate(_lib.ptr(image_rfft), int(image_rfft.dtype == torch.complex128),
+                               _lib.ptr(R), _lib.ptr(acc), params, _lib.stream_of(dev)),
         "insert_central_slices_rfft_3d",
     )
+
+
+def insert_finalize(acc: torch.Tensor, complex128: bool):
+    """Accumulator (c, d, h, w, 4) -> volume (c, d, h, w) complex, weights (d, h, w)."""
+    c, d, h, w = acc.shape[:4]
+    cdt = torch.complex128 if complex128 else torch.complex64
+    wdt = torch.float64 if complex128 else torch.float32
+    volume = torch.empty((c, d, h, w), dtype=cdt, device=acc.device)
+    weights = torch.empty((d, h, w), dtype=wdt, device=acc.device)
+    L = _lib.load()
+    _lib.check(L.tt_insert_finalize(_lib.ptr(acc), int(complex128), c, d, h, w, _lib.ptr(volume),
+                                    _lib.ptr(weights), _lib.stream_of(acc.device)),
+               "insert_central_slices_rfft_3d finalize")
+    return volume, weights
 
 
 def friedel_mirror_x0(volume, weights):
@@ -80,16 +99,13 @@ def insert_central_slices_rfft_3d(
     n = R.shape[0]
     lead = image_rfft.shape[:-2]
     if math.prod(lead) != n:
-        raise ValueError(
-            f"{n} rotation matrices for image stack of shape {tuple(lead)}")
+        raise ValueError(f"{n} rotation matrices for image stack of shape {tuple(lead)}")
     img = image_rfft.reshape(n, *image_rfft.shape[-2:]).contiguous()
-    shape3 = rfft_shape(volume_shape)
-    volume = torch.zeros(shape3, dtype=image_rfft.dtype, device=dev)
-    wdt = torch.float64 if image_rfft.dtype == torch.complex128 else torch.float32
-    weights = torch.zeros(shape3, dtype=wdt, device=dev)
-    insert_splat(img, R, volume_shape, volume, weights, fftfreq_max, zyx_matrices)
-    friedel_mirror_x0(volume, weights)
-    return volume, weights
+    c128 = image_rfft.dtype == torch.complex128
+    acc = new_accumulator(volume_shape, c128, dev)
+    insert_accumulate(img, R, volume_shape, acc, fftfreq_max, zyx_matrices)
+    volume, weights = insert_finalize(acc, c128)
+    return volume[0], weights
 
 
 def insert_central_slices_rfft_3d_multichannel(
@@ -107,15 +123,10 @@ def insert_central_slices_rfft_3d_multichannel(
     dev = image_rfft.device
     c = image_rfft.shape[-3]
     R, stack = rotation_arg(rotation_matrices, dev)
-    shape3 = rfft_shape(volume_shape)
-    volume = torch.zeros((c, *shape3), dtype=image_rfft.dtype, device=dev)
-    wdt = torch.float64 if image_rfft.dtype == torch.complex128 else torch.float32
-    weights = torch.zeros(shape3, dtype=wdt, device=dev)
-    scratch_w = torch.zeros(shape3, dtype=wdt, device=dev)
     n = R.shape[0]
+    c128 = image_rfft.dtype == torch.complex128
+    acc = new_accumulator(volume_shape, c128, dev, channels=c)
     for ch in range(c):
         img = image_rfft[..., ch, :, :].reshape(n, *image_rfft.shape[-2:]).contiguous()
-        insert_splat(img, R, volume_shape, volume[ch], weights if ch == 0 else scratch_w,
-                     fftfreq_max, zyx_matrices)
-    friedel_mirror_x0(volume, weights)
-    return volume, weights
+        insert_accumulate(img, R, volume_shape, acc[ch], fftfreq_max, zyx_matrices)
+    return insert_finalize(acc, c128)

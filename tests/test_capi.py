@@ -73,8 +73,13 @@ def test_validation_rejects_before_launch():
     assert L.tt_extract_central_slices_rfft_3d(None, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
     assert b"NULL" in L.tt_last_error()
     p = _params(vol_w=8)  # insertion needs the rfft of volume_shape
-    assert L.tt_insert_central_slices_rfft_3d(fake, 0, fake, fake, fake, ctypes.byref(p), None) == \
-        _lib.TT_ERR_INVALID
+    assert L.tt_insert_central_slices_rfft_3d(fake, 0, fake, fake, fake, fake, 1 << 30, ctypes.byref(p),
+                                              None) == _lib.TT_ERR_INVALID
+    p = _params()
+    assert L.tt_insert_central_slices_rfft_3d(fake, 0, fake, fake, fake, fake, 16, ctypes.byref(p),
+                                              None) == _lib.TT_ERR_WORKSPACE
+    assert L.tt_insert_accumulate(fake, 0, fake, None, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert L.tt_insert_finalize(fake, 0, 0, 4, 4, 3, fake, fake, None) == _lib.TT_ERR_INVALID
     p = _params()
     assert L.tt_extract_central_slices_rfft_3d_backward(fake, fake, fake, None, fake, None, 0,
                                                         ctypes.byref(p), None) == _lib.TT_ERR_WORKSPACE
@@ -93,8 +98,10 @@ def test_workspace_query():
 
     L = _lib.load()
     p = _params(n=4096, img_d=256, img_h=256, img_w=256, vol_d=256, vol_h=256, vol_w=129)
-    tiles = (256 * 129 + 255) // 256
+    tiles = ((129 + 7) // 8) * ((256 + 31) // 32)  # 8 x 32 pixel tiles
     assert L.tt_extract_backward_workspace_bytes(ctypes.byref(p)) == 4096 * tiles * 6 * 4
+    assert L.tt_insert_accumulator_bytes(0, 1, 256, 256, 129) == 256 * 256 * 129 * 16
+    assert L.tt_insert_accumulator_bytes(1, 2, 4, 4, 3) == 2 * 4 * 4 * 3 * 32
     p = _params(n=0)
     assert L.tt_extract_backward_workspace_bytes(ctypes.byref(p)) == 0
 

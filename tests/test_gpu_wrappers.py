@@ -49,6 +49,14 @@ def test_backproject_matches_reference_golden(golden):
     rec64 = tt().backproject_2d_to_3d(imgs.double(), rot)
     assert rec64.dtype == torch.float64
     assert rel_l2(rec64.cpu().numpy(), golden["backproject_f64_out"]) < RTOL
+    # odd padded box (33 at pad 1.5 -> 49): (d, d-1) projections, (d, d, d-1) volumes
+    po = tt().project_3d_to_2d(cuda(golden["project_odd_volume"]), cuda(golden["project_rot"]), pad_factor=1.5)
+    assert tuple(po.shape) == golden["project_odd_out"].shape
+    assert rel_l2(po.cpu().numpy(), golden["project_odd_out"]) < RTOL
+    bo = tt().backproject_2d_to_3d(cuda(golden["backproject_odd_images"]), cuda(golden["project_rot"]),
+                                   pad_factor=1.5)
+    assert tuple(bo.shape) == golden["backproject_odd_out"].shape
+    assert rel_l2(bo.cpu().numpy(), golden["backproject_odd_out"]) < RTOL
 
 
 @pytest.mark.parametrize("n,pad", [(48, 2.0), (33, 1.5), (40, 1.0)])
@@ -57,9 +65,13 @@ def test_project_backproject_match_oracle(oracle, n, pad):
     rots = rotations(30, seed=n)
     p = tt().project_3d_to_2d(cuda(vol), cuda(rots), pad_factor=pad)
     ref = oracle.project_3d_to_2d(vol, rots, pad_factor=pad)
+    assert p.shape == ref.shape  # (d, d-1) for odd padded boxes, as the reference
     assert rel_l2(p.cpu().numpy(), ref) < RTOL
-    r = tt().backproject_2d_to_3d(p, cuda(rots), pad_factor=pad)
-    ref_r = oracle.backproject_2d_to_3d(ref, rots, pad_factor=pad)
+    # square images (odd-box projections are not square and are rejected, as in the reference)
+    imgs = np.random.default_rng(n).standard_normal((30, n, n)).astype(np.float32)
+    r = tt().backproject_2d_to_3d(cuda(imgs), cuda(rots), pad_factor=pad)
+    ref_r = oracle.backproject_2d_to_3d(imgs, rots, pad_factor=pad)
+    assert r.shape == ref_r.shape
     assert rel_l2(r.cpu().numpy(), ref_r) < RTOL
 
 
