@@ -1,11 +1,13 @@
 // Central-slice extraction from an fftshifted rfft volume, and its backward.
 //
 // Forward (extract_central_slices_rfft_3d, _extract_central_slices_rfft_3d.py:84-222):
-// one thread per slice pixel.  The pixel's frequency is generated in
-// registers, rotated with the reference's float32 operation order, redirected
-// into the stored half (conjugate rule with the x-tolerance tie-break), scaled
-// to array coordinates and sampled trilinearly with grid_sample's semantics
-// (padding_mode='border', align_corners=True, zero outside [0, n-1]).
+// one thread per slice pixel, 8 x 32 pixel tiles per block.  The pixel's
+// frequency is generated in registers, rotated with the reference's float32
+// operation order, redirected into the stored half (conjugate rule with the
+// x-tolerance tie-break), scaled to array coordinates and sampled trilinearly
+// with grid_sample's semantics: padding_mode='border', align_corners=True, the
+// array -> grid -> array round trip of the coordinate (it decides the cell at
+// integer kinks, where the trilinear derivative jumps), zero outside [0, n-1].
 //
 // Backward: the same per-pixel geometry, recomputed rather than stored.
 //   d/dvolume  = trilinear scatter of G' (G conjugated where the sample was)
@@ -25,25 +27,37 @@ namespace tt {
 
 constexpr int kExtractThreads = kTileThreads;
 
+// grid_sample's source index of array coordinate c on an axis of n samples:
+// c -> grid coordinate c / (0.5 n - 0.5) - 1 (grid_sample_utils.py:6-26) ->
+// ((g + 1) / 2) * (n - 1) (align_corners=True), clipped to [0, n-1].
+__device__ __forceinline__ float source_index(float c, float half, float nm1) {
+    const float gc = __fsub_rn(__fdiv_rn(c, half), 1.0f);
+    const float ix = __fmul_rn(__fmul_rn(__fadd_rn(gc, 1.0f), 0.5f), nm1);
+    return fminf(fmaxf(ix, 0.0f), nm1);
+}
+
 struct Corners {
     int z0, y0, x0;
     float ax0, ax1, ay0, ay1, az0, az1;  // per-axis weights of the low/high corner
     bool zin, yin, xin;                  // high corner inside the array
 };
 
-// grid_sample trilinear corner set for an inside coordinate c.
+// grid_sample trilinear corner set of an inside array coordinate c.
 __device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float c[3]) {
+    const float iz = source_index(c[0], 0.5f * (float)g.D - 0.5f, g.ub0);
+    const float iy = source_index(c[1], 0.5f * (float)g.H - 0.5f, g.ub1);
+    const float ix = source_index(c[2], 0.5f * (float)g.W - 0.5f, g.ub2);
     Corners k;
-    float fz = floorf(c[0]), fy = floorf(c[1]), fx = floorf(c[2]);
+    const float fz = floorf(iz), fy = floorf(iy), fx = floorf(ix);
     k.z0 = (int)fz;
     k.y0 = (int)fy;
     k.x0 = (int)fx;
-    k.az0 = (fz + 1.0f) - c[0];
-    k.az1 = c[0] - fz;
-    k.ay0 = (fy + 1.0f) - c[1];
-    k.ay1 = c[1] - fy;
-    k.ax0 = (fx + 1.0f) - c[2];
-    k.ax1 = c[2] - fx;
+    k.az0 = (fz + 1.0f) - iz;
+    k.az1 = iz - fz;
+    k.ay0 = (fy + 1.0f) - iy;
+    k.ay1 = iy - fy;
+    k.ax0 = (fx + 1.0f) - ix;
+    k.ax1 = ix - fx;
     k.zin = k.z0 + 1 < g.D;
     k.yin = k.y0 + 1 < g.H;
     k.xin = k.x0 + 1 < g.W;
@@ -53,6 +67,25 @@ __device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float 
 __device__ __forceinline__ void load_rotation(float* sm, const void* rot, int64_t s,
                                               const SliceGeom& g, bool apply_tol) {
     if (threadIdx.x < 9) sm[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, apply_tol);
+}
+
+// Geometry of one extraction pixel: false when the pixel is outside
+// fftfreq_max or its point outside the volume.
+__device__ __forceinline__ bool extract_geometry(const SliceGeom& g, const float* m, int iy, int ix, float& qy,
+                                                 float& qx, bool& cj, float c[3]) {
+    qy = shifted_freq(iy, g.img_h, g.inv_h);
+    qx = __fmul_rn((float)ix, g.inv_w);
+    if (!in_fmax(g, qy, qx)) return false;
+    float p[3];
+    rotate_slice_point(m, qy, qx, p);
+    cj = extract_conj(g, m, p[2]);
+    if (cj) {
+        p[0] = -p[0];
+        p[1] = -p[1];
+        p[2] = -p[2];
+    }
+    to_dft_coords(g, p, c);
+    return inside_volume(g, c);
 }
 
 __global__ void __launch_bounds__(kExtractThreads)
@@ -65,140 +98,145 @@ extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     __syncthreads();
     int iy, ix;
     if (!tile_pixel(g, tile, iy, ix)) return;
-    const float qy = shifted_freq(iy, g.img_h, g.inv_h);
-    const float qx = __fmul_rn((float)ix, g.inv_w);
+    float qy, qx, c[3];
+    bool cj = false;
     float2 r = make_float2(0.0f, 0.0f);
-    if (in_fmax(g, qy, qx)) {
-        float p[3], c[3];
-        rotate_slice_point(m, qy, qx, p);
-        const bool cj = extract_conj(g, m, p[2]);
-        if (cj) {
-            p[0] = -p[0];
-            p[1] = -p[1];
-            p[2] = -p[2];
-        }
-        to_dft_coords(g, p, c);
-        if (inside_volume(g, c)) {
-            Corners k = make_corners(g, c);
+    if (extract_geometry(g, m, iy, ix, qy, qx, cj, c)) {
+        const Corners k = make_corners(g, c);
 #pragma unroll
-            for (int bz = 0; bz < 2; bz++) {
-                if (bz && !k.zin) continue;
-                const float wz = bz ? k.az1 : k.az0;
+        for (int bz = 0; bz < 2; bz++) {
+            if (bz && !k.zin) continue;
+            const float wz = bz ? k.az1 : k.az0;
 #pragma unroll
-                for (int by = 0; by < 2; by++) {
-                    if (by && !k.yin) continue;
-                    const float wzy = (by ? k.ay1 : k.ay0) * wz;
-                    const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
-                    const float2 v0 = __ldg(vol + base);
-                    const float w0 = k.ax0 * wzy;
-                    r.x = fmaf(v0.x, w0, r.x);
-                    r.y = fmaf(v0.y, w0, r.y);
-                    if (k.xin) {
-                        const float2 v1 = __ldg(vol + base + 1);
-                        const float w1 = k.ax1 * wzy;
-                        r.x = fmaf(v1.x, w1, r.x);
-                        r.y = fmaf(v1.y, w1, r.y);
-                    }
+            for (int by = 0; by < 2; by++) {
+                if (by && !k.yin) continue;
+                const float wzy = (by ? k.ay1 : k.ay0) * wz;
+                const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
+                const float2 v0 = __ldg(vol + base);
+                const float w0 = k.ax0 * wzy;
+                r.x = fmaf(v0.x, w0, r.x);
+                r.y = fmaf(v0.y, w0, r.y);
+                if (k.xin) {
+                    const float2 v1 = __ldg(vol + base + 1);
+                    const float w1 = k.ax1 * wzy;
+                    r.x = fmaf(v1.x, w1, r.x);
+                    r.y = fmaf(v1.y, w1, r.y);
                 }
             }
-            if (cj) r.y = -r.y;
         }
+        if (cj) r.y = -r.y;
     }
-    // streaming store: the slices are written once and must not evict the volume from L2
+    // streaming store: the slices are written once and should not evict the volume from L2
     __stcs(out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, r);
 }
 
-// Backward.  WANT_DV: scatter into dvol; WANT_DR: per-block partial sums of
-// the 6 non-zero entries of d/dR_zyx (column 0 multiplies the zero z
-// frequency) into part[(s*tiles + tile)*6 + k].
+// Backward of one slice pixel; acc receives the pixel's 6 contributions to
+// d/dR_zyx (rows z, y, x x columns y, x — column 0 multiplies the zero z
+// frequency of a central slice).
+template <bool WANT_DV, bool WANT_DR>
+__device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const float* m,
+                                          const float2* __restrict__ grad, float2* __restrict__ dvol,
+                                          const SliceGeom& g, int64_t s, int iy, int ix, float acc[6]) {
+    float qy, qx, c[3];
+    bool cj = false;
+    if (!extract_geometry(g, m, iy, ix, qy, qx, cj, c)) return;
+    const Corners k = make_corners(g, c);
+    float2 gv = __ldcs(grad + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+    if (cj) gv.y = -gv.y;  // G' = conj(G) where the sample was conjugated
+    if (WANT_DV) {
+#pragma unroll
+        for (int bz = 0; bz < 2; bz++) {
+            if (bz && !k.zin) continue;
+            const float wz = bz ? k.az1 : k.az0;
+#pragma unroll
+            for (int by = 0; by < 2; by++) {
+                if (by && !k.yin) continue;
+                const float wzy = (by ? k.ay1 : k.ay0) * wz;
+                const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
+#pragma unroll
+                for (int bx = 0; bx < 2; bx++) {
+                    if (bx && !k.xin) continue;
+                    const float w = (bx ? k.ax1 : k.ax0) * wzy;
+                    if (w != 0.0f) atomicAdd(dvol + base + bx, make_float2(gv.x * w, gv.y * w));
+                }
+            }
+        }
+    }
+    if (WANT_DR) {
+        // trilinear gradient from differences of neighbouring voxels (subtracting
+        // first keeps it accurate where the volume varies slowly); corners past the
+        // last index read as zero, as in grid_sample
+        float2 v[2][2][2];
+#pragma unroll
+        for (int bz = 0; bz < 2; bz++)
+#pragma unroll
+            for (int by = 0; by < 2; by++) {
+                const bool row_ok = (!bz || k.zin) && (!by || k.yin);
+                const int64_t base = vox_index(g, k.z0 + (row_ok ? bz : 0), k.y0 + (row_ok ? by : 0), k.x0);
+#pragma unroll
+                for (int bx = 0; bx < 2; bx++) {
+                    const bool ok = row_ok && (!bx || k.xin);
+                    v[bz][by][bx] = ok ? __ldg(vol + base + bx) : make_float2(0.f, 0.f);
+                }
+            }
+        float2 gz = make_float2(0.f, 0.f), gy = gz, gx = gz;
+        const float wzs[2] = {k.az0, k.az1}, wys[2] = {k.ay0, k.ay1}, wxs[2] = {k.ax0, k.ax1};
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const float wyx = wys[a] * wxs[b], wzx = wzs[a] * wxs[b], wzy = wzs[a] * wys[b];
+                gz.x = fmaf(wyx, v[1][a][b].x - v[0][a][b].x, gz.x);
+                gz.y = fmaf(wyx, v[1][a][b].y - v[0][a][b].y, gz.y);
+                gy.x = fmaf(wzx, v[a][1][b].x - v[a][0][b].x, gy.x);
+                gy.y = fmaf(wzx, v[a][1][b].y - v[a][0][b].y, gy.y);
+                gx.x = fmaf(wzy, v[a][b][1].x - v[a][b][0].x, gx.x);
+                gx.y = fmaf(wzy, v[a][b][1].y - v[a][b][0].y, gx.y);
+            }
+        // Re(conj(G') dV/dc), chained through dc/dp and the redirect sign
+        const float sg = cj ? -1.f : 1.f;
+        const float p0 = fmaf(gv.x, gz.x, gv.y * gz.y) * g.dcdp0 * sg;
+        const float p1 = fmaf(gv.x, gy.x, gv.y * gy.y) * g.dcdp1 * sg;
+        const float p2 = fmaf(gv.x, gx.x, gv.y * gx.y) * g.dcdp2 * sg;
+        acc[0] = p0 * qy;
+        acc[1] = p0 * qx;
+        acc[2] = p1 * qy;
+        acc[3] = p1 * qx;
+        acc[4] = p2 * qy;
+        acc[5] = p2 * qx;
+    }
+}
+
+// One block per (slice, tile).  WANT_DR: the block's partial sums of the 6
+// non-zero entries of d/dR_zyx go to part[(s * tiles + tile) * 6 + k],
+// reduced in double within the block.
 template <bool WANT_DV, bool WANT_DR>
 __global__ void __launch_bounds__(kExtractThreads)
 extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
                    const float2* __restrict__ grad, float2* __restrict__ dvol,
                    float* __restrict__ part, SliceGeom g, int tiles) {
     __shared__ float m[9];
-    __shared__ float red[kExtractThreads / 32][6];
+    __shared__ double red[kExtractThreads / 32][6];
     const int64_t s = blockIdx.x / tiles;
     const int tile = blockIdx.x - (int)(s * tiles);
     load_rotation(m, rot, s, g, true);
     __syncthreads();
-    int iy, ix;
-    const bool have = tile_pixel(g, tile, iy, ix);
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (have) {
-        const float qy = shifted_freq(iy, g.img_h, g.inv_h);
-        const float qx = __fmul_rn((float)ix, g.inv_w);
-        if (in_fmax(g, qy, qx)) {
-            float p[3], c[3];
-            rotate_slice_point(m, qy, qx, p);
-            const bool cj = extract_conj(g, m, p[2]);
-            if (cj) {
-                p[0] = -p[0];
-                p[1] = -p[1];
-                p[2] = -p[2];
-            }
-            to_dft_coords(g, p, c);
-            if (inside_volume(g, c)) {
-                float2 gv = __ldcs(grad + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
-                if (cj) gv.y = -gv.y;
-                Corners k = make_corners(g, c);
-                float dz = 0.f, dy = 0.f, dx = 0.f;
-#pragma unroll
-                for (int bz = 0; bz < 2; bz++) {
-                    if (bz && !k.zin) continue;
-                    const float wz = bz ? k.az1 : k.az0;
-                    const float sz = bz ? 1.f : -1.f;
-#pragma unroll
-                    for (int by = 0; by < 2; by++) {
-                        if (by && !k.yin) continue;
-                        const float wy = by ? k.ay1 : k.ay0;
-                        const float sy = by ? 1.f : -1.f;
-                        const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
-#pragma unroll
-                        for (int bx = 0; bx < 2; bx++) {
-                            if (bx && !k.xin) continue;
-                            const float wx = bx ? k.ax1 : k.ax0;
-                            const float sx = bx ? 1.f : -1.f;
-                            if (WANT_DV) {
-                                const float w = wx * wy * wz;
-                                if (w != 0.0f) atomicAdd(dvol + base + bx, make_float2(gv.x * w, gv.y * w));
-                            }
-                            if (WANT_DR) {
-                                const float2 v = __ldg(vol + base + bx);
-                                const float rv = fmaf(gv.x, v.x, gv.y * v.y);
-                                dx = fmaf(rv, sx * wy * wz, dx);
-                                dy = fmaf(rv, sy * wx * wz, dy);
-                                dz = fmaf(rv, sz * wx * wy, dz);
-                            }
-                        }
-                    }
-                }
-                if (WANT_DR) {
-                    const float sg = cj ? -1.f : 1.f;
-                    const float p0 = dz * g.dcdp0 * sg, p1 = dy * g.dcdp1 * sg, p2 = dx * g.dcdp2 * sg;
-                    acc[0] = p0 * qy;
-                    acc[1] = p0 * qx;
-                    acc[2] = p1 * qy;
-                    acc[3] = p1 * qx;
-                    acc[4] = p2 * qy;
-                    acc[5] = p2 * qx;
-                }
-            }
-        }
-    }
+    int iy, ix;
+    if (tile_pixel(g, tile, iy, ix)) bwd_point<WANT_DV, WANT_DR>(vol, m, grad, dvol, g, s, iy, ix, acc);
     if (WANT_DR) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
         for (int k = 0; k < 6; k++) {
-            float v = warp_sum(acc[k]);
+            const double v = warp_sum_d((double)acc[k]);
             if (lane == 0) red[warp][k] = v;
         }
         __syncthreads();
         if (threadIdx.x < 6) {
-            float v = 0.f;
+            double v = 0.0;
 #pragma unroll
             for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][threadIdx.x];
-            part[((int64_t)s * tiles + tile) * 6 + threadIdx.x] = v;
+            part[((int64_t)s * tiles + tile) * 6 + threadIdx.x] = (float)v;
         }
     }
 }
@@ -265,8 +303,29 @@ __global__ void slice_geometry_kernel(const void* __restrict__ rot, uint8_t* __r
     coords[o * 3 + 2] = c[2];
 }
 
-static int extract_tiles(const SliceGeom& g) {
-    return tiles_per_slice(g.img_h, g.wr);
+static int extract_tiles(const SliceGeom& g) { return tiles_per_slice(g.img_h, g.wr); }
+
+static size_t partial_bytes(int64_t n, int tiles) { return (size_t)(n * tiles * 6) * sizeof(float); }
+
+// Launches the backward and the rotation-gradient reduction; `part` holds
+// n * tiles * 6 floats when grad_rotation is set.
+static int launch_backward(const float2* v, const void* rot, const float2* gr, float2* dv, void* grad_rotation,
+                           float* part, const SliceGeom& g, cudaStream_t st) {
+    const int tiles = extract_tiles(g);
+    const unsigned blocks = (unsigned)((int64_t)g.n * tiles);
+    if (dv && grad_rotation)
+        extract_bwd_kernel<true, true><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, part, g, tiles);
+    else if (dv)
+        extract_bwd_kernel<true, false><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, part, g, tiles);
+    else
+        extract_bwd_kernel<false, true><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, part, g, tiles);
+    if (int e = check_launch("extract_bwd_kernel")) return e;
+    if (grad_rotation) {
+        const int64_t total = (int64_t)g.n * 9;
+        drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rot, grad_rotation, g, tiles);
+        if (int e = check_launch("drot_finish_kernel")) return e;
+    }
+    return TT_OK;
 }
 
 }  // namespace tt
@@ -305,8 +364,7 @@ extern "C" int tt_slice_geometry(const void* rotation_matrices, int32_t mode, ui
 
 extern "C" size_t tt_extract_backward_workspace_bytes(const tt_slice_params* p) {
     if (!p || p->n <= 0 || p->img_h < 1 || p->img_w < 1) return 0;
-    const int64_t tiles = tiles_per_slice((int)p->img_h, (int)(p->img_w / 2 + 1));
-    return (size_t)(p->n * tiles * 6 * sizeof(float));
+    return partial_bytes(p->n, tiles_per_slice((int)p->img_h, (int)(p->img_w / 2 + 1)));
 }
 
 extern "C" int tt_extract_central_slices_rfft_3d_backward(
@@ -319,36 +377,15 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward(
     if (!grad_volume && !grad_rotation) return TT_OK;
     SliceGeom g = make_geom(*p);
     const int tiles = extract_tiles(g);
-    const int64_t blocks = (int64_t)g.n * tiles;
-    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract backward: too many blocks");
-    cudaStream_t st = as_stream(stream);
+    if ((int64_t)g.n * tiles > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract backward: too many blocks");
     if (grad_rotation) {
-        const size_t need = tt_extract_backward_workspace_bytes(p);
+        const size_t need = partial_bytes(g.n, tiles);
         if (!workspace || workspace_bytes < need)
             return fail(TT_ERR_WORKSPACE, "extract backward: workspace of %zu bytes needed, got %zu", need,
                         workspace_bytes);
     }
-    const float2* v = (const float2*)volume_rfft;
-    const float2* gr = (const float2*)grad_slices;
-    float2* dv = (float2*)grad_volume;
-    float* part = (float*)workspace;
-    if (grad_volume && grad_rotation)
-        extract_bwd_kernel<true, true><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr, dv,
-                                                                                  part, g, tiles);
-    else if (grad_volume)
-        extract_bwd_kernel<true, false><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr,
-                                                                                   dv, part, g, tiles);
-    else
-        extract_bwd_kernel<false, true><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr,
-                                                                                   dv, part, g, tiles);
-    if (int e = check_launch("extract_bwd_kernel")) return e;
-    if (grad_rotation) {
-        const int64_t total = (int64_t)g.n * 9;
-        drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rotation_matrices,
-                                                                          grad_rotation, g, tiles);
-        if (int e = check_launch("drot_finish_kernel")) return e;
-    }
-    return TT_OK;
+    return launch_backward((const float2*)volume_rfft, rotation_matrices, (const float2*)grad_slices,
+                           (float2*)grad_volume, grad_rotation, (float*)workspace, g, as_stream(stream));
 }
 
 // ---------------------------------------------------------------------------
@@ -412,19 +449,15 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward_noalloc(const void* vo
     if (!grad_volume && !grad_rotation) return TT_OK;
     SliceGeom g = make_geom(*p);
     const int tiles = extract_tiles(g);
-    const int64_t blocks = (int64_t)g.n * tiles;
-    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "noalloc backward: too many blocks");
+    if ((int64_t)g.n * tiles > 0x7fffffffLL) return fail(TT_ERR_INVALID, "noalloc backward: too many blocks");
     cudaStream_t st = as_stream(stream);
     const float2* v = (const float2*)volume_rfft;
     const float2* gr = (const float2*)grad_slices;
     float2* dv = (float2*)grad_volume;
-    if (!grad_rotation) {
-        // the volume gradient alone needs no scratch
-        extract_bwd_kernel<true, false><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr, dv,
-                                                                                   nullptr, g, tiles);
-        return check_launch("extract_bwd_kernel");
-    }
-    const size_t need = tt_extract_backward_workspace_bytes(p);
+    // the scratch holds n * tiles * 6 partial sums of the rotation gradient
+    if (!grad_rotation)  // the volume gradient alone needs no scratch
+        return launch_backward(v, rotation_matrices, gr, dv, nullptr, nullptr, g, st);
+    const size_t need = partial_bytes(g.n, tiles);
     if (need > (size_t)TT_NOALLOC_SCRATCH_BYTES)
         return fail(TT_ERR_INVALID,
                     "noalloc backward: %lld slices of %lld x %lld need %zu bytes of scratch, more than the "
@@ -434,15 +467,5 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward_noalloc(const void* vo
                     (unsigned)TT_NOALLOC_SCRATCH_BYTES);
     float* part = nullptr;
     if (int e = noalloc_scratch(&part)) return e;
-    if (grad_volume)
-        extract_bwd_kernel<true, true><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr, dv,
-                                                                                  part, g, tiles);
-    else
-        extract_bwd_kernel<false, true><<<(unsigned)blocks, kExtractThreads, 0, st>>>(v, rotation_matrices, gr,
-                                                                                   dv, part, g, tiles);
-    if (int e = check_launch("extract_bwd_kernel")) return e;
-    const int64_t total = (int64_t)g.n * 9;
-    drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rotation_matrices, grad_rotation, g,
-                                                                      tiles);
-    return check_launch("drot_finish_kernel");
+    return launch_backward(v, rotation_matrices, gr, dv, grad_rotation, part, g, st);
 }

@@ -50,17 +50,11 @@ __device__ __forceinline__ void acc_add(double4* a, double re, double im, double
 __device__ __forceinline__ float2 load_slice(const float2* p) { return __ldcs(p); }
 __device__ __forceinline__ double2 load_slice(const double2* p) { return __ldcs(p); }
 
+// Splat of one source pixel.
 template <typename R>
-__global__ void __launch_bounds__(kTileThreads)
-insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void* __restrict__ rot,
-                         typename Acc<R>::T* __restrict__ acc, SliceGeom g, int tiles) {
-    __shared__ float m[9];
-    const int64_t s = blockIdx.x / tiles;
-    const int tile = blockIdx.x - (int)(s * tiles);
-    if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
-    __syncthreads();
-    int iy, ix;
-    if (!tile_pixel(g, tile, iy, ix)) return;
+__device__ __forceinline__ void insert_point(const typename Acc<R>::C* __restrict__ img, const float* m,
+                                             typename Acc<R>::T* __restrict__ acc, const SliceGeom& g, int64_t s,
+                                             int iy, int ix) {
     const float qy = shifted_freq(iy, g.img_h, g.inv_h);
     const float qx = __fmul_rn((float)ix, g.inv_w);
     if (!in_fmax(g, qy, qx)) return;
@@ -84,15 +78,30 @@ insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void*
 #pragma unroll
     for (int k = 0; k < 8; k++) {
         const int bz = (k >> 2) & 1, by = (k >> 1) & 1, bx = k & 1;
+        const int zc = bz ? iz1 : iz0;
         const float fz = bz ? tz : 1.0f - tz;
         const float fy = by ? ty : 1.0f - ty;
         const float fx = bx ? tx : 1.0f - tx;
         const float w = (fz * fy) * fx;
         if (w == 0.0f) continue;  // adds nothing (ceil == floor or zero fraction)
-        const int64_t vi = vox_index(g, bz ? iz1 : iz0, by ? iy1 : iy0, bx ? ix1 : ix0);
+        const int64_t vi = vox_index(g, zc, by ? iy1 : iy0, bx ? ix1 : ix0);
         const R rw = (R)w;
         acc_add(acc + vi, dre * rw, dim * rw, rw);
     }
+}
+
+// One block per (slice, tile).
+template <typename R>
+__global__ void __launch_bounds__(kTileThreads)
+insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void* __restrict__ rot,
+                         typename Acc<R>::T* __restrict__ acc, SliceGeom g, int tiles) {
+    __shared__ float m[9];
+    const int64_t s = blockIdx.x / tiles;
+    const int tile = blockIdx.x - (int)(s * tiles);
+    if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
+    __syncthreads();
+    int iy, ix;
+    if (tile_pixel(g, tile, iy, ix)) insert_point<R>(img, m, acc, g, s, iy, ix);
 }
 
 // Accumulator -> (volume, weights) with the Friedel completion of the x=0
@@ -190,14 +199,14 @@ int launch_insert_accumulate(const void* image_rfft, int32_t complex128, const v
                              const tt_slice_params* p, cudaStream_t st) {
     SliceGeom g = make_geom(*p);
     const int tiles = tiles_per_slice(g.img_h, g.wr);
-    const int64_t blocks = (int64_t)g.n * tiles;
-    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert: too many blocks");
+    const int64_t items = (int64_t)g.n * tiles;
+    if (items > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert: too many blocks");
     if (complex128)
-        insert_accumulate_kernel<double><<<(unsigned)blocks, kTileThreads, 0, st>>>(
-            (const double2*)image_rfft, rot, (double4*)acc, g, tiles);
+        insert_accumulate_kernel<double><<<(unsigned)items, kTileThreads, 0, st>>>((const double2*)image_rfft, rot,
+                                                                                  (double4*)acc, g, tiles);
     else
-        insert_accumulate_kernel<float><<<(unsigned)blocks, kTileThreads, 0, st>>>(
-            (const float2*)image_rfft, rot, (float4*)acc, g, tiles);
+        insert_accumulate_kernel<float><<<(unsigned)items, kTileThreads, 0, st>>>((const float2*)image_rfft, rot,
+                                                                                 (float4*)acc, g, tiles);
     return check_launch("insert_accumulate_kernel");
 }
 

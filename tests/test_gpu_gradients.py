@@ -52,7 +52,8 @@ def test_grad_volume_matches_reference_autograd(golden):
 
 
 @pytest.mark.parametrize("n,nrot,kw", [(64, 48, {}), (33, 20, dict(fftfreq_max=0.3)),
-                                       (48, 16, dict(zyx_matrices=True))])
+                                       (48, 16, dict(zyx_matrices=True)),
+                                       (256, 12, {})])  # 4 z-slab passes of the d/dvolume scatter
 def test_gradients_match_oracle(oracle, n, nrot, kw):
     vol = rfft_volume_np(blob_volume(n, seed=n))
     rots = rotations(nrot, seed=n + 3).astype(np.float32)

@@ -191,7 +191,9 @@ def test_insert_matches_reference_golden(golden):
 
 
 @pytest.mark.parametrize("n,nrot,kw", [(64, 300, {}), (63, 100, {}), (64, 100, dict(fftfreq_max=0.35)),
-                                       (32, 64, dict(zyx_matrices=True))])
+                                       (32, 64, dict(zyx_matrices=True)),
+                                       (256, 40, {}),  # 4 z-slab passes
+                                       (201, 30, dict(fftfreq_max=0.45))])  # odd box, 2 passes
 def test_insert_matches_oracle(oracle, n, nrot, kw):
     rng = np.random.default_rng(n)
     imgs = (rng.standard_normal((nrot, n, n // 2 + 1)) + 1j * rng.standard_normal((nrot, n, n // 2 + 1)))
