@@ -60,6 +60,20 @@ typedef struct tt_slice_params {
     int32_t reserved;
 } tt_slice_params;
 
+/* Per-image contrast transfer function, the scalar arguments of torch-ctf's
+ * calculate_ctf_2d (torch_ctf/ctf_2d.py:12-131) without the Zernike / beam
+ * tilt / anisotropic-magnification extras. */
+typedef struct tt_ctf_params {
+    float defocus_um;              /* (defocus_u + defocus_v) / 2, positive is underfocus */
+    float astigmatism_um;          /* (defocus_u - defocus_v) / 2 */
+    float astigmatism_angle_deg;   /* 0 places defocus_u along y */
+    float voltage_kv;
+    float spherical_aberration_mm;
+    float amplitude_contrast;      /* fraction in [0, 1) */
+    float phase_shift_deg;
+    float pixel_size_a;            /* Angstrom per pixel */
+} tt_ctf_params;
+
 /* Library version (major*10000 + minor*100 + patch) and last error text. */
 int tt_version(void);
 const char *tt_last_error(void);
@@ -167,6 +181,38 @@ int tt_insert_finalize(const void *accumulator, int32_t complex128, int64_t chan
  * NULL).  In place. */
 int tt_friedel_mirror_x0(void *volume_rfft, void *weights, int32_t complex128, int64_t channels,
                          int64_t d, int64_t h, int64_t w_rfft, void *stream);
+
+/* ---- batched, CTF-weighted slices over many volumes -------------------
+ * Many volumes of uneven box size, each with its own rotations and optional
+ * per-image CTF, in ONE persistent launch whose blocks take slices from a
+ * work queue.  The call issues a memset of the workspace (the queue counter)
+ * and the launch on `stream`; it copies nothing and is capturable into a
+ * CUDA graph.  complex64 only.  tile_shape: 0 = 8x32, 1 = 16x16, 2 = 32x8
+ * pixels per block (chosen per box size by the Python autotuner).
+ * The reference has no batched entry point: these run its per-volume
+ * extract / insert semantics for each volume of the list. */
+#define TT_MAX_BATCH_VOLUMES 96
+
+typedef struct tt_batch_volume {
+    tt_slice_params params;          /* geometry of this volume's slices (params.n = its slice count) */
+    const void *volume_rfft;         /* extraction: complex64 source volume */
+    void *slices;                    /* extraction: complex64 output (n, h, w/2+1); insertion: input */
+    void *accumulator;               /* insertion: (re, im, w, pad) float32 slots, zeroed by the caller */
+    const void *rotation_matrices;   /* (n, 3, 3) float32 or float64 */
+    const tt_ctf_params *ctf;        /* device array of n CTFs, or NULL for none.  Extraction
+                                        multiplies each slice by its CTF; insertion weights the
+                                        data by the CTF and the interpolation weights by CTF^2 */
+} tt_batch_volume;
+
+size_t tt_batch_workspace_bytes(void);
+int tt_extract_central_slices_rfft_3d_batched(const tt_batch_volume *volumes, int32_t n_volumes,
+                                              int32_t tile_shape, void *workspace,
+                                              size_t workspace_bytes, void *stream);
+/* Accumulates into each volume's accumulator; finish each volume with
+ * tt_insert_finalize (Friedel completion, volume + weights). */
+int tt_insert_central_slices_rfft_3d_batched(const tt_batch_volume *volumes, int32_t n_volumes,
+                                             int32_t tile_shape, void *workspace,
+                                             size_t workspace_bytes, void *stream);
 
 /* ---- generic 3D interpolation (torch_image_interpolation) -------------
  * dtype codes: 0 float32, 1 float64, 2 complex64, 3 complex128.  Images are

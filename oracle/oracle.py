@@ -230,6 +230,36 @@ def extract_f64(volume_rfft, image_shape, rotation_matrices, zyx_matrices=False)
     return out
 
 
+def ctf_2d(defocus_um, astigmatism_um, astigmatism_angle_deg, voltage_kv, spherical_aberration_mm,
+           amplitude_contrast, phase_shift_deg, pixel_size_a, image_shape, rfft=True, fftshift=True):
+    """Restatement of torch_ctf.calculate_ctf_2d (torch-ctf/src/torch_ctf/ctf_2d.py:12-131,
+    ctf_utils.py:46-86, ctf_aberrations.py:9-81) for scalar parameters, without
+    Zernike / beam-tilt / magnification terms, in float64:
+    -sin(k1 s^2 df + k2 s^4 - phase - atan(A / sqrt(1 - A^2)))."""
+    h, w = image_shape
+    fy = np.fft.fftfreq(h)
+    fx = np.fft.rfftfreq(w) if rfft else np.fft.fftfreq(w)
+    if fftshift:
+        fy = np.fft.fftshift(fy)
+        if not rfft:
+            fx = np.fft.fftshift(fx)
+    y, x = np.meshgrid(fy / pixel_size_a, fx / pixel_size_a, indexing="ij")
+    s2 = y * y + x * x
+    nrm = np.sqrt(s2 + np.finfo(np.float32).eps)
+    th = np.deg2rad(astigmatism_angle_deg)
+    a = np.sqrt(astigmatism_um) * np.array([np.sin(th), np.cos(th)])
+    df = defocus_um - astigmatism_um + 2 * ((y / nrm) * a[0] + (x / nrm) * a[1]) ** 2
+    h_pl, c, m0, e = 6.62607015e-34, 299792458.0, 9.1093837015e-31, 1.602176634e-19
+    ev = e * voltage_kv * 1e3
+    lam = h_pl * c / np.sqrt(ev * (2 * m0 * c * c + ev)) * 1e10
+    k1 = -np.pi * lam
+    k2 = np.pi / 2 * spherical_aberration_mm * 1e7 * lam ** 3
+    ac = amplitude_contrast
+    chi = (k1 * s2 * df * 1e4 + k2 * s2 * s2 - np.deg2rad(phase_shift_deg)
+           - np.arctan(ac / np.sqrt(1 - ac * ac)))
+    return -np.sin(chi)
+
+
 def mirror_x0_post_pass(vol, wts):
     """Friedel completion of the x=0 plane as one post-pass (numpy):
     out[v] = acc[v] + conj(acc[m v]) unless m v is the DC voxel,

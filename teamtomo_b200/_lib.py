@@ -38,6 +38,26 @@ class SliceParams(ctypes.Structure):
     ]
 
 
+class CtfParams(ctypes.Structure):
+    """Mirror of ``tt_ctf_params`` (8 float32, the row layout of CTF tensors)."""
+
+    _fields_ = [(name, _f32) for name in (
+        "defocus_um", "astigmatism_um", "astigmatism_angle_deg", "voltage_kv",
+        "spherical_aberration_mm", "amplitude_contrast", "phase_shift_deg", "pixel_size_a")]
+
+
+class BatchVolume(ctypes.Structure):
+    """Mirror of ``tt_batch_volume``."""
+
+    _fields_ = [
+        ("params", SliceParams),
+        ("volume_rfft", _vp), ("slices", _vp), ("accumulator", _vp),
+        ("rotation_matrices", _vp), ("ctf", _vp),
+    ]
+
+
+MAX_BATCH_VOLUMES = 96
+
 # name -> (argtypes, restype); every symbol the header declares
 SIGNATURES = {
     "tt_version": ([], _i32),
@@ -55,6 +75,11 @@ SIGNATURES = {
     "tt_insert_accumulate": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_finalize": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp, _vp], _i32),
     "tt_friedel_mirror_x0": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp], _i32),
+    "tt_batch_workspace_bytes": ([], _sz),
+    "tt_extract_central_slices_rfft_3d_batched": (
+        [ctypes.POINTER(BatchVolume), _i32, _i32, _vp, _sz, _vp], _i32),
+    "tt_insert_central_slices_rfft_3d_batched": (
+        [ctypes.POINTER(BatchVolume), _i32, _i32, _vp, _sz, _vp], _i32),
     "tt_sample_image_3d": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i32, _vp], _i32),
     "tt_insert_into_image_3d": (
         [_vp, _i32, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _i32, _i32, _vp], _i32),

@@ -1,0 +1,100 @@
+"""Tile-shape autotuner for the batched slice kernels.
+
+The batched kernels are compiled for three tile shapes (8x32, 16x16 and 32x8
+pixels per 256-thread block).  Which one is fastest depends on the box size
+(how a warp's pixels spread over the volume's cache lines).  ``tune`` times
+each shape on synthetic data of a given box size with CUDA events and records
+the winner in a JSON cache keyed by (GPU name, kind, box); the batched API
+looks the cache up (``cached_tile_shape``) and falls back to 8x32 (shape 0)
+for box sizes never tuned.
+
+Cache file: ``$TT_AUTOTUNE_CACHE`` or ``~/.cache/teamtomo_b200/autotune.json``.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import threading
+
+import torch
+
+TILE_SHAPES = {0: (8, 32), 1: (16, 16), 2: (32, 8)}
+DEFAULT_TILE_SHAPE = 0
+_lock = threading.Lock()
+_mem: dict[str, int] | None = None
+
+
+def cache_path() -> str:
+    return os.environ.get("TT_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "teamtomo_b200", "autotune.json"))
+
+
+def _key(kind: str, box: int, device) -> str:
+    return f"{torch.cuda.get_device_name(device)}:{kind}:{int(box)}"
+
+
+def _load() -> dict[str, int]:
+    global _mem
+    if _mem is None:
+        try:
+            with open(cache_path()) as f:
+                _mem = {k: int(v) for k, v in json.load(f).items()}
+        except (OSError, ValueError):
+            _mem = {}
+    return _mem
+
+
+def _save() -> None:
+    path = cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(_load(), f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass  # a read-only home only loses the cache, not the result
+
+
+def cached_tile_shape(kind: str, box: int, device) -> int:
+    with _lock:
+        return _load().get(_key(kind, box, device), DEFAULT_TILE_SHAPE)
+
+
+def tune(kind: str, box: int, n_slices: int = 512, device=None, repeats: int = 5) -> dict[int, float]:
+    """Time every tile shape for `kind` ('extract' or 'insert') at box size
+    `box`, store the fastest in the cache and return {shape: ms}."""
+    from . import batched
+
+    dev = torch.device(device or "cuda")
+    g = torch.Generator(device=dev).manual_seed(box)
+    shape3 = (box, box, box // 2 + 1)
+    R = torch.linalg.qr(torch.randn((n_slices, 3, 3), device=dev, generator=g))[0].contiguous()
+    ctf = batched.ctf_params(1.5, n=n_slices, device=dev)
+    if kind == "extract":
+        vol = torch.randn(shape3, dtype=torch.complex64, device=dev, generator=g)
+        run = lambda ts: batched.extract_central_slices_rfft_3d_batched(  # noqa: E731
+            [vol], [R], ctf=[ctf], tile_shape=ts)
+    elif kind == "insert":
+        img = torch.randn((n_slices, box, box // 2 + 1), dtype=torch.complex64, device=dev, generator=g)
+        run = lambda ts: batched.insert_central_slices_rfft_3d_batched(  # noqa: E731
+            [img], [R], ctf=[ctf], tile_shape=ts)
+    else:
+        raise ValueError("kind must be 'extract' or 'insert'")
+    times = {}
+    for ts in TILE_SHAPES:
+        run(ts)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        start.record()
+        for _ in range(repeats):
+            run(ts)
+        end.record()
+        torch.cuda.synchronize(dev)
+        times[ts] = start.elapsed_time(end) / repeats
+    best = min(times, key=times.get)
+    with _lock:
+        _load()[_key(kind, box, dev)] = best
+        _save()
+    return times

@@ -1,0 +1,228 @@
+"""Batched, CTF-weighted central-slice extraction and insertion.
+
+Many volumes of uneven box size, each with its own rotations and an optional
+per-image CTF, run in ONE persistent kernel launch that takes slices from a
+work queue (``csrc/batched.cu``).  The reference has no batched API: for each
+volume these compute exactly what ``extract_central_slices_rfft_3d`` /
+``insert_central_slices_rfft_3d`` compute, with the CTF of torch-ctf's
+``calculate_ctf_2d`` (rfft, fftshifted grid of the image shape) applied in the
+kernel:
+
+* extraction returns ``ctf * slice``;
+* insertion accumulates ``ctf * image`` and the interpolation weights times
+  ``ctf**2`` (the usual CTF-weighted backprojection numerator/denominator).
+
+``BatchedSlicePlan`` captures a fixed-shape batch into a CUDA graph for
+repeated replay.  The tile shape of the launch is chosen per box size by the
+autotuner in ``teamtomo_b200.autotune`` (cached; 8x32 when never tuned).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Sequence
+
+import torch
+
+from . import _lib
+from .torch_fourier_slice._params import rfft_shape, rotation_arg, slice_params
+from .torch_fourier_slice.slice_insertion import insert_finalize, new_accumulator
+
+CTF_FIELDS = ("defocus_um", "astigmatism_um", "astigmatism_angle_deg", "voltage_kv",
+              "spherical_aberration_mm", "amplitude_contrast", "phase_shift_deg", "pixel_size_a")
+
+
+def ctf_params(defocus_um, astigmatism_um=0.0, astigmatism_angle_deg=0.0, voltage_kv=300.0,
+               spherical_aberration_mm=2.7, amplitude_contrast=0.07, phase_shift_deg=0.0,
+               pixel_size_a=1.0, n: int | None = None, device=None) -> torch.Tensor:
+    """Per-image CTF parameter rows, shape (n, 8) float32, in the field order of
+    ``tt_ctf_params`` (the scalar arguments of torch-ctf's calculate_ctf_2d).
+    Each argument is a scalar or a length-n sequence/tensor."""
+    vals = [defocus_um, astigmatism_um, astigmatism_angle_deg, voltage_kv, spherical_aberration_mm,
+            amplitude_contrast, phase_shift_deg, pixel_size_a]
+    cols = [torch.as_tensor(v, dtype=torch.float32).reshape(-1) for v in vals]
+    m = max(c.numel() for c in cols) if n is None else n
+    cols = [c.expand(m) if c.numel() == 1 else c for c in cols]
+    for c in cols:
+        if c.numel() != m:
+            raise ValueError(f"CTF parameter of length {c.numel()}, expected {m}")
+    out = torch.stack(cols, dim=-1).contiguous()
+    return out.to(device) if device is not None else out
+
+
+def _ws(device) -> torch.Tensor:
+    return torch.empty(int(_lib.load().tt_batch_workspace_bytes()), dtype=torch.uint8, device=device)
+
+
+def _tile_shape(kind: str, boxes: Sequence[int], device, tile_shape):
+    if tile_shape is not None:
+        return int(tile_shape)
+    from . import autotune
+
+    return autotune.cached_tile_shape(kind, max(boxes), device)
+
+
+def _check_ctf(ctf, n, device):
+    if ctf is None:
+        return None
+    ctf = torch.as_tensor(ctf, dtype=torch.float32).to(device).reshape(-1, 8).contiguous()
+    if ctf.shape[0] != n:
+        raise ValueError(f"{ctf.shape[0]} CTF rows for {n} slices")
+    return ctf
+
+
+def _batches(items, size=_lib.MAX_BATCH_VOLUMES):
+    for i in range(0, len(items), size):
+        yield items[i:i + size]
+
+
+def _run(fn_name, entries, tile_shape, device, what):
+    L = _lib.load()
+    arr = (_lib.BatchVolume * len(entries))(*entries)
+    ws = _ws(device)
+    _lib.check(getattr(L, fn_name)(arr, len(entries), int(tile_shape), _lib.ptr(ws), ws.numel(),
+                                   _lib.stream_of(device)), what)
+
+
+def extract_central_slices_rfft_3d_batched(
+    volumes: Sequence[torch.Tensor],
+    rotation_matrices: Sequence[torch.Tensor],
+    image_shapes: Sequence[tuple[int, int, int]] | None = None,
+    ctf: Sequence[torch.Tensor | None] | None = None,
+    fftfreq_max: float | None = None,
+    zyx_matrices: bool = False,
+    x_tolerance: float = 1e-8,
+    rot_tolerance: float | None = 1e-8,
+    tile_shape: int | None = None,
+) -> list[torch.Tensor]:
+    """Extract slices from every volume in one launch.
+
+    ``volumes[i]`` is an fftshifted rfft volume (d, d, d//2+1) complex64,
+    ``rotation_matrices[i]`` (n_i, 3, 3), ``image_shapes[i]`` defaults to
+    (d, d, d), ``ctf[i]`` is None or (n_i, 8) CTF rows (see ``ctf_params``).
+    Returns the list of (n_i, h_i, w_i//2+1) complex64 slice stacks."""
+    if not volumes:
+        return []
+    dev = _lib.require_cuda(*volumes)
+    ctf = list(ctf) if ctf is not None else [None] * len(volumes)
+    shapes = list(image_shapes) if image_shapes is not None else [
+        (v.shape[0], v.shape[0], v.shape[0]) for v in volumes]
+    outs, entries, keep = [], [], []
+    for vol, R, shape, c in zip(volumes, rotation_matrices, shapes, ctf):
+        if vol.ndim != 3 or vol.dtype != torch.complex64:
+            raise ValueError("batched extraction takes complex64 (d, h, w//2+1) volumes")
+        vol = vol.contiguous()
+        Rm, _ = rotation_arg(R, dev)
+        n = Rm.shape[0]
+        h, w = int(shape[-2]), int(shape[-1])
+        out = torch.empty((n, h, w // 2 + 1), dtype=torch.complex64, device=dev)
+        cc = _check_ctf(c, n, dev)
+        p = slice_params(n=n, image_shape=shape, volume=vol, rotation=Rm, fftfreq_max=fftfreq_max,
+                         zyx_matrices=zyx_matrices, x_tolerance=x_tolerance,
+                         rot_tolerance=rot_tolerance)
+        entries.append(_lib.BatchVolume(p, vol.data_ptr(), out.data_ptr(), None, Rm.data_ptr(),
+                                        cc.data_ptr() if cc is not None else None))
+        keep += [vol, Rm, cc]
+        outs.append(out)
+    ts = _tile_shape("extract", [v.shape[0] for v in volumes], dev, tile_shape)
+    for chunk in _batches(entries):
+        _run("tt_extract_central_slices_rfft_3d_batched", chunk, ts, dev,
+             "extract_central_slices_rfft_3d_batched")
+    return outs
+
+
+def insert_central_slices_rfft_3d_batched(
+    images: Sequence[torch.Tensor],
+    rotation_matrices: Sequence[torch.Tensor],
+    volume_shapes: Sequence[tuple[int, int, int]] | None = None,
+    ctf: Sequence[torch.Tensor | None] | None = None,
+    fftfreq_max: float | None = None,
+    zyx_matrices: bool = False,
+    tile_shape: int | None = None,
+) -> list[tuple[torch.Tensor, torch.Tensor]]:
+    """Insert every image stack into its own volume in one launch.
+
+    ``images[i]`` (n_i, h, w//2+1) complex64 fftshifted rffts,
+    ``volume_shapes[i]`` defaults to (h, h, h).  Returns a list of
+    (volume (d, h, w//2+1) complex64, weights float32), Friedel-completed;
+    with a CTF the weights are sums of CTF^2-weighted interpolation weights."""
+    if not images:
+        return []
+    dev = _lib.require_cuda(*images)
+    ctf = list(ctf) if ctf is not None else [None] * len(images)
+    shapes = list(volume_shapes) if volume_shapes is not None else [
+        (im.shape[-2], im.shape[-2], im.shape[-2]) for im in images]
+    accs, entries, keep = [], [], []
+    for img, R, shape, c in zip(images, rotation_matrices, shapes, ctf):
+        if img.dtype != torch.complex64:
+            raise ValueError("batched insertion takes complex64 slices")
+        h, w = int(shape[-2]), int(shape[-1])
+        if tuple(img.shape[-2:]) != (h, w // 2 + 1):
+            raise ValueError(f"slices of shape {tuple(img.shape[-2:])} for volume_shape {tuple(shape)}")
+        Rm, _ = rotation_arg(R, dev)
+        n = Rm.shape[0]
+        if math.prod(img.shape[:-2]) != n:
+            raise ValueError(f"{n} rotation matrices for {math.prod(img.shape[:-2])} slices")
+        img = img.reshape(n, *img.shape[-2:]).contiguous()
+        acc = new_accumulator(shape, False, dev)
+        cc = _check_ctf(c, n, dev)
+        p = slice_params(n=n, image_shape=shape, volume=None, rotation=Rm, fftfreq_max=fftfreq_max,
+                         zyx_matrices=zyx_matrices, vol_dims=rfft_shape(shape))
+        entries.append(_lib.BatchVolume(p, None, img.data_ptr(), acc.data_ptr(), Rm.data_ptr(),
+                                        cc.data_ptr() if cc is not None else None))
+        keep += [img, Rm, cc]
+        accs.append(acc)
+    ts = _tile_shape("insert", [s[-2] for s in shapes], dev, tile_shape)
+    for chunk in _batches(entries):
+        _run("tt_insert_central_slices_rfft_3d_batched", chunk, ts, dev,
+             "insert_central_slices_rfft_3d_batched")
+    out = []
+    for acc in accs:
+        v, w = insert_finalize(acc, False)
+        out.append((v[0], w))
+    return out
+
+
+class BatchedSlicePlan:
+    """A fixed-shape batch of volumes captured into one CUDA graph.
+
+    Allocates static buffers for the volumes, rotations and CTF rows (fill
+    them in place: ``plan.volumes[i].copy_(...)``), captures the batched
+    launch (extraction, or insertion + per-volume finalize) once, and replays
+    it with ``run()``.  Outputs live in ``plan.outputs``."""
+
+    def __init__(self, box_sizes: Sequence[int], n_slices: Sequence[int], mode: str = "extract",
+                 with_ctf: bool = True, device=None, tile_shape: int | None = None):
+        if mode not in ("extract", "insert"):
+            raise ValueError("mode must be 'extract' or 'insert'")
+        self.device = torch.device(device or "cuda")
+        self.mode = mode
+        dev = self.device
+        self.rotations = [torch.zeros((n, 3, 3), device=dev) for n in n_slices]
+        for r in self.rotations:
+            r[:] = torch.eye(3, device=dev)
+        self.ctf = [ctf_params(1.5, n=n, device=dev) for n in n_slices] if with_ctf else None
+        if mode == "extract":
+            self.volumes = [torch.zeros(rfft_shape((b, b, b)), dtype=torch.complex64, device=dev)
+                            for b in box_sizes]
+            call = lambda: extract_central_slices_rfft_3d_batched(  # noqa: E731
+                self.volumes, self.rotations, ctf=self.ctf, tile_shape=tile_shape)
+        else:
+            self.images = [torch.zeros((n, b, b // 2 + 1), dtype=torch.complex64, device=dev)
+                           for b, n in zip(box_sizes, n_slices)]
+            call = lambda: insert_central_slices_rfft_3d_batched(  # noqa: E731
+                self.images, self.rotations, ctf=self.ctf, tile_shape=tile_shape)
+        # warm up (tuner cache lookup, library load) outside the capture
+        side = torch.cuda.Stream(device=dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            call()
+        torch.cuda.current_stream(dev).wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.outputs = call()
+
+    def run(self):
+        self.graph.replay()
+        return self.outputs

@@ -22,70 +22,15 @@
 
 #include "capi_util.cuh"
 #include "slice_common.cuh"
+#include "slice_ops.cuh"
 
 namespace tt {
 
 constexpr int kExtractThreads = kTileThreads;
 
-// grid_sample's source index of array coordinate c on an axis of n samples:
-// c -> grid coordinate c / (0.5 n - 0.5) - 1 (grid_sample_utils.py:6-26) ->
-// ((g + 1) / 2) * (n - 1) (align_corners=True), clipped to [0, n-1].
-__device__ __forceinline__ float source_index(float c, float half, float nm1) {
-    const float gc = __fsub_rn(__fdiv_rn(c, half), 1.0f);
-    const float ix = __fmul_rn(__fmul_rn(__fadd_rn(gc, 1.0f), 0.5f), nm1);
-    return fminf(fmaxf(ix, 0.0f), nm1);
-}
-
-struct Corners {
-    int z0, y0, x0;
-    float ax0, ax1, ay0, ay1, az0, az1;  // per-axis weights of the low/high corner
-    bool zin, yin, xin;                  // high corner inside the array
-};
-
-// grid_sample trilinear corner set of an inside array coordinate c.
-__device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float c[3]) {
-    const float iz = source_index(c[0], 0.5f * (float)g.D - 0.5f, g.ub0);
-    const float iy = source_index(c[1], 0.5f * (float)g.H - 0.5f, g.ub1);
-    const float ix = source_index(c[2], 0.5f * (float)g.W - 0.5f, g.ub2);
-    Corners k;
-    const float fz = floorf(iz), fy = floorf(iy), fx = floorf(ix);
-    k.z0 = (int)fz;
-    k.y0 = (int)fy;
-    k.x0 = (int)fx;
-    k.az0 = (fz + 1.0f) - iz;
-    k.az1 = iz - fz;
-    k.ay0 = (fy + 1.0f) - iy;
-    k.ay1 = iy - fy;
-    k.ax0 = (fx + 1.0f) - ix;
-    k.ax1 = ix - fx;
-    k.zin = k.z0 + 1 < g.D;
-    k.yin = k.y0 + 1 < g.H;
-    k.xin = k.x0 + 1 < g.W;
-    return k;
-}
-
 __device__ __forceinline__ void load_rotation(float* sm, const void* rot, int64_t s,
                                               const SliceGeom& g, bool apply_tol) {
     if (threadIdx.x < 9) sm[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, apply_tol);
-}
-
-// Geometry of one extraction pixel: false when the pixel is outside
-// fftfreq_max or its point outside the volume.
-__device__ __forceinline__ bool extract_geometry(const SliceGeom& g, const float* m, int iy, int ix, float& qy,
-                                                 float& qx, bool& cj, float c[3]) {
-    qy = shifted_freq(iy, g.img_h, g.inv_h);
-    qx = __fmul_rn((float)ix, g.inv_w);
-    if (!in_fmax(g, qy, qx)) return false;
-    float p[3];
-    rotate_slice_point(m, qy, qx, p);
-    cj = extract_conj(g, m, p[2]);
-    if (cj) {
-        p[0] = -p[0];
-        p[1] = -p[1];
-        p[2] = -p[2];
-    }
-    to_dft_coords(g, p, c);
-    return inside_volume(g, c);
 }
 
 __global__ void __launch_bounds__(kExtractThreads)
@@ -102,28 +47,7 @@ extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     bool cj = false;
     float2 r = make_float2(0.0f, 0.0f);
     if (extract_geometry(g, m, iy, ix, qy, qx, cj, c)) {
-        const Corners k = make_corners(g, c);
-#pragma unroll
-        for (int bz = 0; bz < 2; bz++) {
-            if (bz && !k.zin) continue;
-            const float wz = bz ? k.az1 : k.az0;
-#pragma unroll
-            for (int by = 0; by < 2; by++) {
-                if (by && !k.yin) continue;
-                const float wzy = (by ? k.ay1 : k.ay0) * wz;
-                const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
-                const float2 v0 = __ldg(vol + base);
-                const float w0 = k.ax0 * wzy;
-                r.x = fmaf(v0.x, w0, r.x);
-                r.y = fmaf(v0.y, w0, r.y);
-                if (k.xin) {
-                    const float2 v1 = __ldg(vol + base + 1);
-                    const float w1 = k.ax1 * wzy;
-                    r.x = fmaf(v1.x, w1, r.x);
-                    r.y = fmaf(v1.y, w1, r.y);
-                }
-            }
-        }
+        r = sample_trilinear(vol, g, make_corners(g, c));
         if (cj) r.y = -r.y;
     }
     // streaming store: the slices are written once and should not evict the volume from L2

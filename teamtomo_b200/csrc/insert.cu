@@ -22,73 +22,9 @@
 
 #include "capi_util.cuh"
 #include "slice_common.cuh"
+#include "slice_ops.cuh"
 
 namespace tt {
-
-template <typename R>
-struct Acc;
-template <>
-struct Acc<float> {
-    using T = float4;
-    using C = float2;
-};
-template <>
-struct Acc<double> {
-    using T = double4;
-    using C = double2;
-};
-
-__device__ __forceinline__ void acc_add(float4* a, float re, float im, float w) {
-    atomicAdd(a, make_float4(re, im, w, 0.0f));
-}
-__device__ __forceinline__ void acc_add(double4* a, double re, double im, double w) {
-    atomicAdd(&a->x, re);
-    atomicAdd(&a->y, im);
-    atomicAdd(&a->z, w);
-}
-
-__device__ __forceinline__ float2 load_slice(const float2* p) { return __ldcs(p); }
-__device__ __forceinline__ double2 load_slice(const double2* p) { return __ldcs(p); }
-
-// Splat of one source pixel.
-template <typename R>
-__device__ __forceinline__ void insert_point(const typename Acc<R>::C* __restrict__ img, const float* m,
-                                             typename Acc<R>::T* __restrict__ acc, const SliceGeom& g, int64_t s,
-                                             int iy, int ix) {
-    const float qy = shifted_freq(iy, g.img_h, g.inv_h);
-    const float qx = __fmul_rn((float)ix, g.inv_w);
-    if (!in_fmax(g, qy, qx)) return;
-    if (qx == 0.0f && qy < 0.0f) return;  // Friedel-redundant source pixel
-    float p[3], c[3];
-    rotate_slice_point(m, qy, qx, p);
-    const typename Acc<R>::C d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
-    R dre = d.x, dim = d.y;
-    if (p[2] < 0.0f) {
-        p[0] = -p[0];
-        p[1] = -p[1];
-        p[2] = -p[2];
-        dim = -dim;
-    }
-    to_dft_coords(g, p, c);
-    if (!inside_volume(g, c)) return;
-    const float z0 = floorf(c[0]), y0 = floorf(c[1]), x0 = floorf(c[2]);
-    const float tz = c[0] - z0, ty = c[1] - y0, tx = c[2] - x0;
-    const int iz0 = (int)z0, iy0 = (int)y0, ix0 = (int)x0;
-    const int iz1 = (int)ceilf(c[0]), iy1 = (int)ceilf(c[1]), ix1 = (int)ceilf(c[2]);
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int bz = (k >> 2) & 1, by = (k >> 1) & 1, bx = k & 1;
-        const int zc = bz ? iz1 : iz0;
-        const float fz = bz ? tz : 1.0f - tz;
-        const float fy = by ? ty : 1.0f - ty;
-        const float fx = bx ? tx : 1.0f - tx;
-        const float w = (fz * fy) * fx;
-        if (w == 0.0f) continue;  // adds nothing (ceil == floor or zero fraction)
-        const int64_t vi = vox_index(g, zc, by ? iy1 : iy0, bx ? ix1 : ix0);
-        const R rw = (R)w;
-        acc_add(acc + vi, dre * rw, dim * rw, rw);
-    }
-}
 
 // One block per (slice, tile).
 template <typename R>

@@ -1,0 +1,223 @@
+// Per-point operations shared by the single-volume and the batched kernels:
+// grid_sample-style trilinear sampling of an rfft volume, the insertion splat,
+// and the in-kernel CTF.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "slice_common.cuh"
+
+namespace tt {
+
+// ---------------------------------------------------------------- sampling
+
+// grid_sample's source index of array coordinate c on an axis of n samples:
+// c -> grid coordinate c / (0.5 n - 0.5) - 1 (grid_sample_utils.py:6-26) ->
+// ((g + 1) / 2) * (n - 1) (align_corners=True), clipped to [0, n-1].
+__device__ __forceinline__ float source_index(float c, float half, float nm1) {
+    const float gc = __fsub_rn(__fdiv_rn(c, half), 1.0f);
+    const float ix = __fmul_rn(__fmul_rn(__fadd_rn(gc, 1.0f), 0.5f), nm1);
+    return fminf(fmaxf(ix, 0.0f), nm1);
+}
+
+struct Corners {
+    int z0, y0, x0;
+    float ax0, ax1, ay0, ay1, az0, az1;  // per-axis weights of the low/high corner
+    bool zin, yin, xin;                  // high corner inside the array
+};
+
+// grid_sample trilinear corner set of an inside array coordinate c (the
+// round trip decides the cell at integer kinks, where the derivative jumps).
+__device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float c[3]) {
+    const float iz = source_index(c[0], 0.5f * (float)g.D - 0.5f, g.ub0);
+    const float iy = source_index(c[1], 0.5f * (float)g.H - 0.5f, g.ub1);
+    const float ix = source_index(c[2], 0.5f * (float)g.W - 0.5f, g.ub2);
+    Corners k;
+    const float fz = floorf(iz), fy = floorf(iy), fx = floorf(ix);
+    k.z0 = (int)fz;
+    k.y0 = (int)fy;
+    k.x0 = (int)fx;
+    k.az0 = (fz + 1.0f) - iz;
+    k.az1 = iz - fz;
+    k.ay0 = (fy + 1.0f) - iy;
+    k.ay1 = iy - fy;
+    k.ax0 = (fx + 1.0f) - ix;
+    k.ax1 = ix - fx;
+    k.zin = k.z0 + 1 < g.D;
+    k.yin = k.y0 + 1 < g.H;
+    k.xin = k.x0 + 1 < g.W;
+    return k;
+}
+
+// Geometry of one extraction pixel: false when the pixel is outside
+// fftfreq_max or its point outside the volume.
+__device__ __forceinline__ bool extract_geometry(const SliceGeom& g, const float* m, int iy, int ix, float& qy,
+                                                 float& qx, bool& cj, float c[3]) {
+    qy = shifted_freq(iy, g.img_h, g.inv_h);
+    qx = __fmul_rn((float)ix, g.inv_w);
+    if (!in_fmax(g, qy, qx)) return false;
+    float p[3];
+    rotate_slice_point(m, qy, qx, p);
+    cj = extract_conj(g, m, p[2]);
+    if (cj) {
+        p[0] = -p[0];
+        p[1] = -p[1];
+        p[2] = -p[2];
+    }
+    to_dft_coords(g, p, c);
+    return inside_volume(g, c);
+}
+
+// Trilinear sample of the complex volume at corner set k.
+__device__ __forceinline__ float2 sample_trilinear(const float2* __restrict__ vol, const SliceGeom& g,
+                                                   const Corners& k) {
+    float2 r = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int bz = 0; bz < 2; bz++) {
+        if (bz && !k.zin) continue;
+        const float wz = bz ? k.az1 : k.az0;
+#pragma unroll
+        for (int by = 0; by < 2; by++) {
+            if (by && !k.yin) continue;
+            const float wzy = (by ? k.ay1 : k.ay0) * wz;
+            const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
+            const float2 v0 = __ldg(vol + base);
+            const float w0 = k.ax0 * wzy;
+            r.x = fmaf(v0.x, w0, r.x);
+            r.y = fmaf(v0.y, w0, r.y);
+            if (k.xin) {
+                const float2 v1 = __ldg(vol + base + 1);
+                const float w1 = k.ax1 * wzy;
+                r.x = fmaf(v1.x, w1, r.x);
+                r.y = fmaf(v1.y, w1, r.y);
+            }
+        }
+    }
+    return r;
+}
+
+// --------------------------------------------------------------------- CTF
+
+// Per-image constants of the 2D CTF -sin(chi) of torch-ctf's calculate_ctf_2d
+// (ctf_2d.py:12-131, ctf_utils.py:46-86, ctf_aberrations.py:42-81):
+//   chi = k1 * s^2 * df(direction) + k2 * s^4 - phase_shift - atan(A / sqrt(1 - A^2))
+//   k1 = -pi * lambda, k2 = pi / 2 * Cs * lambda^3 (Angstrom), s in cycles/Angstrom,
+//   df = defocus - astig + 2 * (u . a)^2, u the unit frequency direction
+//   (with float32 epsilon in its norm), a = sqrt(astig) * (sin theta, cos theta) (yx).
+struct CtfConst {
+    double k1, k2, phase;        // Angstrom units; phase includes the amplitude-contrast term
+    double defocus, astig;       // micrometres (the astigmatism adjustment is done in um)
+    double ay, ax;               // astigmatism vector sqrt(astig) * (sin, cos)
+    double inv_px;               // 1 / pixel size (1/Angstrom)
+};
+
+// Constants of one image from its tt_ctf_params (double precision, once per image).
+__host__ __device__ inline CtfConst make_ctf_const(const tt_ctf_params& p) {
+    const double h = 6.62607015e-34, c = 299792458.0, m0 = 9.1093837015e-31, e = 1.602176634e-19;
+    const double volts = (double)p.voltage_kv * 1e3;
+    const double ev = e * volts;
+    const double lambda = h * c / sqrt(ev * (2.0 * m0 * c * c + ev)) * 1e10;  // Angstrom
+    const double pi = 3.14159265358979323846;
+    const double cs = (double)p.spherical_aberration_mm * 1e7;
+    const double ac = (double)p.amplitude_contrast;
+    CtfConst k;
+    k.k1 = -pi * lambda;
+    k.k2 = pi / 2.0 * cs * lambda * lambda * lambda;
+    k.phase = (double)p.phase_shift_deg * pi / 180.0 + atan(ac / sqrt(1.0 - ac * ac));
+    k.defocus = p.defocus_um;
+    k.astig = p.astigmatism_um;
+    const double th = (double)p.astigmatism_angle_deg * pi / 180.0;
+    const double sa = sqrt((double)(p.astigmatism_um > 0 ? p.astigmatism_um : 0.0f));
+    k.ay = sa * sin(th);
+    k.ax = sa * cos(th);
+    k.inv_px = 1.0 / (double)p.pixel_size_a;
+    return k;
+}
+
+// CTF at slice frequency (qy, qx) in cycles/pixel.  The phase reaches hundreds
+// of radians at high frequency, so it and its sine are evaluated in double.
+__device__ __forceinline__ float ctf_value(const CtfConst& k, float qy, float qx) {
+    const double y = (double)qy * k.inv_px, x = (double)qx * k.inv_px;
+    const double s2 = y * y + x * x;
+    const double nrm = sqrt(s2 + 1.1920928955078125e-07);  // torch.finfo(float32).eps
+    const double dot = (y / nrm) * k.ay + (x / nrm) * k.ax;
+    const double df = (k.defocus - k.astig + 2.0 * dot * dot) * 1e4;  // um -> Angstrom
+    const double chi = k.k1 * s2 * df + k.k2 * s2 * s2 - k.phase;
+    return (float)-sin(chi);
+}
+
+// ---------------------------------------------------------------- insertion
+
+template <typename R>
+struct Acc;
+template <>
+struct Acc<float> {
+    using T = float4;
+    using C = float2;
+};
+template <>
+struct Acc<double> {
+    using T = double4;
+    using C = double2;
+};
+
+__device__ __forceinline__ void acc_add(float4* a, float re, float im, float w) {
+    atomicAdd(a, make_float4(re, im, w, 0.0f));
+}
+__device__ __forceinline__ void acc_add(double4* a, double re, double im, double w) {
+    atomicAdd(&a->x, re);
+    atomicAdd(&a->y, im);
+    atomicAdd(&a->z, w);
+}
+
+__device__ __forceinline__ float2 load_slice(const float2* p) { return __ldcs(p); }
+__device__ __forceinline__ double2 load_slice(const double2* p) { return __ldcs(p); }
+
+// Splat of one source pixel into the (re, im, w) accumulator, following
+// _insert_central_slices_rfft_3d.py:30-85 and _insert_into_3d_dft_linear
+// :289-346.  With a CTF (ctf != nullptr) the data are weighted by the CTF
+// and the interpolation weights by its square.
+template <typename R>
+__device__ __forceinline__ void insert_point(const typename Acc<R>::C* __restrict__ img, const float* m,
+                                             typename Acc<R>::T* __restrict__ acc, const SliceGeom& g, int64_t s,
+                                             int iy, int ix, const CtfConst* ctf = nullptr) {
+    const float qy = shifted_freq(iy, g.img_h, g.inv_h);
+    const float qx = __fmul_rn((float)ix, g.inv_w);
+    if (!in_fmax(g, qy, qx)) return;
+    if (qx == 0.0f && qy < 0.0f) return;  // Friedel-redundant source pixel
+    float p[3], c[3];
+    rotate_slice_point(m, qy, qx, p);
+    const typename Acc<R>::C d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+    R dre = d.x, dim = d.y, wscale = (R)1;
+    if (ctf) {
+        const float cv = ctf_value(*ctf, qy, qx);
+        dre *= (R)cv;
+        dim *= (R)cv;
+        wscale = (R)(cv * cv);
+    }
+    if (p[2] < 0.0f) {
+        p[0] = -p[0];
+        p[1] = -p[1];
+        p[2] = -p[2];
+        dim = -dim;
+    }
+    to_dft_coords(g, p, c);
+    if (!inside_volume(g, c)) return;
+    const float z0 = floorf(c[0]), y0 = floorf(c[1]), x0 = floorf(c[2]);
+    const float tz = c[0] - z0, ty = c[1] - y0, tx = c[2] - x0;
+    const int iz0 = (int)z0, iy0 = (int)y0, ix0 = (int)x0;
+    const int iz1 = (int)ceilf(c[0]), iy1 = (int)ceilf(c[1]), ix1 = (int)ceilf(c[2]);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int bz = (k >> 2) & 1, by = (k >> 1) & 1, bx = k & 1;
+        const float fz = bz ? tz : 1.0f - tz;
+        const float fy = by ? ty : 1.0f - ty;
+        const float fx = bx ? tx : 1.0f - tx;
+        const float w = (fz * fy) * fx;
+        if (w == 0.0f) continue;  // adds nothing (ceil == floor or zero fraction)
+        const int64_t vi = vox_index(g, bz ? iz1 : iz0, by ? iy1 : iy0, bx ? ix1 : ix0);
+        const R rw = (R)w;
+        acc_add(acc + vi, dre * rw, dim * rw, rw * wscale);
+    }
+}
+
+}  // namespace tt

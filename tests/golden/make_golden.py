@@ -217,6 +217,27 @@ def main():
     g["backproject_odd_images"] = imgs_odd.numpy()
     g["backproject_odd_out"] = backproject_2d_to_3d(imgs_odd, torch.tensor(rots), pad_factor=1.5).numpy()
 
+    # ---------------- CTF (torch-ctf calculate_ctf_2d) ----------------
+    sys.path.insert(0, os.path.join(REF, "packages", "primitives", "torch-ctf", "src"))
+    from torch_ctf import calculate_ctf_2d
+
+    ctf_cases = [  # defocus, astig, angle, kV, Cs, Ac, phase, px, shape, rfft, fftshift
+        (1.5, 0.0, 0.0, 300.0, 2.7, 0.1, 0.0, 8.0, (10, 10), False, False),  # test_torch_ctf.py:376-392
+        (2.5, 0.0, 0.0, 300.0, 2.7, 0.1, 0.0, 8.0, (10, 10), False, False),
+        (2.0, 0.5, 30.0, 300.0, 2.7, 0.07, 0.0, 1.0, (64, 64), True, True),
+        (0.8, 0.2, 75.0, 200.0, 2.0, 0.1, 20.0, 1.5, (33, 33), True, True),
+        (3.0, 0.0, 0.0, 300.0, 2.7, 0.07, 0.0, 1.0, (128, 128), True, True),
+    ]
+    for i, (df, ast, ang, kv, cs, ac, ps, px, shape, rf, fs) in enumerate(ctf_cases):
+        ctf = calculate_ctf_2d(defocus=df, astigmatism=ast, astigmatism_angle=ang, voltage=kv,
+                               spherical_aberration=cs, amplitude_contrast=ac, phase_shift=ps,
+                               pixel_size=px, image_shape=shape, rfft=rf, fftshift=fs)
+        g[f"ctf_{i}_params"] = np.array([df, ast, ang, kv, cs, ac, ps, px], np.float64)
+        g[f"ctf_{i}_shape"] = np.array(shape)
+        g[f"ctf_{i}_flags"] = np.array([int(rf), int(fs)])
+        g[f"ctf_{i}_out"] = ctf.numpy()
+    g["ctf_cases"] = np.array(len(ctf_cases))
+
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {os.path.getsize(OUT) / 1e6:.2f} MB, {len(g)} arrays")
 

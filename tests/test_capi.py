@@ -93,6 +93,35 @@ def test_validation_rejects_before_launch():
     assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_OK
 
 
+def test_batched_validation_and_layout():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    assert ctypes.sizeof(_lib.CtfParams) == 32
+    assert ctypes.sizeof(_lib.BatchVolume) == 104 + 5 * 8
+    assert L.tt_batch_workspace_bytes() >= 8
+    fake = ctypes.c_void_p(16)
+    arr = (_lib.BatchVolume * 1)(_lib.BatchVolume(_params(), fake, fake, fake, fake, None))
+    assert L.tt_extract_central_slices_rfft_3d_batched(arr, 97, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+    assert L.tt_extract_central_slices_rfft_3d_batched(arr, 1, 3, fake, 256, None) == _lib.TT_ERR_INVALID
+    assert L.tt_extract_central_slices_rfft_3d_batched(arr, 1, 0, None, 0, None) == _lib.TT_ERR_WORKSPACE
+    bad = (_lib.BatchVolume * 1)(_lib.BatchVolume(_params(vol_w=8), None, fake, fake, fake, None))
+    assert L.tt_insert_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+    assert L.tt_extract_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+
+
+def test_ctf_params_rows():
+    from teamtomo_b200.batched import ctf_params
+
+    rows = ctf_params([1.0, 2.0, 3.0], astigmatism_um=0.1)
+    assert rows.shape == (3, 8) and rows.dtype == torch.float32
+    assert torch.equal(rows[:, 0], torch.tensor([1.0, 2.0, 3.0]))
+    assert torch.allclose(rows[:, 1], torch.full((3,), 0.1))
+    assert torch.equal(rows[:, 3], torch.full((3,), 300.0))
+    with pytest.raises(ValueError):
+        ctf_params([1.0, 2.0], astigmatism_um=[0.1, 0.2, 0.3])
+
+
 def test_workspace_query():
     from teamtomo_b200 import _lib
 

@@ -135,6 +135,17 @@ def test_project_backproject(golden, oracle):
     assert rel_l2(bo, golden["backproject_odd_out"]) < 1e-5
 
 
+def test_ctf_matches_reference(golden, oracle):
+    """torch-ctf calculate_ctf_2d golden grids (incl. the 10x10 case of
+    test_torch_ctf.py:376-392), atol 1e-4 as the reference test."""
+    for i in range(int(golden["ctf_cases"])):
+        rf, fs = (bool(x) for x in golden[f"ctf_{i}_flags"])
+        out = oracle.ctf_2d(*golden[f"ctf_{i}_params"], image_shape=tuple(golden[f"ctf_{i}_shape"]),
+                            rfft=rf, fftshift=fs)
+        assert out.shape == golden[f"ctf_{i}_out"].shape
+        np.testing.assert_allclose(out, golden[f"ctf_{i}_out"], atol=1e-4)
+
+
 def test_insert_mirror_is_plane_post_pass(golden, oracle):
     """The reference's per-corner Friedel mirror equals a splat without it
     followed by one post-pass over the x=0 plane (the form the CUDA path uses)."""
