@@ -34,7 +34,7 @@ class SliceParams(ctypes.Structure):
         ("x_tolerance", _f32), ("x_tolerance10", _f32),
         ("has_rot_tolerance", _i32), ("rot_tolerance", _f32),
         ("rotation_f64", _i32), ("volume_unshifted", _i32), ("slices_unshifted", _i32),
-        ("reserved", _i32),
+        ("deterministic", _i32),
     ]
 
 
@@ -75,6 +75,11 @@ SIGNATURES = {
     "tt_insert_accumulate": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_finalize": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp, _vp], _i32),
     "tt_friedel_mirror_x0": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp], _i32),
+    "tt_insert_workspace_bytes": ([_i32, ctypes.POINTER(SliceParams)], _sz),
+    "tt_fixed_absmax": ([_vp, _i32, _i64, _vp, _vp], _i32),
+    "tt_insert_fixed_accumulator_bytes": ([_i64, _i64, _i64, _i64], _sz),
+    "tt_insert_fixed_accumulate": ([_vp, _i32, _vp, _vp, _vp, _i64, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_insert_fixed_finalize": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _vp], _i32),
     "tt_batch_workspace_bytes": ([], _sz),
     "tt_extract_central_slices_rfft_3d_batched": (
         [ctypes.POINTER(BatchVolume), _i32, _i32, _vp, _sz, _vp], _i32),
@@ -128,8 +133,20 @@ def check(status: int, what: str) -> None:
     raise RuntimeError(f"{what}: {msg}")
 
 
+def dense(t: torch.Tensor) -> torch.Tensor:
+    """``t`` as a C-contiguous tensor whose memory holds its values: lazy
+    conjugate / negative views (``x.conj()``, and the gradients autograd
+    passes through them) are materialised first."""
+    return t.resolve_conj().resolve_neg().contiguous()
+
+
 def ptr(t: torch.Tensor | None):
-    return None if t is None else ctypes.c_void_p(t.data_ptr())
+    if t is None:
+        return None
+    if t.is_conj() or t.is_neg():
+        # the memory of a lazy view does not hold its values
+        raise ValueError("tensor is a lazy conjugate/negative view; materialise it with dense()")
+    return ctypes.c_void_p(t.data_ptr())
 
 
 def stream_of(device: torch.device):

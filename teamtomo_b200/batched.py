@@ -112,7 +112,7 @@ def extract_central_slices_rfft_3d_batched(
     for vol, R, shape, c in zip(volumes, rotation_matrices, shapes, ctf):
         if vol.ndim != 3 or vol.dtype != torch.complex64:
             raise ValueError("batched extraction takes complex64 (d, h, w//2+1) volumes")
-        vol = vol.contiguous()
+        vol = _lib.dense(vol)
         Rm, _ = rotation_arg(R, dev)
         n = Rm.shape[0]
         h, w = int(shape[-2]), int(shape[-1])
@@ -164,7 +164,7 @@ def insert_central_slices_rfft_3d_batched(
         n = Rm.shape[0]
         if math.prod(img.shape[:-2]) != n:
             raise ValueError(f"{n} rotation matrices for {math.prod(img.shape[:-2])} slices")
-        img = img.reshape(n, *img.shape[-2:]).contiguous()
+        img = _lib.dense(img.reshape(n, *img.shape[-2:]))
         acc = new_accumulator(shape, False, dev)
         cc = _check_ctf(c, n, dev)
         p = slice_params(n=n, image_shape=shape, volume=None, rotation=Rm, fftfreq_max=fftfreq_max,

@@ -74,12 +74,12 @@ def project_prepare(volume: torch.Tensor, pad: int) -> torch.Tensor:
     _lib.require_cuda(volume)
     if volume.dtype not in (torch.float32, torch.float64):
         volume = volume.to(torch.float32)
-    return _ProjectPrepare.apply(volume.contiguous(), int(pad))
+    return _ProjectPrepare.apply(_lib.dense(volume), int(pad))
 
 
 def recentre_crop_2d(images: torch.Tensor, pad: int) -> torch.Tensor:
     h, w = images.shape[-2:]
-    flat = images.reshape(-1, h, w).contiguous()
+    flat = _lib.dense(images.reshape(-1, h, w))
     return _RecentreCrop2d.apply(flat, int(pad))
 
 
@@ -113,7 +113,7 @@ def backproject_finish(volume: torch.Tensor, pad: int) -> torch.Tensor:
     n0, n1, n2 = volume.shape[-3:]
     lead = volume.shape[:-3]
     channels = volume.numel() // (n0 * n1 * n2)
-    volume = volume.contiguous()
+    volume = _lib.dense(volume)
     out = torch.empty((*lead, n0 - 2 * pad, n1 - 2 * pad, n2 - 2 * pad), dtype=volume.dtype,
                       device=volume.device)
     L = _lib.load()

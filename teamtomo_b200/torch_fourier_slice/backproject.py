@@ -40,7 +40,7 @@ def _backproject(images, rotation_matrices, pad_factor, fftfreq_max, zyx_matrice
     nrot = R.shape[0]
     lead = images.shape[:-3] if channels else images.shape[:-2]
     c = images.shape[-3] if channels else 1
-    flat = images.reshape(-1, d, d).contiguous()
+    flat = _lib.dense(images.reshape(-1, d, d))
     fft_in = _wrappers.pad_fftshift_2d(flat, p)
     spec = torch.fft.rfftn(fft_in, dim=(-2, -1)).reshape(*lead, c, n, n // 2 + 1)
     spec = spec.reshape(nrot, c, n, n // 2 + 1)

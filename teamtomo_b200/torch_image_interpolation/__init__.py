@@ -40,11 +40,11 @@ def sample_image_3d(
     _lib.require_cuda(image)
     code = _code(image.dtype)
     multi = image.ndim == 4
-    img = (image if multi else image[None]).contiguous()
+    img = _lib.dense(image if multi else image[None])
     C, D, H, W = img.shape
     coords = torch.as_tensor(coordinates).to(image.device)
     batch = coords.shape[:-1]
-    c = coords.reshape(-1, 3).to(_REAL[image.dtype]).contiguous()
+    c = _lib.dense(coords.reshape(-1, 3).to(_REAL[image.dtype]))
     n = c.shape[0]
     out = torch.empty((n, C), dtype=image.dtype, device=image.device)
     L = _lib.load()
@@ -86,7 +86,7 @@ def insert_into_image_3d(
         raise ValueError(f"weights must be float32 or float64, got {weights.dtype}")
     code = _code(image.dtype)
     C = image.shape[0] if multi else 1
-    vals = values.to(image.device).reshape(-1, C).contiguous()
+    vals = _lib.dense(values.to(image.device).reshape(-1, C))
     c = coordinates.to(image.device).reshape(-1, 3).float().contiguous()
     img = image if image.is_contiguous() else image.contiguous()
     wts = weights if weights.is_contiguous() else weights.contiguous()
