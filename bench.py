@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1024, help="slices per CPU-baseline sample")
+    ap.add_argument("--deterministic", action="store_true",
+                    help="64-bit fixed-point insertion and volume gradient (bit-reproducible)")
     ap.add_argument("--workload", choices=["differentiation", "batched"], default="differentiation",
                     help="differentiation: the 256^3 extract+insert+bwd step (headline); batched: 32 "
                          "uneven CTF-weighted volumes in one graph-captured launch per stage")
@@ -392,13 +394,21 @@ def main():
             (r,) = ctx.saved_tensors
             return r.mul_(g * (2.0 / ctx.m)), None
 
+    det = bool(args.deterministic)
+
+    def insert(images, rot):
+        # N > 1: every rank splats its own targets, one all-reduce sums the volumes
+        if world > 1:
+            return tt.distributed.insert_central_slices_rfft_3d(images, shape, rot, deterministic=det)
+        return tt.insert_central_slices_rfft_3d(images, shape, rot, deterministic=det)
+
     def step(with_events=False):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)] if with_events else None
         V.grad = None
         R.grad = None
         if ev:
             ev[0].record(stream)
-        S = tt.extract_central_slices_rfft_3d(V, shape, R)
+        S = tt.extract_central_slices_rfft_3d(V, shape, R, deterministic=det)
         if ev:
             ev[1].record(stream)
             S.register_hook(on_grad)
@@ -406,13 +416,11 @@ def main():
         loss.backward()
         if ev:
             ev[2].record(stream)
-        vol, w = tt.insert_central_slices_rfft_3d(T, shape, R.detach())
+        vol, w = insert(T, R.detach())
         if ev:
             ev[3].record(stream)
         if world > 1:
-            dist.all_reduce(V.grad)
-            dist.all_reduce(vol)
-            dist.all_reduce(w)
+            tt.distributed.all_reduce_volume_gradient(V.grad)
         return loss, ev, (vol, w)
 
     for _ in range(max(args.warmup, 0)):
@@ -486,14 +494,12 @@ def main():
             Vd = hV.to(dev, non_blocking=True).requires_grad_(True)
             Rd = hR.to(dev, non_blocking=True).requires_grad_(True)
             Td = hT.to(dev, non_blocking=True)
-            S = tt.extract_central_slices_rfft_3d(Vd, shape, Rd)
+            S = tt.extract_central_slices_rfft_3d(Vd, shape, Rd, deterministic=det)
             loss = _ResidualMSE.apply(S, Td)
             loss.backward()
-            vol, w = tt.insert_central_slices_rfft_3d(Td, shape, Rd.detach())
+            vol, w = insert(Td, Rd.detach())
             if world > 1:
-                dist.all_reduce(Vd.grad)
-                dist.all_reduce(vol)
-                dist.all_reduce(w)
+                tt.distributed.all_reduce_volume_gradient(Vd.grad)
             h_loss.copy_(loss.detach(), non_blocking=True)
             h_dR.copy_(Rd.grad, non_blocking=True)
 
@@ -528,9 +534,12 @@ def main():
             "config": {"workload": WORKLOAD, "box": n, "slices_per_gpu": ns, "global_batch": ns * world,
                        "rotation_seed": ROT_SEED, "l2": "inputs larger than L2 (1.08 GB of targets per step)",
                        "parallelism": f"dp{world}" + (" (all_reduce of d/dvolume and inserted volume)"
-                                                      if world > 1 else "")},
+                                                      if world > 1 else ""),
+                       "deterministic": det},
             "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": 5 * args.steps,
+            # extract, backward, rotation-gradient finish, insert splat, insert finalize
+            # (+ absmax pre-passes and the fixed-point add-back when deterministic)
+            "gpu_launches": (8 if det else 5) * args.steps,
             "loss": float(loss.item()),
         }
         print(json.dumps(line))

@@ -57,7 +57,9 @@ typedef struct tt_slice_params {
     int32_t rotation_f64;          /* rotation matrices are float64 (else float32) */
     int32_t volume_unshifted;      /* volume is plain rfftn output (z, y not fftshifted) */
     int32_t slices_unshifted;      /* slices stored ifftshifted along rows (irfft-ready) */
-    int32_t reserved;
+    int32_t deterministic;         /* 1: insertion and the volume gradient accumulate in 64-bit
+                                      fixed point, bit-identical for any launch order (the
+                                      workspace queries grow accordingly) */
 } tt_slice_params;
 
 /* Per-image contrast transfer function, the scalar arguments of torch-ctf's
@@ -99,7 +101,8 @@ int tt_slice_geometry(const void *rotation_matrices, int32_t mode, uint8_t *flag
                       const tt_slice_params *p, void *stream);
 
 /* Bytes of workspace tt_extract_central_slices_rfft_3d_backward needs when a
- * rotation gradient is requested (0 otherwise is also accepted then). */
+ * rotation gradient or (p->deterministic) a volume gradient is requested
+ * (otherwise 0 is also accepted). */
 size_t tt_extract_backward_workspace_bytes(const tt_slice_params *p);
 
 /* Backward of the extraction.  grad_slices: complex64 (n, img_h, img_w/2+1),
@@ -107,7 +110,9 @@ size_t tt_extract_backward_workspace_bytes(const tt_slice_params *p);
  * grad_volume (nullable): complex64 (vol_d, vol_h, vol_w), ACCUMULATED into.
  * grad_rotation (nullable): (n, 3, 3) in the rotation dtype, overwritten; the
  * elements zeroed by rot_tolerance get zero gradient.  The rotation gradient
- * is reduced deterministically through the caller's workspace.
+ * is reduced deterministically through the caller's workspace; with
+ * p->deterministic the volume gradient is accumulated in 64-bit fixed point
+ * there too (scale from the grads' max |re|, |im| and n) and then added in.
  * Replaces the autograd graph of extract_central_slices_rfft_3d
  * (grid_sampler_3d_backward + the coordinate chain of _dft_utils.py:61-67). */
 int tt_extract_central_slices_rfft_3d_backward(const void *volume_rfft,
@@ -137,6 +142,8 @@ int tt_extract_central_slices_rfft_3d_backward(const void *volume_rfft,
  *    stream capture.
  *  - All calls share the array: calls that overlap on the GPU race and must be
  *    serialised by the caller.  Nothing needs clearing between calls.
+ *  - The deterministic (fixed-point) volume gradient needs a workspace: a
+ *    call with p->deterministic and a grad_volume fails with TT_ERR_INVALID.
  * This entry point has no counterpart in the reference. */
 int tt_extract_central_slices_rfft_3d_backward_noalloc(const void *volume_rfft,
                                                        const void *rotation_matrices,
@@ -181,6 +188,54 @@ int tt_insert_finalize(const void *accumulator, int32_t complex128, int64_t chan
  * NULL).  In place. */
 int tt_friedel_mirror_x0(void *volume_rfft, void *weights, int32_t complex128, int64_t channels,
                          int64_t d, int64_t h, int64_t w_rfft, void *stream);
+
+/* ---- deterministic scatters (64-bit fixed point) ----------------------
+ * Every contribution data*w is rounded to a 64-bit integer at a power-of-two
+ * scale and added with integer atomics, which are associative: the sums are
+ * identical for any launch order, any split of the slices into calls and,
+ * summing accumulators with an integer all-reduce, any number of GPUs.  The
+ * scale follows from a bound on |data| (the float32 bit pattern of max |re|,
+ * |im| -- see tt_fixed_absmax) and on the number of slices ever added to the
+ * accumulator (max_slices): data scale 2^(54 - ceil(log2 max_slices) - E)
+ * with |data| < 2^E, weight scale 2^(54 - ceil(log2 max_slices)), which keeps
+ * every sum below 2^62 (a voxel receives at most 256 contributions of at most
+ * |data| per slice, Friedel completion included).  All calls that add into
+ * one accumulator must use the same absmax value and max_slices.  Non-finite
+ * data are not supported in this mode.
+ * One-shot use: set tt_slice_params.deterministic = 1 on
+ * tt_insert_central_slices_rfft_3d (workspace: tt_insert_workspace_bytes) or
+ * on tt_extract_central_slices_rfft_3d_backward (volume gradient; workspace:
+ * tt_extract_backward_workspace_bytes).  The reference accumulates with
+ * float atomics (index_put_ with accumulate=True) and has no such mode. */
+
+/* Bytes of workspace tt_insert_central_slices_rfft_3d needs for p
+ * (p->deterministic selects the fixed-point layout). */
+size_t tt_insert_workspace_bytes(int32_t complex128, const tt_slice_params *p);
+
+/* *absmax_bits = max(*absmax_bits, bits of max |x| over count float32 (is_f64 = 0)
+ * or float64 (is_f64 = 1, rounded up to float32) values).  Non-negative
+ * float32 values order like their bit patterns, so the caller zeroes the word
+ * once and may run this over several buffers (or all-reduce it with MAX). */
+int tt_fixed_absmax(const void *data, int32_t is_f64, int64_t count, uint32_t *absmax_bits,
+                    void *stream);
+
+/* Bytes of a fixed-point insertion accumulator: 4 int64 (re, im, w, pad) per voxel. */
+size_t tt_insert_fixed_accumulator_bytes(int64_t channels, int64_t d, int64_t h, int64_t w_rfft);
+
+/* Two-stage deterministic insertion: adds the splat of n slices into a
+ * caller-zeroed fixed-point accumulator, at the scale given by *absmax_bits
+ * (device memory) and max_slices. */
+int tt_insert_fixed_accumulate(const void *image_rfft, int32_t complex128,
+                               const void *rotation_matrices, void *accumulator,
+                               const uint32_t *absmax_bits, int64_t max_slices,
+                               const tt_slice_params *p, void *stream);
+
+/* Fixed-point accumulator -> volume (channels, d, h, w_rfft) and weights
+ * (d, h, w_rfft, may be NULL), Friedel completion of the x=0 plane done in
+ * integers, then one conversion back at the same scale. */
+int tt_insert_fixed_finalize(const void *accumulator, int32_t complex128, int64_t channels,
+                             int64_t d, int64_t h, int64_t w_rfft, const uint32_t *absmax_bits,
+                             int64_t max_slices, void *volume_rfft, void *weights, void *stream);
 
 /* ---- batched, CTF-weighted slices over many volumes -------------------
  * Many volumes of uneven box size, each with its own rotations and optional

@@ -278,6 +278,110 @@ def mirror_x0_post_pass(vol, wts):
 
 
 # ----------------------------------------------------------------------------
+# deterministic insertion: 64-bit fixed point (numpy, bit-exact restatement of
+# the CUDA fixed-point mode; the reference has no such mode, so it is pinned
+# through its float outputs)
+# ----------------------------------------------------------------------------
+
+FIXED_HEADROOM_BITS = 8
+
+
+def _ceil_log2(n: int) -> int:
+    l = 0
+    while l < 62 and (1 << l) < n:
+        l += 1
+    return l
+
+
+def fixed_absmax_bits(*arrays) -> int:
+    """uint32 bit pattern of max |re|, |im| over the arrays, as float32
+    (float64 magnitudes rounded up to float32)."""
+    best = np.float32(0)
+    for a in arrays:
+        a = np.asarray(a)
+        if a.size == 0:
+            continue
+        real = a.view(a.real.dtype) if np.iscomplexobj(a) else a
+        v = np.abs(real).max()
+        f = np.float32(v)
+        if float(f) < float(v):
+            f = np.nextafter(f, np.float32(np.inf))
+        best = max(best, f)
+    return int(np.array([best], np.float32).view(np.uint32)[0])
+
+
+def fixed_scales(absmax_bits: int, max_slices: int) -> tuple[float, float]:
+    """(data scale, weight scale): 2^(62 - 8 - ceil(log2 max_slices) - E) with
+    |data| < 2^E, and 2^(62 - 8 - ceil(log2 max_slices))."""
+    a = np.array([absmax_bits], np.uint32).view(np.float32)[0]
+    e = 0
+    if 0 < a <= np.finfo(np.float32).max:
+        e = int(np.frexp(a)[1])
+    l = _ceil_log2(int(max_slices))
+    return 2.0 ** (62 - FIXED_HEADROOM_BITS - l - e), 2.0 ** (62 - FIXED_HEADROOM_BITS - l)
+
+
+def insert_fixed(image_rfft, volume_shape, rotation_matrices, absmax_bits, max_slices,
+                 fftfreq_max=None, zyx_matrices=False):
+    """Fixed-point accumulator (d, h, w//2+1, 3) int64 (re, im, w) of the
+    deterministic insertion, before the Friedel completion.  Same pixels,
+    redirect, bounds and float32 corner weights ((1-t) / t products, left to
+    right) as insert(); each term data*w rounded once (half to even)."""
+    img = np.asarray(image_rfft)
+    vd, vh, vw = (int(s) for s in volume_shape)
+    wr = vw // 2 + 1
+    r = _rot_f32(rotation_matrices)
+    n = r.shape[0]
+    img = img.reshape(n, vh, wr)
+    flags, coords = slice_geometry(r, volume_shape, (vd, vh, wr), 1, fftfreq_max=fftfreq_max,
+                                   zyx_matrices=zyx_matrices)
+    sel = (flags & 5) == 5
+    c = coords[sel]
+    d = img[sel]
+    re = d.real.astype(np.float64)
+    im = np.where((flags[sel] & 2) != 0, -d.imag, d.imag).astype(np.float64)
+    lo = np.floor(c)
+    hi = np.ceil(c)
+    t = (c - lo).astype(np.float32)
+    one = np.float32(1)
+    sd, sw = fixed_scales(absmax_bits, max_slices)
+    acc = np.zeros((vd * vh * wr, 3), np.int64)
+    for k in range(8):
+        b = ((k >> 2) & 1, (k >> 1) & 1, k & 1)
+        f = [t[:, a] if b[a] else one - t[:, a] for a in range(3)]
+        w = (f[0] * f[1]) * f[2]
+        idx = [(hi if b[a] else lo)[:, a].astype(np.int64) for a in range(3)]
+        vi = (idx[0] * vh + idx[1]) * wr + idx[2]
+        nz = w != 0
+        w64 = w.astype(np.float64)
+        for col, val in ((0, re * w64 * sd), (1, im * w64 * sd), (2, w64 * 1.0 * sw)):
+            np.add.at(acc[:, col], vi[nz], np.rint(val[nz]).astype(np.int64))
+    return acc.reshape(vd, vh, wr, 3)
+
+
+def fixed_finalize(acc, absmax_bits, max_slices, complex128=False):
+    """Fixed-point accumulator (d, h, w, 3) -> (volume, weights): Friedel
+    completion of the x=0 plane on the integers, then one conversion."""
+    a = np.array(acc, dtype=np.int64, copy=True)
+    d, h = a.shape[:2]
+    z = np.arange(d)[:, None]
+    y = np.arange(h)[None, :]
+    zm, ym = (d - z) % d, (h - y) % h
+    keep = ~((zm == d // 2) & (ym == h // 2))
+    p = np.array(acc[:, :, 0, :], dtype=np.int64)
+    a[:, :, 0, 0] = p[..., 0] + np.where(keep, p[zm, ym, 0], 0)
+    a[:, :, 0, 1] = p[..., 1] - np.where(keep, p[zm, ym, 1], 0)
+    a[:, :, 0, 2] = p[..., 2] + np.where(keep, p[zm, ym, 2], 0)
+    sd, sw = fixed_scales(absmax_bits, max_slices)
+    real = np.float64 if complex128 else np.float32
+    vol = np.empty(a.shape[:3], np.complex128 if complex128 else np.complex64)
+    vol.real = (a[..., 0].astype(np.float64) * (1.0 / sd)).astype(real)
+    vol.imag = (a[..., 1].astype(np.float64) * (1.0 / sd)).astype(real)
+    wts = (a[..., 2].astype(np.float64) * (1.0 / sw)).astype(real)
+    return vol, wts
+
+
+# ----------------------------------------------------------------------------
 # torch_image_interpolation restatements (numpy)
 # ----------------------------------------------------------------------------
 

@@ -5,7 +5,7 @@ the 3D interpolation API of torch-image-interpolation, running on
 hand-written sm_100a CUDA kernels through the C ABI in include/teamtomo_b200.h.
 """
 
-from . import torch_fourier_slice, torch_image_interpolation
+from . import distributed, torch_fourier_slice, torch_image_interpolation
 from .torch_fourier_slice import (
     backproject_2d_to_3d,
     backproject_2d_to_3d_multichannel,
@@ -21,6 +21,7 @@ from .torch_image_interpolation import insert_into_image_3d, sample_image_3d
 __version__ = "0.1.0"
 
 __all__ = [
+    "distributed",
     "torch_fourier_slice",
     "torch_image_interpolation",
     "backproject_2d_to_3d",

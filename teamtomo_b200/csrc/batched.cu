@@ -154,6 +154,8 @@ static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_
     for (int v = 0; v < n_volumes; v++) {
         const tt_batch_volume& x = volumes[v];
         if (int e = validate_params(&x.params)) return e;
+        if (x.params.deterministic)
+            return fail(TT_ERR_INVALID, "%s: volume %d: the batched launch has no deterministic mode", what, v);
         if (x.params.n > 0) {
             if (!x.rotation_matrices || !x.slices) return fail(TT_ERR_INVALID, "%s: volume %d: NULL pointer", what, v);
             if (insert) {

@@ -46,6 +46,7 @@ inline int validate_params(const tt_slice_params* p) {
     if ((long long)p->img_h * (p->img_w / 2 + 1) >= lim || p->vol_d * p->vol_h * p->vol_w >= lim * 4)
         return fail(TT_ERR_INVALID, "slice or volume too large");
     if (p->n > (1LL << 31) - 1) return fail(TT_ERR_INVALID, "too many slices");
+    if (p->deterministic != 0 && p->deterministic != 1) return fail(TT_ERR_INVALID, "deterministic must be 0 or 1");
     return TT_OK;
 }
 

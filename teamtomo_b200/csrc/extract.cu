@@ -21,6 +21,7 @@
 #include <mutex>
 
 #include "capi_util.cuh"
+#include "fixed_point.cuh"
 #include "slice_common.cuh"
 #include "slice_ops.cuh"
 
@@ -54,12 +55,29 @@ extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     __stcs(out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, r);
 }
 
+// Volume-gradient target: float2 atomics, or (FIXED, the deterministic mode)
+// two 64-bit fixed-point words per voxel at scale `scale`.
+template <bool FIXED>
+struct DvTarget {
+    float2* dvol;
+    unsigned long long* fixed;
+    double scale;
+    __device__ __forceinline__ void add(int64_t vi, float2 gv, float w) const {
+        if (FIXED) {
+            fixed_add(fixed + 2 * vi, (double)gv.x * (double)w * scale);
+            fixed_add(fixed + 2 * vi + 1, (double)gv.y * (double)w * scale);
+        } else {
+            atomicAdd(dvol + vi, make_float2(gv.x * w, gv.y * w));
+        }
+    }
+};
+
 // Backward of one slice pixel; acc receives the pixel's 6 contributions to
 // d/dR_zyx (rows z, y, x x columns y, x — column 0 multiplies the zero z
 // frequency of a central slice).
-template <bool WANT_DV, bool WANT_DR>
+template <bool WANT_DV, bool WANT_DR, bool FIXED>
 __device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const float* m,
-                                          const float2* __restrict__ grad, float2* __restrict__ dvol,
+                                          const float2* __restrict__ grad, const DvTarget<FIXED>& dv,
                                           const SliceGeom& g, int64_t s, int iy, int ix, float acc[6]) {
     float qy, qx, c[3];
     bool cj = false;
@@ -81,7 +99,7 @@ __device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const 
                 for (int bx = 0; bx < 2; bx++) {
                     if (bx && !k.xin) continue;
                     const float w = (bx ? k.ax1 : k.ax0) * wzy;
-                    if (w != 0.0f) atomicAdd(dvol + base + bx, make_float2(gv.x * w, gv.y * w));
+                    if (w != 0.0f) dv.add(base + bx, gv, w);
                 }
             }
         }
@@ -133,11 +151,13 @@ __device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const 
 
 // One block per (slice, tile).  WANT_DR: the block's partial sums of the 6
 // non-zero entries of d/dR_zyx go to part[(s * tiles + tile) * 6 + k],
-// reduced in double within the block.
-template <bool WANT_DV, bool WANT_DR>
+// reduced in double within the block.  FIXED: the volume gradient goes to the
+// fixed-point words `fixed` at the scale set by *absmax and n.
+template <bool WANT_DV, bool WANT_DR, bool FIXED>
 __global__ void __launch_bounds__(kExtractThreads)
 extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
                    const float2* __restrict__ grad, float2* __restrict__ dvol,
+                   unsigned long long* __restrict__ fixed, const uint32_t* __restrict__ absmax,
                    float* __restrict__ part, SliceGeom g, int tiles) {
     __shared__ float m[9];
     __shared__ double red[kExtractThreads / 32][6];
@@ -146,8 +166,10 @@ extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     load_rotation(m, rot, s, g, true);
     __syncthreads();
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    DvTarget<FIXED> dv{dvol, fixed, 0.0};
+    if (FIXED) dv.scale = fixed_data_scale(*absmax, ceil_log2(g.n));
     int iy, ix;
-    if (tile_pixel(g, tile, iy, ix)) bwd_point<WANT_DV, WANT_DR>(vol, m, grad, dvol, g, s, iy, ix, acc);
+    if (tile_pixel(g, tile, iy, ix)) bwd_point<WANT_DV, WANT_DR, FIXED>(vol, m, grad, dv, g, s, iy, ix, acc);
     if (WANT_DR) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -229,20 +251,58 @@ __global__ void slice_geometry_kernel(const void* __restrict__ rot, uint8_t* __r
 
 static int extract_tiles(const SliceGeom& g) { return tiles_per_slice(g.img_h, g.wr); }
 
+// grad_volume += the fixed-point volume gradient, converted back once.
+__global__ void dv_fixed_add_kernel(const long long* __restrict__ fixed, float2* __restrict__ dvol,
+                                    const uint32_t* __restrict__ absmax, int slices_log2, int64_t voxels) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= voxels) return;
+    const double inv = 1.0 / fixed_data_scale(*absmax, slices_log2);
+    const longlong2 q = reinterpret_cast<const longlong2*>(fixed)[i];
+    float2 o = dvol[i];
+    o.x += (float)((double)q.x * inv);
+    o.y += (float)((double)q.y * inv);
+    dvol[i] = o;
+}
+
 static size_t partial_bytes(int64_t n, int tiles) { return (size_t)(n * tiles * 6) * sizeof(float); }
 
+// Fixed-point volume gradient of the deterministic mode: 256-byte header
+// (absmax word) + 2 words per voxel, ahead of the rotation partials.
+static size_t fixed_dv_bytes(const tt_slice_params* p) {
+    return p->deterministic ? kFixedHeaderBytes + (size_t)(p->vol_d * p->vol_h * p->vol_w) * 16 : 0;
+}
+
 // Launches the backward and the rotation-gradient reduction; `part` holds
-// n * tiles * 6 floats when grad_rotation is set.
+// n * tiles * 6 floats when grad_rotation is set; `fixed` (deterministic
+// volume gradient) is the zeroed header + accumulator of fixed_dv_bytes.
 static int launch_backward(const float2* v, const void* rot, const float2* gr, float2* dv, void* grad_rotation,
-                           float* part, const SliceGeom& g, cudaStream_t st) {
+                           float* part, const SliceGeom& g, cudaStream_t st, void* fixed = nullptr) {
     const int tiles = extract_tiles(g);
     const unsigned blocks = (unsigned)((int64_t)g.n * tiles);
-    if (dv && grad_rotation)
-        extract_bwd_kernel<true, true><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, part, g, tiles);
-    else if (dv)
-        extract_bwd_kernel<true, false><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, part, g, tiles);
-    else
-        extract_bwd_kernel<false, true><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, part, g, tiles);
+    uint32_t* absmax = (uint32_t*)fixed;
+    unsigned long long* facc = fixed ? (unsigned long long*)((char*)fixed + kFixedHeaderBytes) : nullptr;
+    if (dv && fixed) {
+        if (int e = launch_fixed_absmax(gr, 0, (int64_t)g.n * g.img_h * g.wr * 2, absmax, st)) return e;
+        if (grad_rotation)
+            extract_bwd_kernel<true, true, true><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, facc, absmax,
+                                                                                    part, g, tiles);
+        else
+            extract_bwd_kernel<true, false, true><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, facc, absmax,
+                                                                                     part, g, tiles);
+        if (int e = check_launch("extract_bwd_kernel")) return e;
+        const int64_t vox = (int64_t)g.D * g.H * g.W;
+        dv_fixed_add_kernel<<<(unsigned)((vox + 255) / 256), 256, 0, st>>>((const long long*)facc, dv, absmax,
+                                                                           ceil_log2(g.n), vox);
+    } else if (dv && grad_rotation) {
+        extract_bwd_kernel<true, true, false><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
+                                                                                 part, g, tiles);
+    } else if (dv) {
+        extract_bwd_kernel<true, false, false><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
+                                                                                  part, g, tiles);
+    } else {
+        extract_bwd_kernel<false, true, false><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
+                                                                                  part, g, tiles);
+    }
     if (int e = check_launch("extract_bwd_kernel")) return e;
     if (grad_rotation) {
         const int64_t total = (int64_t)g.n * 9;
@@ -288,7 +348,7 @@ extern "C" int tt_slice_geometry(const void* rotation_matrices, int32_t mode, ui
 
 extern "C" size_t tt_extract_backward_workspace_bytes(const tt_slice_params* p) {
     if (!p || p->n <= 0 || p->img_h < 1 || p->img_w < 1) return 0;
-    return partial_bytes(p->n, tiles_per_slice((int)p->img_h, (int)(p->img_w / 2 + 1)));
+    return fixed_dv_bytes(p) + partial_bytes(p->n, tiles_per_slice((int)p->img_h, (int)(p->img_w / 2 + 1)));
 }
 
 extern "C" int tt_extract_central_slices_rfft_3d_backward(
@@ -302,14 +362,21 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward(
     SliceGeom g = make_geom(*p);
     const int tiles = extract_tiles(g);
     if ((int64_t)g.n * tiles > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract backward: too many blocks");
-    if (grad_rotation) {
-        const size_t need = partial_bytes(g.n, tiles);
+    const size_t fixed = grad_volume ? fixed_dv_bytes(p) : 0;
+    if (grad_rotation || fixed) {
+        const size_t need = fixed + (grad_rotation ? partial_bytes(g.n, tiles) : 0);
         if (!workspace || workspace_bytes < need)
             return fail(TT_ERR_WORKSPACE, "extract backward: workspace of %zu bytes needed, got %zu", need,
                         workspace_bytes);
     }
+    cudaStream_t st = as_stream(stream);
+    if (fixed) {
+        cudaError_t e = cudaMemsetAsync(workspace, 0, fixed, st);
+        if (e != cudaSuccess) return fail(TT_ERR_CUDA, "extract backward: memset: %s", cudaGetErrorString(e));
+    }
     return launch_backward((const float2*)volume_rfft, rotation_matrices, (const float2*)grad_slices,
-                           (float2*)grad_volume, grad_rotation, (float*)workspace, g, as_stream(stream));
+                           (float2*)grad_volume, grad_rotation, (float*)((char*)workspace + fixed), g, st,
+                           fixed ? workspace : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -371,6 +438,9 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward_noalloc(const void* vo
     if (!volume_rfft || !rotation_matrices || !grad_slices)
         return fail(TT_ERR_INVALID, "noalloc backward: NULL pointer argument");
     if (!grad_volume && !grad_rotation) return TT_OK;
+    if (p->deterministic && grad_volume)
+        return fail(TT_ERR_INVALID, "noalloc backward: the deterministic volume gradient needs a workspace "
+                                    "(tt_extract_central_slices_rfft_3d_backward)");
     SliceGeom g = make_geom(*p);
     const int tiles = extract_tiles(g);
     if ((int64_t)g.n * tiles > 0x7fffffffLL) return fail(TT_ERR_INVALID, "noalloc backward: too many blocks");

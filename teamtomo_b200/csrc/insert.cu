@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include "capi_util.cuh"
+#include "fixed_point.cuh"
 #include "slice_common.cuh"
 #include "slice_ops.cuh"
 
@@ -123,6 +124,9 @@ __global__ void mirror_x0_kernel(typename Acc<R>::C* __restrict__ vol, R* __rest
     }
 }
 
+int insert_deterministic(const void* image_rfft, int32_t complex128, const void* rot, void* volume, void* weights,
+                         void* workspace, const tt_slice_params* p, cudaStream_t st);
+
 static int check_insert_params(const tt_slice_params* p) {
     if (int e = validate_params(p)) return e;
     if (p->vol_d != p->img_d || p->vol_h != p->img_h || p->vol_w != p->img_w / 2 + 1)
@@ -169,9 +173,18 @@ extern "C" size_t tt_insert_accumulator_bytes(int32_t complex128, int64_t channe
     return (size_t)(channels * d * h * w_rfft) * (complex128 ? sizeof(double4) : sizeof(float4));
 }
 
+extern "C" size_t tt_insert_workspace_bytes(int32_t complex128, const tt_slice_params* p) {
+    if (!p) return 0;
+    if (p->deterministic) return kFixedHeaderBytes + tt_insert_fixed_accumulator_bytes(1, p->vol_d, p->vol_h, p->vol_w);
+    return tt_insert_accumulator_bytes(complex128, 1, p->vol_d, p->vol_h, p->vol_w);
+}
+
 extern "C" int tt_insert_accumulate(const void* image_rfft, int32_t complex128, const void* rotation_matrices,
                                     void* accumulator, const tt_slice_params* p, void* stream) {
     if (int e = check_insert_params(p)) return e;
+    if (p->deterministic)
+        return fail(TT_ERR_INVALID, "insert_accumulate: the deterministic mode accumulates through "
+                                    "tt_insert_fixed_accumulate");
     if (p->n == 0) return TT_OK;
     if (!image_rfft || !rotation_matrices || !accumulator)
         return fail(TT_ERR_INVALID, "insert_accumulate: NULL pointer argument");
@@ -193,10 +206,12 @@ extern "C" int tt_insert_central_slices_rfft_3d(const void* image_rfft, int32_t 
     if (int e = check_insert_params(p)) return e;
     if (!volume_rfft || !weights || (p->n > 0 && (!image_rfft || !rotation_matrices)))
         return fail(TT_ERR_INVALID, "insert: NULL pointer argument");
-    const size_t need = tt_insert_accumulator_bytes(complex128, 1, p->vol_d, p->vol_h, p->vol_w);
+    const size_t need = tt_insert_workspace_bytes(complex128, p);
     if (!workspace || workspace_bytes < need)
         return fail(TT_ERR_WORKSPACE, "insert: workspace of %zu bytes needed, got %zu", need, workspace_bytes);
     cudaStream_t st = as_stream(stream);
+    if (p->deterministic)
+        return insert_deterministic(image_rfft, complex128, rotation_matrices, volume_rfft, weights, workspace, p, st);
     cudaError_t e = cudaMemsetAsync(workspace, 0, need, st);
     if (e != cudaSuccess) return fail(TT_ERR_CUDA, "insert: memset: %s", cudaGetErrorString(e));
     if (p->n > 0)

@@ -172,14 +172,24 @@ __device__ __forceinline__ void acc_add(double4* a, double re, double im, double
 __device__ __forceinline__ float2 load_slice(const float2* p) { return __ldcs(p); }
 __device__ __forceinline__ double2 load_slice(const double2* p) { return __ldcs(p); }
 
-// Splat of one source pixel into the (re, im, w) accumulator, following
-// _insert_central_slices_rfft_3d.py:30-85 and _insert_into_3d_dft_linear
-// :289-346.  With a CTF (ctf != nullptr) the data are weighted by the CTF
-// and the interpolation weights by its square.
+// Float accumulation target: one (re, im, w, 0) vector reduction per corner.
 template <typename R>
-__device__ __forceinline__ void insert_point(const typename Acc<R>::C* __restrict__ img, const float* m,
-                                             typename Acc<R>::T* __restrict__ acc, const SliceGeom& g, int64_t s,
-                                             int iy, int ix, const CtfConst* ctf = nullptr) {
+struct FloatSplat {
+    typename Acc<R>::T* acc;
+    __device__ __forceinline__ void operator()(int64_t vi, R dre, R dim, R w, R wscale) const {
+        acc_add(acc + vi, dre * w, dim * w, w * wscale);
+    }
+};
+
+// Splat of one source pixel, following _insert_central_slices_rfft_3d.py:30-85
+// and _insert_into_3d_dft_linear :289-346: each of the eight corners receives
+// (data * w, w) through sink(voxel, re, im, w, weight scale).  With a CTF
+// (ctf != nullptr) the data are weighted by the CTF and the interpolation
+// weights by its square.
+template <typename R, typename Sink>
+__device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __restrict__ img, const float* m,
+                                                const Sink& sink, const SliceGeom& g, int64_t s, int iy, int ix,
+                                                const CtfConst* ctf = nullptr) {
     const float qy = shifted_freq(iy, g.img_h, g.inv_h);
     const float qx = __fmul_rn((float)ix, g.inv_w);
     if (!in_fmax(g, qy, qx)) return;
@@ -215,9 +225,16 @@ __device__ __forceinline__ void insert_point(const typename Acc<R>::C* __restric
         const float w = (fz * fy) * fx;
         if (w == 0.0f) continue;  // adds nothing (ceil == floor or zero fraction)
         const int64_t vi = vox_index(g, bz ? iz1 : iz0, by ? iy1 : iy0, bx ? ix1 : ix0);
-        const R rw = (R)w;
-        acc_add(acc + vi, dre * rw, dim * rw, rw * wscale);
+        sink(vi, dre, dim, (R)w, wscale);
     }
+}
+
+// Splat into the float (re, im, w, 0) accumulator.
+template <typename R>
+__device__ __forceinline__ void insert_point(const typename Acc<R>::C* __restrict__ img, const float* m,
+                                             typename Acc<R>::T* __restrict__ acc, const SliceGeom& g, int64_t s,
+                                             int iy, int ix, const CtfConst* ctf = nullptr) {
+    insert_point_to<R>(img, m, FloatSplat<R>{acc}, g, s, iy, ix, ctf);
 }
 
 }  // namespace tt

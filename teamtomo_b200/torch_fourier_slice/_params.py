@@ -30,7 +30,7 @@ def _f32(x: float) -> float:
 
 def slice_params(n, image_shape, volume, rotation, fftfreq_max=None, zyx_matrices=False,
                  x_tolerance=1e-8, rot_tolerance=None, volume_unshifted=False,
-                 slices_unshifted=False, vol_dims=None) -> _lib.SliceParams:
+                 slices_unshifted=False, vol_dims=None, deterministic=False) -> _lib.SliceParams:
     d, h, w = (int(s) for s in image_shape)
     vd, vh, vw = vol_dims if vol_dims is not None else tuple(int(s) for s in volume.shape[-3:])
     p = _lib.SliceParams()
@@ -47,7 +47,13 @@ def slice_params(n, image_shape, volume, rotation, fftfreq_max=None, zyx_matrice
     p.rotation_f64 = int(rotation.dtype == torch.float64)
     p.volume_unshifted = int(bool(volume_unshifted))
     p.slices_unshifted = int(bool(slices_unshifted))
+    p.deterministic = int(bool(deterministic))
     return p
+
+
+def resolve_deterministic(flag: bool | None) -> bool:
+    """``None`` follows ``torch.use_deterministic_algorithms``."""
+    return torch.are_deterministic_algorithms_enabled() if flag is None else bool(flag)
 
 
 def rfft_shape(shape):

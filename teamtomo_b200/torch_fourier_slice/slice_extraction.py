@@ -6,6 +6,11 @@ and runs on the sm_100a gather kernel.  It is differentiable w.r.t. the volume
 and the rotation matrices through one fused backward kernel; interpolation
 weights are recomputed in the backward pass, not stored.
 
+Deterministic mode (``deterministic=True``, or ``None`` with
+``torch.use_deterministic_algorithms(True)``): the volume gradient is
+accumulated in 64-bit fixed point and is bit-identical from run to run; the
+rotation gradient is reduced in a fixed order in both modes.
+
 Deliberate difference: the reference zeroes near-zero rotation elements IN
 PLACE on the caller's float32 tensor (:147-151), which also raises for a leaf
 that requires grad.  Here the caller's tensor is never modified; the zeroing
@@ -18,7 +23,7 @@ from __future__ import annotations
 import torch
 
 from .. import _lib
-from ._params import rotation_arg, slice_params
+from ._params import resolve_deterministic, rotation_arg, slice_params
 
 
 class _ExtractCentralSlices(torch.autograd.Function):
@@ -54,13 +59,13 @@ def extract_backward(volume_rfft, rotation_matrices, grad, params, want_volume=T
                      want_rotation=True):
     """Fused backward: (d/dvolume, d/drotation) for upstream slice gradient ``grad``."""
     dev = volume_rfft.device
-    grad = grad.to(torch.complex64).contiguous()
+    grad = _lib.dense(grad.to(torch.complex64))
     L = _lib.load()
     dvol = torch.zeros_like(volume_rfft) if want_volume else None
     drot = torch.empty_like(rotation_matrices) if want_rotation else None
     ws = None
     nbytes = 0
-    if want_rotation:
+    if want_rotation or (want_volume and params.deterministic):
         nbytes = int(L.tt_extract_backward_workspace_bytes(params))
         ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     _lib.check(
@@ -80,6 +85,7 @@ def extract_central_slices_rfft_3d(
     zyx_matrices: bool = False,
     x_tolerance: float = 1e-8,
     rot_tolerance: float | None = 1e-8,
+    deterministic: bool | None = None,
 ) -> torch.Tensor:
     """Extract central slices from an fftshifted rfft volume.
 
@@ -87,7 +93,8 @@ def extract_central_slices_rfft_3d(
     ``(d, d, d//2+1)`` complex64 (fftshifted in the first two dims),
     ``image_shape`` the real-space shape defining the slice grid,
     ``rotation_matrices`` ``(..., 3, 3)``; returns ``(..., h, w//2+1)``
-    complex64 slices (zero outside ``fftfreq_max``).
+    complex64 slices (zero outside ``fftfreq_max``).  ``deterministic``
+    (not in the reference) selects the fixed-point volume gradient.
     """
     assert volume_rfft.ndim == 3, "Input volume_rfft must be 3D tensor."
     _lib.require_cuda(volume_rfft)
@@ -95,12 +102,13 @@ def extract_central_slices_rfft_3d(
         raise RuntimeError(
             f"extract_central_slices_rfft_3d supports complex64 volumes (got {volume_rfft.dtype})"
         )
-    volume_rfft = volume_rfft.contiguous()
+    volume_rfft = _lib.dense(volume_rfft)
     R, stack = rotation_arg(rotation_matrices, volume_rfft.device)
     h, w = int(image_shape[-2]), int(image_shape[-1])
     params = slice_params(n=R.shape[0], image_shape=image_shape, volume=volume_rfft,
                           rotation=R, fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
-                          x_tolerance=x_tolerance, rot_tolerance=rot_tolerance)
+                          x_tolerance=x_tolerance, rot_tolerance=rot_tolerance,
+                          deterministic=resolve_deterministic(deterministic))
     out = _ExtractCentralSlices.apply(volume_rfft, R, params, (R.shape[0], h, w // 2 + 1))
     return out.reshape(*stack, h, w // 2 + 1)
 
@@ -147,6 +155,7 @@ def extract_central_slices_rfft_3d_multichannel(
     zyx_matrices: bool = False,
     x_tolerance: float = 1e-8,
     rot_tolerance: float | None = 1e-8,
+    deterministic: bool | None = None,
 ) -> torch.Tensor:  # (..., c, h, w)
     """Multichannel extraction (_extract_central_slices_rfft_3d.py:225-367):
     ``(c, d, d, d//2+1)`` -> ``(..., c, h, w//2+1)``, the same rotations for
@@ -155,7 +164,8 @@ def extract_central_slices_rfft_3d_multichannel(
     slices = [
         extract_central_slices_rfft_3d(volume_rfft[c], image_shape, rotation_matrices,
                                        fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
-                                       x_tolerance=x_tolerance, rot_tolerance=rot_tolerance)
+                                       x_tolerance=x_tolerance, rot_tolerance=rot_tolerance,
+                                       deterministic=deterministic)
         for c in range(volume_rfft.shape[0])
     ]
     return torch.stack(slices, dim=-3)

@@ -7,6 +7,13 @@ complex64 slices give a complex64 volume with float32 weights, complex128
 slices a complex128 volume with float64 weights.  The splat runs on the
 sm_100a scatter kernel into an (re, im, w) accumulator; one finalize pass
 applies the Friedel completion of the x=0 plane and writes the two outputs.
+
+Deterministic mode (``deterministic=True``, or ``None`` with
+``torch.use_deterministic_algorithms(True)``; not in the reference): the splat
+accumulates in 64-bit fixed point, so the outputs are bit-identical for any
+launch order, any split of the slices into calls and any slice order.  The
+scale comes from max |re|, |im| of all images that go into one accumulator
+(``fixed_absmax``) and the total slice count (``max_slices``).
 """
 
 from __future__ import annotations
@@ -16,7 +23,7 @@ import math
 import torch
 
 from .. import _lib
-from ._params import rfft_shape, rotation_arg, slice_params
+from ._params import resolve_deterministic, rfft_shape, rotation_arg, slice_params
 
 
 def _check_image(image_rfft: torch.Tensor, volume_shape):
@@ -71,6 +78,64 @@ def insert_finalize(acc: torch.Tensor, complex128: bool):
     return volume, weights
 
 
+def fixed_absmax(*images: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """Float32 bit pattern of max |re|, |im| over ``images`` as a (1,) int32
+    device tensor (maxed into ``out`` when given): the scale input of the
+    fixed-point accumulation.  All-reduce it with MAX to share one scale
+    across processes."""
+    dev = images[0].device
+    if out is None:
+        out = torch.zeros(1, dtype=torch.int32, device=dev)
+    L = _lib.load()
+    for t in images:
+        t = _lib.dense(t)
+        real = torch.view_as_real(t) if t.is_complex() else t
+        _lib.check(L.tt_fixed_absmax(_lib.ptr(real), int(real.dtype == torch.float64), real.numel(),
+                                     _lib.ptr(out), _lib.stream_of(dev)), "fixed_absmax")
+    return out
+
+
+def new_fixed_accumulator(volume_shape, device, channels: int = 1) -> torch.Tensor:
+    """Zeroed fixed-point accumulator: (channels, d, h, w//2+1, 4) int64
+    (re, im, w, pad)."""
+    d, h, w = rfft_shape(volume_shape)
+    return torch.zeros((channels, d, h, w, 4), dtype=torch.int64, device=device)
+
+
+def insert_fixed_accumulate(image_rfft, R, volume_shape, acc, absmax, max_slices, fftfreq_max=None,
+                            zyx_matrices=False, images_unshifted=False):
+    """Deterministic splat of (n, h, w//2+1) slices into a fixed-point
+    accumulator at the scale of ``absmax`` and ``max_slices``."""
+    dev = acc.device
+    if not (image_rfft.is_contiguous() and R.is_contiguous() and acc.is_contiguous()):
+        raise ValueError("insertion needs C-contiguous slices, rotations and accumulator")
+    params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=None, rotation=R,
+                          fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                          slices_unshifted=images_unshifted, vol_dims=rfft_shape(volume_shape))
+    L = _lib.load()
+    _lib.check(
+        L.tt_insert_fixed_accumulate(_lib.ptr(image_rfft), int(image_rfft.dtype == torch.complex128),
+                                     _lib.ptr(R), _lib.ptr(acc), _lib.ptr(absmax), int(max_slices), params,
+                                     _lib.stream_of(dev)),
+        "insert_central_slices_rfft_3d (deterministic)",
+    )
+
+
+def insert_fixed_finalize(acc: torch.Tensor, complex128: bool, absmax, max_slices):
+    """Fixed-point accumulator (c, d, h, w, 4) -> volume (c, d, h, w), weights (d, h, w)."""
+    c, d, h, w = acc.shape[:4]
+    cdt = torch.complex128 if complex128 else torch.complex64
+    wdt = torch.float64 if complex128 else torch.float32
+    volume = torch.empty((c, d, h, w), dtype=cdt, device=acc.device)
+    weights = torch.empty((d, h, w), dtype=wdt, device=acc.device)
+    L = _lib.load()
+    _lib.check(L.tt_insert_fixed_finalize(_lib.ptr(acc), int(complex128), c, d, h, w, _lib.ptr(absmax),
+                                          int(max(max_slices, 1)), _lib.ptr(volume), _lib.ptr(weights),
+                                          _lib.stream_of(acc.device)),
+               "insert_central_slices_rfft_3d finalize (deterministic)")
+    return volume, weights
+
+
 def friedel_mirror_x0(volume, weights):
     """In-place Friedel completion of the x=0 plane of (c?, d, h, w) volumes."""
     dev = volume.device
@@ -91,6 +156,7 @@ def insert_central_slices_rfft_3d(
     rotation_matrices: torch.Tensor,
     fftfreq_max: float | None = None,
     zyx_matrices: bool = False,
+    deterministic: bool | None = None,
 ) -> tuple[torch.Tensor, torch.Tensor]:
     _lib.require_cuda(image_rfft)
     _check_image(image_rfft, volume_shape)
@@ -100,8 +166,14 @@ def insert_central_slices_rfft_3d(
     lead = image_rfft.shape[:-2]
     if math.prod(lead) != n:
         raise ValueError(f"{n} rotation matrices for image stack of shape {tuple(lead)}")
-    img = image_rfft.reshape(n, *image_rfft.shape[-2:]).contiguous()
+    img = _lib.dense(image_rfft.reshape(n, *image_rfft.shape[-2:]))
     c128 = image_rfft.dtype == torch.complex128
+    if resolve_deterministic(deterministic):
+        absmax = fixed_absmax(img)
+        acc = new_fixed_accumulator(volume_shape, dev)
+        insert_fixed_accumulate(img, R, volume_shape, acc, absmax, max(n, 1), fftfreq_max, zyx_matrices)
+        volume, weights = insert_fixed_finalize(acc, c128, absmax, n)
+        return volume[0], weights
     acc = new_accumulator(volume_shape, c128, dev)
     insert_accumulate(img, R, volume_shape, acc, fftfreq_max, zyx_matrices)
     volume, weights = insert_finalize(acc, c128)
@@ -114,6 +186,7 @@ def insert_central_slices_rfft_3d_multichannel(
     rotation_matrices: torch.Tensor,  # (..., 3, 3)
     fftfreq_max: float | None = None,
     zyx_matrices: bool = False,
+    deterministic: bool | None = None,
 ) -> tuple[torch.Tensor, torch.Tensor]:
     """Multichannel insertion (_insert_central_slices_rfft_3d.py:109-210):
     returns ``(c, d, h, w//2+1)`` volumes and ONE ``(d, h, w//2+1)`` weight
@@ -125,8 +198,14 @@ def insert_central_slices_rfft_3d_multichannel(
     R, stack = rotation_arg(rotation_matrices, dev)
     n = R.shape[0]
     c128 = image_rfft.dtype == torch.complex128
+    chans = [_lib.dense(image_rfft[..., ch, :, :].reshape(n, *image_rfft.shape[-2:])) for ch in range(c)]
+    if resolve_deterministic(deterministic):
+        absmax = fixed_absmax(*chans)
+        acc = new_fixed_accumulator(volume_shape, dev, channels=c)
+        for ch, img in enumerate(chans):
+            insert_fixed_accumulate(img, R, volume_shape, acc[ch], absmax, max(n, 1), fftfreq_max, zyx_matrices)
+        return insert_fixed_finalize(acc, c128, absmax, n)
     acc = new_accumulator(volume_shape, c128, dev, channels=c)
-    for ch in range(c):
-        img = image_rfft[..., ch, :, :].reshape(n, *image_rfft.shape[-2:]).contiguous()
+    for ch, img in enumerate(chans):
         insert_accumulate(img, R, volume_shape, acc[ch], fftfreq_max, zyx_matrices)
     return insert_finalize(acc, c128)

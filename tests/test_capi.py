@@ -56,7 +56,7 @@ def test_param_struct_layout():
 
     # 7 int64 + 11 four-byte fields, padded to the 8-byte alignment of the struct
     assert ctypes.sizeof(_lib.SliceParams) == 104
-    assert _lib.SliceParams.fftfreq_max.offset == 60 and _lib.SliceParams.reserved.offset == 96
+    assert _lib.SliceParams.fftfreq_max.offset == 60 and _lib.SliceParams.deterministic.offset == 96
 
 
 def test_validation_rejects_before_launch():
@@ -108,6 +108,69 @@ def test_batched_validation_and_layout():
     bad = (_lib.BatchVolume * 1)(_lib.BatchVolume(_params(vol_w=8), None, fake, fake, fake, None))
     assert L.tt_insert_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
     assert L.tt_extract_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+
+
+def test_deterministic_mode_workspace_and_validation():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    fake = ctypes.c_void_p(16)
+    vox = 16 * 16 * 9
+    p = _params()
+    assert L.tt_insert_workspace_bytes(0, ctypes.byref(p)) == vox * 16
+    assert L.tt_insert_workspace_bytes(1, ctypes.byref(p)) == vox * 32
+    base = L.tt_extract_backward_workspace_bytes(ctypes.byref(p))
+    p = _params(deterministic=1)
+    assert L.tt_insert_workspace_bytes(0, ctypes.byref(p)) == 256 + vox * 32
+    assert L.tt_extract_backward_workspace_bytes(ctypes.byref(p)) == base + 256 + vox * 16
+    assert L.tt_insert_fixed_accumulator_bytes(2, 16, 16, 9) == 2 * vox * 32
+    # a deterministic one-shot insertion checks its larger workspace
+    assert L.tt_insert_central_slices_rfft_3d(fake, 0, fake, fake, fake, fake, vox * 16, ctypes.byref(p),
+                                              None) == _lib.TT_ERR_WORKSPACE
+    # the float two-stage API refuses the flag; the fixed one checks max_slices and pointers
+    assert L.tt_insert_accumulate(fake, 0, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert L.tt_insert_fixed_accumulate(fake, 0, fake, fake, fake, 3, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert b"max_slices" in L.tt_last_error()
+    assert L.tt_insert_fixed_accumulate(fake, 0, fake, fake, None, 4, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert L.tt_insert_fixed_finalize(fake, 0, 1, 16, 16, 9, fake, 0, fake, fake, None) == _lib.TT_ERR_INVALID
+    assert L.tt_fixed_absmax(fake, 0, -1, fake, None) == _lib.TT_ERR_INVALID
+    assert L.tt_fixed_absmax(None, 0, 0, None, None) == _lib.TT_OK  # empty: nothing to do
+    # the no-allocation backward cannot hold a fixed-point volume gradient
+    assert L.tt_extract_central_slices_rfft_3d_backward_noalloc(fake, fake, fake, fake, None, ctypes.byref(p),
+                                                                None) == _lib.TT_ERR_INVALID
+    arr = (_lib.BatchVolume * 1)(_lib.BatchVolume(p, fake, fake, fake, fake, None))
+    assert L.tt_extract_central_slices_rfft_3d_batched(arr, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+    p = _params(deterministic=2)
+    assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+
+
+def test_deterministic_flag_follows_torch():
+    from teamtomo_b200.torch_fourier_slice._params import resolve_deterministic
+
+    assert resolve_deterministic(True) and not resolve_deterministic(False)
+    before = torch.are_deterministic_algorithms_enabled()
+    try:
+        torch.use_deterministic_algorithms(True)
+        assert resolve_deterministic(None)
+        torch.use_deterministic_algorithms(False)
+        assert not resolve_deterministic(None)
+    finally:
+        torch.use_deterministic_algorithms(before)
+
+
+def test_lazy_conjugate_views_are_materialised():
+    """x.conj() is a lazy view whose memory holds x: the pointer layer refuses
+    it and dense() resolves it (autograd passes such views as gradients)."""
+    from teamtomo_b200 import _lib
+
+    x = torch.tensor([1 + 2j, 3 - 4j], dtype=torch.complex64)
+    with pytest.raises(ValueError, match="lazy conjugate"):
+        _lib.ptr(x.conj())
+    with pytest.raises(ValueError, match="lazy conjugate"):
+        _lib.ptr(torch.view_as_real(x)._neg_view())
+    y = _lib.dense(x.conj())
+    assert not y.is_conj() and torch.equal(y, torch.conj_physical(x))
+    assert _lib.dense(x) is x  # nothing to do: no copy
 
 
 def test_ctf_params_rows():
