@@ -79,6 +79,11 @@ def all_reduce_volume_gradient(grad: torch.Tensor, group=None) -> torch.Tensor:
     return _all_reduce_sum(grad, group)
 
 
+def all_reduce_sum(t: torch.Tensor, group=None) -> torch.Tensor:
+    """In-place SUM over the ranks of a (complex or real) partial volume."""
+    return _all_reduce_sum(t, group)
+
+
 def insert_central_slices_rfft_3d(
     image_rfft: torch.Tensor,
     volume_shape: tuple[int, int, int],

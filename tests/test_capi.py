@@ -253,3 +253,16 @@ def test_reference_exceptions_on_host():
         tt.insert_into_image_3d(torch.zeros(4, dtype=torch.float64), torch.zeros((4, 3)), torch.zeros((4, 4, 4)))
     with pytest.raises(ValueError, match="shape \\(d, h, w\\)"):
         tt.sample_image_3d(torch.zeros((4, 4)), torch.zeros((2, 3)))
+
+
+def test_streaming_host_checks():
+    from teamtomo_b200 import streaming
+
+    assert streaming.chunk_bounds(10, 4) == [(0, 4), (4, 8), (8, 10)]
+    assert streaming.chunk_bounds(0, 4) == []
+    with pytest.raises(ValueError):
+        streaming.chunk_bounds(10, 0)
+    with pytest.raises(ValueError, match="leading size"):
+        next(streaming.prefetch_to_device([torch.zeros(3), torch.zeros(4)], 2, "cpu"))
+    with pytest.raises(ValueError, match="data_bound"):
+        streaming.InsertionAccumulator((8, 8, 8), "cpu", deterministic=True)
