@@ -165,6 +165,19 @@ int tt_insert_central_slices_rfft_3d(const void *image_rfft, int32_t complex128,
                                      void *weights, void *workspace, size_t workspace_bytes,
                                      const tt_slice_params *p, void *stream);
 
+/* Backward of the insertion w.r.t. the slices: grad_image (n, img_h, img_w/2+1)
+ * is OVERWRITTEN with dL/dslices for upstream grad_volume (vol dims), both
+ * complex64 (complex128 = 0) or complex128, in PyTorch's complex-gradient
+ * convention.  The adjoint of the splat (the same float32 corner weights,
+ * gathered; conjugated where the point was redirected; zero for dropped
+ * pixels) and of the Friedel completion of the x=0 plane.  The weights output
+ * does not depend on the slices, so its gradient contributes nothing.
+ * Replaces the autograd graph of insert_central_slices_rfft_3d w.r.t. image_rfft
+ * (index_put_ backward of _insert_central_slices_rfft_3d.py:213-406). */
+int tt_insert_central_slices_rfft_3d_backward(const void *grad_volume, int32_t complex128,
+                                              const void *rotation_matrices, void *grad_image,
+                                              const tt_slice_params *p, void *stream);
+
 /* Bytes of an insertion accumulator for `channels` volumes of (d, h, w_rfft):
  * one (re, im, w, pad) slot per voxel, 16 bytes (complex64) or 32 (complex128). */
 size_t tt_insert_accumulator_bytes(int32_t complex128, int64_t channels, int64_t d, int64_t h,

@@ -277,6 +277,49 @@ def mirror_x0_post_pass(vol, wts):
     return vol, wts
 
 
+def insert_grad_images(grad_volume, volume_shape, rotation_matrices, fftfreq_max=None,
+                       zyx_matrices=False, dtype=np.complex64):
+    """Gradient of insert_central_slices_rfft_3d's volume w.r.t. its images
+    (PyTorch's complex convention) for upstream gradient ``grad_volume``: the
+    adjoint of the Friedel completion (G[v] + conj(G[m v]) on the x=0 plane
+    unless v itself is DC: out[u] takes conj(acc[m u]) unless m u is DC, and m
+    is its own inverse — for odd boxes m(DC) is not DC), then the insertion's own trilinear weights gathered back to
+    each kept source pixel, conjugated where the point was redirected.  The
+    weights output does not depend on the images.  (numpy, float64 sums)"""
+    gv = np.asarray(grad_volume).astype(np.complex128)
+    vd, vh, vw = (int(s) for s in volume_shape)
+    wr = vw // 2 + 1
+    z = np.arange(vd)[:, None]
+    y = np.arange(vh)[None, :]
+    zm, ym = (vd - z) % vd, (vh - y) % vh
+    keep = ~((z == vd // 2) & (y == vh // 2))
+    ga = gv.copy()
+    ga[:, :, 0] = gv[:, :, 0] + np.where(keep, np.conj(gv[zm, ym, 0]), 0)
+    r = _rot_f32(rotation_matrices)
+    n = r.shape[0]
+    flags, coords = slice_geometry(r, volume_shape, (vd, vh, wr), 1, fftfreq_max=fftfreq_max,
+                                   zyx_matrices=zyx_matrices)
+    sel = (flags & 5) == 5
+    c = coords[sel]
+    lo = np.floor(c)
+    hi = np.ceil(c)
+    t = (c - lo).astype(np.float32)
+    one = np.float32(1)
+    acc = np.zeros(len(c), np.complex128)
+    flat = ga.reshape(-1)
+    for k in range(8):
+        b = ((k >> 2) & 1, (k >> 1) & 1, k & 1)
+        f = [t[:, a] if b[a] else one - t[:, a] for a in range(3)]
+        w = (f[0] * f[1]) * f[2]
+        idx = [(hi if b[a] else lo)[:, a].astype(np.int64) for a in range(3)]
+        vi = (idx[0] * vh + idx[1]) * wr + idx[2]
+        acc += np.where(w != 0, w.astype(np.float64) * flat[vi], 0)
+    acc = np.where((flags[sel] & 2) != 0, np.conj(acc), acc)
+    out = np.zeros((n, vh, wr), dtype)
+    out[sel] = acc.astype(dtype)
+    return out
+
+
 # ----------------------------------------------------------------------------
 # deterministic insertion: 64-bit fixed point (numpy, bit-exact restatement of
 # the CUDA fixed-point mode; the reference has no such mode, so it is pinned

@@ -72,6 +72,7 @@ SIGNATURES = {
     "tt_insert_central_slices_rfft_3d": (
         [_vp, _i32, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_accumulator_bytes": ([_i32, _i64, _i64, _i64, _i64], _sz),
+    "tt_insert_central_slices_rfft_3d_backward": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_accumulate": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_finalize": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp, _vp], _i32),
     "tt_friedel_mirror_x0": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp], _i32),

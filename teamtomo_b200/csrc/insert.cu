@@ -124,6 +124,60 @@ __global__ void mirror_x0_kernel(typename Acc<R>::C* __restrict__ vol, R* __rest
     }
 }
 
+// Backward of the insertion w.r.t. the slices, the adjoint of the splat and of
+// the Friedel completion.  The completion adds conj(acc[m u]) to out[u] unless
+// m u is DC; m is its own inverse, so acc[v] reaches out[m v] unless v is DC
+// (for odd boxes m(DC) is not DC):
+//   dL/dacc[v] = G[v] + conj(G[m v])  on the x = 0 plane, v not DC
+// and each kept source pixel gathers sum_k w_k dL/dacc[corner k] with the
+// splat's own float32 weights, conjugated where the point was redirected.
+// One thread per slice pixel; every pixel is written (zero when dropped).
+template <typename R>
+__device__ __forceinline__ typename Acc<R>::C completed_grad(const typename Acc<R>::C* __restrict__ gvol,
+                                                            const SliceGeom& g, int z, int y, int x) {
+    typename Acc<R>::C a = gvol[vox_index(g, z, y, x)];
+    if (x == 0 && !(z == g.D / 2 && y == g.H / 2)) {
+        const typename Acc<R>::C b = gvol[vox_index(g, (g.D - z) % g.D, (g.H - y) % g.H, 0)];
+        a.x += b.x;
+        a.y -= b.y;
+    }
+    return a;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kTileThreads)
+insert_bwd_kernel(const typename Acc<R>::C* __restrict__ gvol, const void* __restrict__ rot,
+                  typename Acc<R>::C* __restrict__ gimg, SliceGeom g, int tiles) {
+    __shared__ float m[9];
+    const int64_t s = blockIdx.x / tiles;
+    const int tile = blockIdx.x - (int)(s * tiles);
+    if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
+    __syncthreads();
+    int iy, ix;
+    if (!tile_pixel(g, tile, iy, ix)) return;
+    typename Acc<R>::C out;
+    out.x = 0;
+    out.y = 0;
+    const float qy = shifted_freq(iy, g.img_h, g.inv_h);
+    const float qx = __fmul_rn((float)ix, g.inv_w);
+    bool cj;
+    InsertCell k;
+    if (insert_pixel_kept(g, qy, qx) && insert_cell(g, m, qy, qx, cj, k)) {
+#pragma unroll
+        for (int corner = 0; corner < 8; corner++) {
+            const float w = insert_corner_weight(k, corner);
+            if (w == 0.0f) continue;
+            int z, y, x;
+            insert_corner_zyx(k, corner, z, y, x);
+            const typename Acc<R>::C gv = completed_grad<R>(gvol, g, z, y, x);
+            out.x += (R)w * gv.x;
+            out.y += (R)w * gv.y;
+        }
+        if (cj) out.y = -out.y;
+    }
+    __stcs(gimg + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, out);
+}
+
 int insert_deterministic(const void* image_rfft, int32_t complex128, const void* rot, void* volume, void* weights,
                          void* workspace, const tt_slice_params* p, cudaStream_t st);
 
@@ -217,6 +271,29 @@ extern "C" int tt_insert_central_slices_rfft_3d(const void* image_rfft, int32_t 
     if (p->n > 0)
         if (int r = launch_insert_accumulate(image_rfft, complex128, rotation_matrices, workspace, p, st)) return r;
     return launch_insert_finalize(workspace, complex128, 1, p->vol_d, p->vol_h, p->vol_w, volume_rfft, weights, st);
+}
+
+extern "C" int tt_insert_central_slices_rfft_3d_backward(const void* grad_volume, int32_t complex128,
+                                                         const void* rotation_matrices, void* grad_image,
+                                                         const tt_slice_params* p, void* stream) {
+    if (int e = check_insert_params(p)) return e;
+    if (p->n == 0) return TT_OK;
+    if (!grad_volume || !rotation_matrices || !grad_image)
+        return fail(TT_ERR_INVALID, "insert backward: NULL pointer argument");
+    SliceGeom g = make_geom(*p);
+    const int tiles = tiles_per_slice(g.img_h, g.wr);
+    const int64_t items = (int64_t)g.n * tiles;
+    if (items > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert backward: too many blocks");
+    cudaStream_t st = as_stream(stream);
+    if (complex128)
+        insert_bwd_kernel<double><<<(unsigned)items, kTileThreads, 0, st>>>((const double2*)grad_volume,
+                                                                           rotation_matrices, (double2*)grad_image,
+                                                                           g, tiles);
+    else
+        insert_bwd_kernel<float><<<(unsigned)items, kTileThreads, 0, st>>>((const float2*)grad_volume,
+                                                                          rotation_matrices, (float2*)grad_image, g,
+                                                                          tiles);
+    return check_launch("insert_bwd_kernel");
 }
 
 extern "C" int tt_friedel_mirror_x0(void* volume_rfft, void* weights, int32_t complex128, int64_t channels,

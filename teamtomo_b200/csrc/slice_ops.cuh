@@ -181,6 +181,61 @@ struct FloatSplat {
     }
 };
 
+// Source pixels the insertion skips: outside fftfreq_max, and the
+// Friedel-redundant half of the x = 0 column (x == 0, y < 0).
+__device__ __forceinline__ bool insert_pixel_kept(const SliceGeom& g, float qy, float qx) {
+    return in_fmax(g, qy, qx) && !(qx == 0.0f && qy < 0.0f);
+}
+
+// Floor / ceil cell of an insertion point and its fractional offsets.
+struct InsertCell {
+    int iz0, iy0, ix0, iz1, iy1, ix1;
+    float tz, ty, tx;
+};
+
+// Insertion geometry of slice frequency (qy, qx): rotation, the strict x' < 0
+// redirect (cj), array coordinates and the whole-point bounds test.
+__device__ __forceinline__ bool insert_cell(const SliceGeom& g, const float* m, float qy, float qx, bool& cj,
+                                            InsertCell& k) {
+    float p[3], c[3];
+    rotate_slice_point(m, qy, qx, p);
+    cj = p[2] < 0.0f;
+    if (cj) {
+        p[0] = -p[0];
+        p[1] = -p[1];
+        p[2] = -p[2];
+    }
+    to_dft_coords(g, p, c);
+    if (!inside_volume(g, c)) return false;
+    const float z0 = floorf(c[0]), y0 = floorf(c[1]), x0 = floorf(c[2]);
+    k.tz = c[0] - z0;
+    k.ty = c[1] - y0;
+    k.tx = c[2] - x0;
+    k.iz0 = (int)z0;
+    k.iy0 = (int)y0;
+    k.ix0 = (int)x0;
+    k.iz1 = (int)ceilf(c[0]);
+    k.iy1 = (int)ceilf(c[1]);
+    k.ix1 = (int)ceilf(c[2]);
+    return true;
+}
+
+// Weight of corner `corner` (bit 2: z, bit 1: y, bit 0: x high) with the
+// reference's float32 products, left to right.
+__device__ __forceinline__ float insert_corner_weight(const InsertCell& k, int corner) {
+    const int bz = (corner >> 2) & 1, by = (corner >> 1) & 1, bx = corner & 1;
+    const float fz = bz ? k.tz : 1.0f - k.tz;
+    const float fy = by ? k.ty : 1.0f - k.ty;
+    const float fx = bx ? k.tx : 1.0f - k.tx;
+    return (fz * fy) * fx;
+}
+
+__device__ __forceinline__ void insert_corner_zyx(const InsertCell& k, int corner, int& z, int& y, int& x) {
+    z = (corner & 4) ? k.iz1 : k.iz0;
+    y = (corner & 2) ? k.iy1 : k.iy0;
+    x = (corner & 1) ? k.ix1 : k.ix0;
+}
+
 // Splat of one source pixel, following _insert_central_slices_rfft_3d.py:30-85
 // and _insert_into_3d_dft_linear :289-346: each of the eight corners receives
 // (data * w, w) through sink(voxel, re, im, w, weight scale).  With a CTF
@@ -192,11 +247,12 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
                                                 const CtfConst* ctf = nullptr) {
     const float qy = shifted_freq(iy, g.img_h, g.inv_h);
     const float qx = __fmul_rn((float)ix, g.inv_w);
-    if (!in_fmax(g, qy, qx)) return;
-    if (qx == 0.0f && qy < 0.0f) return;  // Friedel-redundant source pixel
-    float p[3], c[3];
-    rotate_slice_point(m, qy, qx, p);
+    if (!insert_pixel_kept(g, qy, qx)) return;
+    // issued before the geometry so the load overlaps it
     const typename Acc<R>::C d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+    bool cj;
+    InsertCell k;
+    if (!insert_cell(g, m, qy, qx, cj, k)) return;
     R dre = d.x, dim = d.y, wscale = (R)1;
     if (ctf) {
         const float cv = ctf_value(*ctf, qy, qx);
@@ -204,28 +260,14 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
         dim *= (R)cv;
         wscale = (R)(cv * cv);
     }
-    if (p[2] < 0.0f) {
-        p[0] = -p[0];
-        p[1] = -p[1];
-        p[2] = -p[2];
-        dim = -dim;
-    }
-    to_dft_coords(g, p, c);
-    if (!inside_volume(g, c)) return;
-    const float z0 = floorf(c[0]), y0 = floorf(c[1]), x0 = floorf(c[2]);
-    const float tz = c[0] - z0, ty = c[1] - y0, tx = c[2] - x0;
-    const int iz0 = (int)z0, iy0 = (int)y0, ix0 = (int)x0;
-    const int iz1 = (int)ceilf(c[0]), iy1 = (int)ceilf(c[1]), ix1 = (int)ceilf(c[2]);
+    if (cj) dim = -dim;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        const int bz = (k >> 2) & 1, by = (k >> 1) & 1, bx = k & 1;
-        const float fz = bz ? tz : 1.0f - tz;
-        const float fy = by ? ty : 1.0f - ty;
-        const float fx = bx ? tx : 1.0f - tx;
-        const float w = (fz * fy) * fx;
+    for (int corner = 0; corner < 8; corner++) {
+        const float w = insert_corner_weight(k, corner);
         if (w == 0.0f) continue;  // adds nothing (ceil == floor or zero fraction)
-        const int64_t vi = vox_index(g, bz ? iz1 : iz0, by ? iy1 : iy0, bx ? ix1 : ix0);
-        sink(vi, dre, dim, (R)w, wscale);
+        int z, y, x;
+        insert_corner_zyx(k, corner, z, y, x);
+        sink(vox_index(g, z, y, x), dre, dim, (R)w, wscale);
     }
 }
 

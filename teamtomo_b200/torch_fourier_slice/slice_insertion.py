@@ -7,6 +7,8 @@ complex64 slices give a complex64 volume with float32 weights, complex128
 slices a complex128 volume with float64 weights.  The splat runs on the
 sm_100a scatter kernel into an (re, im, w) accumulator; one finalize pass
 applies the Friedel completion of the x=0 plane and writes the two outputs.
+The insertion is differentiable w.r.t. the slices: the backward is the gather
+adjoint of the splat and of the Friedel completion (one kernel, no atomics).
 
 Deterministic mode (``deterministic=True``, or ``None`` with
 ``torch.use_deterministic_algorithms(True)``; not in the reference): the splat
@@ -150,6 +152,67 @@ def friedel_mirror_x0(volume, weights):
     )
 
 
+def _splat(chans, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, c128, dev):
+    """Insertion of per-channel (n, h, w//2+1) stacks -> ((c, d, h, w) volumes, weights)."""
+    n = R.shape[0]
+    if deterministic:
+        absmax = fixed_absmax(*chans)
+        acc = new_fixed_accumulator(volume_shape, dev, channels=len(chans))
+        for ch, img in enumerate(chans):
+            insert_fixed_accumulate(img, R, volume_shape, acc[ch], absmax, max(n, 1), fftfreq_max, zyx_matrices)
+        return insert_fixed_finalize(acc, c128, absmax, n)
+    acc = new_accumulator(volume_shape, c128, dev, channels=len(chans))
+    for ch, img in enumerate(chans):
+        insert_accumulate(img, R, volume_shape, acc[ch], fftfreq_max, zyx_matrices)
+    return insert_finalize(acc, c128)
+
+
+def insert_backward(grad_volume, R, volume_shape, fftfreq_max=None, zyx_matrices=False,
+                    images_unshifted=False) -> torch.Tensor:
+    """dL/dslices (n, h, w//2+1) of one insertion for upstream dL/dvolume
+    (d, h, w//2+1): the gather adjoint of the splat and of the Friedel
+    completion (the weights output does not depend on the slices)."""
+    dev = grad_volume.device
+    grad_volume = _lib.dense(grad_volume)
+    c128 = grad_volume.dtype == torch.complex128
+    d, h, w = rfft_shape(volume_shape)
+    out = torch.empty((R.shape[0], h, w), dtype=grad_volume.dtype, device=dev)
+    params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=None, rotation=R,
+                          fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                          slices_unshifted=images_unshifted, vol_dims=(d, h, w))
+    L = _lib.load()
+    _lib.check(L.tt_insert_central_slices_rfft_3d_backward(_lib.ptr(grad_volume), int(c128), _lib.ptr(R),
+                                                           _lib.ptr(out), params, _lib.stream_of(dev)),
+               "insert_central_slices_rfft_3d backward")
+    return out
+
+
+class _InsertCentralSlices(torch.autograd.Function):
+    """(n, c, h, w//2+1) slices -> ((c, d, h, w//2+1) volumes, weights),
+    differentiable w.r.t. the slices (not the rotations, which are constants
+    here; the weights carry no gradient)."""
+
+    @staticmethod
+    def forward(ctx, images, R, volume_shape, fftfreq_max, zyx_matrices, deterministic):
+        chans = [_lib.dense(images[:, ch]) for ch in range(images.shape[1])]
+        c128 = images.dtype == torch.complex128
+        volumes, weights = _splat(chans, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, c128,
+                                  images.device)
+        ctx.mark_non_differentiable(weights)
+        ctx.save_for_backward(R)
+        ctx.args = (volume_shape, fftfreq_max, zyx_matrices)
+        return volumes, weights
+
+    @staticmethod
+    def backward(ctx, grad_volumes, grad_weights):
+        if grad_volumes is None or not ctx.needs_input_grad[0]:
+            return None, None, None, None, None, None
+        (R,) = ctx.saved_tensors
+        grads = torch.stack([insert_backward(grad_volumes[ch], R, *ctx.args)
+                             for ch in range(grad_volumes.shape[0])], dim=1)
+        return grads, None, None, None, None, None
+
+
 def insert_central_slices_rfft_3d(
     image_rfft: torch.Tensor,  # fftshifted rfft of (..., h, w) 2d image
     volume_shape: tuple[int, int, int],
@@ -158,6 +221,10 @@ def insert_central_slices_rfft_3d(
     zyx_matrices: bool = False,
     deterministic: bool | None = None,
 ) -> tuple[torch.Tensor, torch.Tensor]:
+    """Insert central slices into an fftshifted rfft volume; returns
+    ``(volume, weights)``.  Differentiable w.r.t. ``image_rfft`` (the gather
+    adjoint, not in the reference's API but what its autograd computes);
+    ``deterministic`` (not in the reference) selects the fixed-point splat."""
     _lib.require_cuda(image_rfft)
     _check_image(image_rfft, volume_shape)
     dev = image_rfft.device
@@ -166,18 +233,10 @@ def insert_central_slices_rfft_3d(
     lead = image_rfft.shape[:-2]
     if math.prod(lead) != n:
         raise ValueError(f"{n} rotation matrices for image stack of shape {tuple(lead)}")
-    img = _lib.dense(image_rfft.reshape(n, *image_rfft.shape[-2:]))
-    c128 = image_rfft.dtype == torch.complex128
-    if resolve_deterministic(deterministic):
-        absmax = fixed_absmax(img)
-        acc = new_fixed_accumulator(volume_shape, dev)
-        insert_fixed_accumulate(img, R, volume_shape, acc, absmax, max(n, 1), fftfreq_max, zyx_matrices)
-        volume, weights = insert_fixed_finalize(acc, c128, absmax, n)
-        return volume[0], weights
-    acc = new_accumulator(volume_shape, c128, dev)
-    insert_accumulate(img, R, volume_shape, acc, fftfreq_max, zyx_matrices)
-    volume, weights = insert_finalize(acc, c128)
-    return volume[0], weights
+    img = image_rfft.reshape(n, 1, *image_rfft.shape[-2:])
+    volumes, weights = _InsertCentralSlices.apply(img, R, tuple(int(x) for x in volume_shape), fftfreq_max,
+                                                  zyx_matrices, resolve_deterministic(deterministic))
+    return volumes[0], weights
 
 
 def insert_central_slices_rfft_3d_multichannel(
@@ -197,15 +256,6 @@ def insert_central_slices_rfft_3d_multichannel(
     c = image_rfft.shape[-3]
     R, stack = rotation_arg(rotation_matrices, dev)
     n = R.shape[0]
-    c128 = image_rfft.dtype == torch.complex128
-    chans = [_lib.dense(image_rfft[..., ch, :, :].reshape(n, *image_rfft.shape[-2:])) for ch in range(c)]
-    if resolve_deterministic(deterministic):
-        absmax = fixed_absmax(*chans)
-        acc = new_fixed_accumulator(volume_shape, dev, channels=c)
-        for ch, img in enumerate(chans):
-            insert_fixed_accumulate(img, R, volume_shape, acc[ch], absmax, max(n, 1), fftfreq_max, zyx_matrices)
-        return insert_fixed_finalize(acc, c128, absmax, n)
-    acc = new_accumulator(volume_shape, c128, dev, channels=c)
-    for ch, img in enumerate(chans):
-        insert_accumulate(img, R, volume_shape, acc[ch], fftfreq_max, zyx_matrices)
-    return insert_finalize(acc, c128)
+    img = image_rfft.reshape(n, c, *image_rfft.shape[-2:])
+    return _InsertCentralSlices.apply(img, R, tuple(int(x) for x in volume_shape), fftfreq_max, zyx_matrices,
+                                      resolve_deterministic(deterministic))

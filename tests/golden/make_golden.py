@@ -20,6 +20,8 @@ Cases (reference test each one mirrors):
   insimg_*       insert_into_image_3d (trilinear / nearest, f32 / c64, f64 weights)
   project_*      project_3d_to_2d of the conftest cube (torch-fourier-slice/tests/conftest.py:5-10)
   backproject_*  backproject_2d_to_3d of those projections (float32 and float64)
+  ctf_*          torch-ctf calculate_ctf_2d grids
+  insgrad_*      reference autograd of insert_central_slices_rfft_3d w.r.t. the images
 """
 
 from __future__ import annotations
@@ -237,6 +239,27 @@ def main():
         g[f"ctf_{i}_flags"] = np.array([int(rf), int(fs)])
         g[f"ctf_{i}_out"] = ctf.numpy()
     g["ctf_cases"] = np.array(len(ctf_cases))
+
+    # ---------------- insertion backward w.r.t. the images (reference autograd) ----------------
+    gen = torch.Generator().manual_seed(21)
+    names = []
+    for n, dt, kw in ((16, torch.complex64, {}), (17, torch.complex64, {}), (16, torch.complex128, {}),
+                      (16, torch.complex64, dict(fftfreq_max=0.3, zyx_matrices=True))):
+        rots = np.concatenate([special_ortho_group.rvs(3, size=10, random_state=n + 31),
+                               special_rotations()])
+        imgs = torch.randn(len(rots), n, n // 2 + 1, dtype=dt, generator=gen).requires_grad_(True)
+        gvol = torch.randn(n, n, n // 2 + 1, dtype=dt, generator=gen)
+        vol, _ = insert_central_slices_rfft_3d(imgs, (n, n, n), torch.tensor(rots), **kw)
+        (vol * gvol.conj()).real.sum().backward()
+        name = f"n{n}_{str(dt).split('.')[-1]}" + "".join(f"_{k}" for k in kw)
+        g[f"insgrad_{name}_images"] = imgs.detach().numpy()
+        g[f"insgrad_{name}_rot"] = rots
+        g[f"insgrad_{name}_gvol"] = gvol.numpy()
+        g[f"insgrad_{name}_fmax"] = np.array(kw.get("fftfreq_max", -1.0))
+        g[f"insgrad_{name}_zyx"] = np.array(int(kw.get("zyx_matrices", False)))
+        g[f"insgrad_{name}_out"] = imgs.grad.numpy()
+        names.append(name)
+    g["insgrad_cases"] = np.array(names)
 
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {os.path.getsize(OUT) / 1e6:.2f} MB, {len(g)} arrays")

@@ -159,3 +159,20 @@ def test_insert_mirror_is_plane_post_pass(golden, oracle):
         tol = 1e-12 if vol.dtype == np.complex128 else 1e-6
         assert rel_l2(vol, golden[f"insert_{name}_volume"]) < tol, name
         assert rel_l2(w, golden[f"insert_{name}_weights"]) < tol, name
+
+
+def test_insert_image_gradient_matches_reference_autograd(golden, oracle):
+    """The gather adjoint of the insertion (with the Friedel completion's
+    adjoint) against the reference's autograd w.r.t. the images."""
+    for name in golden["insgrad_cases"]:
+        name = str(name)
+        imgs = golden[f"insgrad_{name}_images"]
+        n = imgs.shape[-2]
+        fmax = float(golden[f"insgrad_{name}_fmax"])
+        out = oracle.insert_grad_images(golden[f"insgrad_{name}_gvol"], (n, n, n), golden[f"insgrad_{name}_rot"],
+                                        fftfreq_max=None if fmax < 0 else fmax,
+                                        zyx_matrices=bool(int(golden[f"insgrad_{name}_zyx"])), dtype=imgs.dtype)
+        ref = golden[f"insgrad_{name}_out"]
+        tol = 1e-12 if imgs.dtype == np.complex128 else 1e-6
+        assert rel_l2(out, ref) < tol, name
+        assert np.array_equal(out == 0, ref == 0), name  # same pixels receive no gradient
