@@ -1,9 +1,10 @@
 """Host side of the elementwise passes around the FFTs of project / backproject.
 
 Each forward runs one fused CUDA kernel (see ``csrc/wrappers.cu``).  The
-projection passes are differentiable; their backward passes are the exact
-adjoints (a permutation, a crop or zero-pad and a fixed sinc^2 weight),
-written with torch ops because they are off the hot path.
+passes of both projection and backprojection are differentiable; their
+backward passes are the exact adjoints (a permutation, a crop or zero-pad and
+a fixed sinc^2 weight), written with torch ops because they are off the hot
+path.
 """
 
 from __future__ import annotations
@@ -25,6 +26,18 @@ def sinc2_grid(n: int, device, dtype=torch.float32) -> torch.Tensor:
         1.0 / n, dtype=torch.float32)
     f = torch.fft.fftshift(f)
     r = torch.sqrt(f[:, None, None] ** 2 + f[None, :, None] ** 2 + f[None, None, :] ** 2)
+    return (torch.sinc(r) ** 2).to(dtype)
+
+
+def sinc2_grid_3(n0: int, n1: int, n2: int, device, dtype=torch.float32) -> torch.Tensor:
+    """sinc(|f|)^2 on the fftshifted frequency grid of an (n0, n1, n2) array."""
+    def axis(n):
+        k = torch.arange(n, device=device)
+        f = torch.where(k < (n + 1) // 2, k, k - n).to(torch.float32) * torch.tensor(1.0 / n, dtype=torch.float32)
+        return torch.fft.fftshift(f)
+
+    f0, f1, f2 = axis(n0), axis(n1), axis(n2)
+    r = torch.sqrt(f0[:, None, None] ** 2 + f1[None, :, None] ** 2 + f2[None, None, :] ** 2)
     return (torch.sinc(r) ** 2).to(dtype)
 
 
@@ -83,15 +96,30 @@ def recentre_crop_2d(images: torch.Tensor, pad: int) -> torch.Tensor:
     return _RecentreCrop2d.apply(flat, int(pad))
 
 
+class _PadFftshift2d(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, images, pad):
+        m, d = images.shape[0], images.shape[-1]
+        n = d + 2 * pad
+        out = torch.empty((m, n, n), dtype=images.dtype, device=images.device)
+        L = _lib.load()
+        _lib.check(L.tt_pad_fftshift_2d(_lib.ptr(images), _is_f64(images), m, d, pad, _lib.ptr(out),
+                                        _lib.stream_of(images.device)), "pad_fftshift_2d")
+        ctx.pad = pad
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        # adjoint of fftshift(pad(x)): crop(ifftshift(g))
+        p = ctx.pad
+        n = g.shape[-1]
+        g = torch.fft.ifftshift(g, dim=(-2, -1))
+        return g[..., p:n - p, p:n - p], None
+
+
 def pad_fftshift_2d(images: torch.Tensor, pad: int) -> torch.Tensor:
     """(m, d, d) real -> fftshift(pad(images)) (m, n, n)."""
-    m, d = images.shape[0], images.shape[-1]
-    n = d + 2 * pad
-    out = torch.empty((m, n, n), dtype=images.dtype, device=images.device)
-    L = _lib.load()
-    _lib.check(L.tt_pad_fftshift_2d(_lib.ptr(images), _is_f64(images), m, d, pad, _lib.ptr(out),
-                                    _lib.stream_of(images.device)), "pad_fftshift_2d")
-    return out
+    return _PadFftshift2d.apply(_lib.dense(images), int(pad))
 
 
 def backproject_normalize(acc: torch.Tensor) -> torch.Tensor:
@@ -108,16 +136,33 @@ def backproject_normalize(acc: torch.Tensor) -> torch.Tensor:
     return out
 
 
+class _BackprojectFinish(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, volume, pad):
+        n0, n1, n2 = volume.shape[-3:]
+        lead = volume.shape[:-3]
+        channels = volume.numel() // (n0 * n1 * n2)
+        out = torch.empty((*lead, n0 - 2 * pad, n1 - 2 * pad, n2 - 2 * pad), dtype=volume.dtype,
+                          device=volume.device)
+        L = _lib.load()
+        _lib.check(L.tt_backproject_finish(_lib.ptr(volume), _is_f64(volume), channels, n0, n1, n2,
+                                           pad, _lib.ptr(out), _lib.stream_of(volume.device)),
+                   "backproject_finish")
+        ctx.pad = pad
+        ctx.dims = (n0, n1, n2)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        # adjoint of crop(ifftshift(v) / sinc^2): fftshift(pad(g) / sinc^2)
+        p = ctx.pad
+        n0, n1, n2 = ctx.dims
+        if p:
+            g = F.pad(g, [p] * 6)
+        g = g / sinc2_grid_3(n0, n1, n2, g.device, g.dtype)
+        return torch.fft.fftshift(g, dim=(-3, -2, -1)), None
+
+
 def backproject_finish(volume: torch.Tensor, pad: int) -> torch.Tensor:
     """(c?, n0, n1, n2) irfft output -> crop(ifftshift(v) / sinc^2)."""
-    n0, n1, n2 = volume.shape[-3:]
-    lead = volume.shape[:-3]
-    channels = volume.numel() // (n0 * n1 * n2)
-    volume = _lib.dense(volume)
-    out = torch.empty((*lead, n0 - 2 * pad, n1 - 2 * pad, n2 - 2 * pad), dtype=volume.dtype,
-                      device=volume.device)
-    L = _lib.load()
-    _lib.check(L.tt_backproject_finish(_lib.ptr(volume), _is_f64(volume), channels, n0, n1, n2,
-                                       pad, _lib.ptr(out), _lib.stream_of(volume.device)),
-               "backproject_finish")
-    return out
+    return _BackprojectFinish.apply(_lib.dense(volume), int(pad))

@@ -6,6 +6,12 @@ sinc^2, crop — with the fftshifts folded into kernel addressing: one kernel
 pads and shifts the images, the insertion reads the unshifted 2D rfft, one
 kernel applies the Friedel completion, the normalisation and the inverse
 shift, and one kernel recentres, divides by sinc^2 and crops.
+
+When the images require grad, the same steps run as differentiable pieces
+(each fused pass has its exact adjoint; the insertion's backward is the
+gather adjoint of the splat; the normalisation divides by the weights, which
+do not depend on the images), so a reconstruction can be differentiated
+w.r.t. its projections, as with the reference's torch code.
 """
 
 from __future__ import annotations
@@ -15,7 +21,7 @@ import torch
 from .. import _lib
 from . import _wrappers
 from ._params import rotation_arg
-from .slice_insertion import insert_accumulate, new_accumulator
+from .slice_insertion import _InsertCentralSlices, insert_accumulate, new_accumulator
 
 
 def _pad_amount(n: int, pad_factor: float) -> int:
@@ -44,6 +50,12 @@ def _backproject(images, rotation_matrices, pad_factor, fftfreq_max, zyx_matrice
     fft_in = _wrappers.pad_fftshift_2d(flat, p)
     spec = torch.fft.rfftn(fft_in, dim=(-2, -1)).reshape(*lead, c, n, n // 2 + 1)
     spec = spec.reshape(nrot, c, n, n // 2 + 1)
+    if torch.is_grad_enabled() and images.requires_grad:
+        vols, weights = _InsertCentralSlices.apply(spec, R, shape, fftfreq_max, zyx_matrices, False, True)
+        dft = torch.fft.ifftshift(vols / torch.clamp(weights, min=1.0), dim=(-3, -2))
+        real = torch.fft.irfftn(dft, dim=(-3, -2, -1))
+        out = _wrappers.backproject_finish(real, p)
+        return out if channels else out[0]
     acc = new_accumulator(shape, spec.dtype == torch.complex128, dev, channels=c)
     for ch in range(c):
         insert_accumulate(spec[:, ch].contiguous(), R, shape, acc[ch], fftfreq_max, zyx_matrices,

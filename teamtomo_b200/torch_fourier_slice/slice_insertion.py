@@ -152,18 +152,19 @@ def friedel_mirror_x0(volume, weights):
     )
 
 
-def _splat(chans, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, c128, dev):
+def _splat(chans, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, c128, dev, unshifted=False):
     """Insertion of per-channel (n, h, w//2+1) stacks -> ((c, d, h, w) volumes, weights)."""
     n = R.shape[0]
     if deterministic:
         absmax = fixed_absmax(*chans)
         acc = new_fixed_accumulator(volume_shape, dev, channels=len(chans))
         for ch, img in enumerate(chans):
-            insert_fixed_accumulate(img, R, volume_shape, acc[ch], absmax, max(n, 1), fftfreq_max, zyx_matrices)
+            insert_fixed_accumulate(img, R, volume_shape, acc[ch], absmax, max(n, 1), fftfreq_max, zyx_matrices,
+                                    images_unshifted=unshifted)
         return insert_fixed_finalize(acc, c128, absmax, n)
     acc = new_accumulator(volume_shape, c128, dev, channels=len(chans))
     for ch, img in enumerate(chans):
-        insert_accumulate(img, R, volume_shape, acc[ch], fftfreq_max, zyx_matrices)
+        insert_accumulate(img, R, volume_shape, acc[ch], fftfreq_max, zyx_matrices, images_unshifted=unshifted)
     return insert_finalize(acc, c128)
 
 
@@ -190,27 +191,28 @@ def insert_backward(grad_volume, R, volume_shape, fftfreq_max=None, zyx_matrices
 class _InsertCentralSlices(torch.autograd.Function):
     """(n, c, h, w//2+1) slices -> ((c, d, h, w//2+1) volumes, weights),
     differentiable w.r.t. the slices (not the rotations, which are constants
-    here; the weights carry no gradient)."""
+    here; the weights carry no gradient).  ``unshifted``: slice rows stored
+    ifftshifted (the plain rfft of a real image)."""
 
     @staticmethod
-    def forward(ctx, images, R, volume_shape, fftfreq_max, zyx_matrices, deterministic):
+    def forward(ctx, images, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, unshifted=False):
         chans = [_lib.dense(images[:, ch]) for ch in range(images.shape[1])]
         c128 = images.dtype == torch.complex128
         volumes, weights = _splat(chans, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, c128,
-                                  images.device)
+                                  images.device, unshifted)
         ctx.mark_non_differentiable(weights)
         ctx.save_for_backward(R)
-        ctx.args = (volume_shape, fftfreq_max, zyx_matrices)
+        ctx.args = (volume_shape, fftfreq_max, zyx_matrices, unshifted)
         return volumes, weights
 
     @staticmethod
     def backward(ctx, grad_volumes, grad_weights):
         if grad_volumes is None or not ctx.needs_input_grad[0]:
-            return None, None, None, None, None, None
+            return None, None, None, None, None, None, None
         (R,) = ctx.saved_tensors
         grads = torch.stack([insert_backward(grad_volumes[ch], R, *ctx.args)
                              for ch in range(grad_volumes.shape[0])], dim=1)
-        return grads, None, None, None, None, None
+        return grads, None, None, None, None, None, None
 
 
 def insert_central_slices_rfft_3d(

@@ -22,6 +22,7 @@ Cases (reference test each one mirrors):
   backproject_*  backproject_2d_to_3d of those projections (float32 and float64)
   ctf_*          torch-ctf calculate_ctf_2d grids
   insgrad_*      reference autograd of insert_central_slices_rfft_3d w.r.t. the images
+  bpgrad_*       reference autograd of backproject_2d_to_3d w.r.t. the images
 """
 
 from __future__ import annotations
@@ -260,6 +261,18 @@ def main():
         g[f"insgrad_{name}_out"] = imgs.grad.numpy()
         names.append(name)
     g["insgrad_cases"] = np.array(names)
+
+    # ---------------- backprojection backward w.r.t. the images (reference autograd) ----------------
+    gen = torch.Generator().manual_seed(23)
+    for name, d, pf in (("even", 16, 2.0), ("odd", 17, 1.5)):
+        rots = special_ortho_group.rvs(3, size=5, random_state=d)
+        imgs = torch.randn(5, d, d, generator=gen).requires_grad_(True)
+        rec = backproject_2d_to_3d(imgs, torch.tensor(rots), pad_factor=pf)
+        G = torch.randn(rec.shape, generator=gen)
+        (rec * G).sum().backward()
+        g[f"bpgrad_{name}_images"], g[f"bpgrad_{name}_rot"] = imgs.detach().numpy(), rots
+        g[f"bpgrad_{name}_G"], g[f"bpgrad_{name}_pad"] = G.numpy(), np.array(pf)
+        g[f"bpgrad_{name}_out"] = imgs.grad.numpy()
 
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {os.path.getsize(OUT) / 1e6:.2f} MB, {len(g)} arrays")
