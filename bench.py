@@ -57,6 +57,7 @@ def parse_args():
     ap.add_argument("--box", type=int, default=N_BOX)
     ap.add_argument("--slices", type=int, default=N_SLICES)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fused", action="store_true", help="skip the fused-MSE leg")
     ap.add_argument("--e2e-chunk", type=int, default=256, help="slices per streamed chunk in the e2e leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1024, help="slices per CPU-baseline sample")
@@ -481,6 +482,51 @@ def main():
             "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
             else "fallback 6.65 TB/s"}
 
+    # ---- the same step with the fused loss op (losses.central_slice_mse) ----
+    # extraction, squared error and both gradients in one kernel (the slices
+    # are never written, the upstream gradient never read); then the insertion.
+    fused = None
+    if not args.no_fused and not det:
+        def fused_step(ev=None):
+            V.grad = None
+            R.grad = None
+            if ev:
+                ev[0].record(stream)
+            lf = tt.losses.central_slice_mse(V, shape, R, T)
+            lf.backward()
+            if ev:
+                ev[1].record(stream)
+            insert(T, R.detach())
+            if ev:
+                ev[2].record(stream)
+            if world > 1:
+                tt.distributed.all_reduce_volume_gradient(V.grad)
+            return lf
+
+        for _ in range(max(args.warmup, 0)):
+            fused_step()
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+        f_ev = []
+        fs, fe = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fs.record(stream)
+        for _ in range(args.steps):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            fused_step(ev)
+            f_ev.append(ev)
+        fe.record(stream)
+        torch.cuda.synchronize(dev)
+        el_f = fs.elapsed_time(fe)
+        if world > 1:
+            t = torch.tensor([el_f], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            el_f = float(t.item())
+        fused = {"value": world * ns * args.steps / (el_f / 1e3), "unit": UNIT, "ms_per_step": el_f / args.steps,
+                 "op": "losses.central_slice_mse (extract + MSE + d/dvolume + d/drotation, one kernel) + insert",
+                 "kernels_ms": {"fused_mse": round(statistics.mean(e[0].elapsed_time(e[1]) for e in f_ev), 4),
+                                "insert": round(statistics.mean(e[1].elapsed_time(e[2]) for e in f_ev), 4)}}
+
     # ---- end to end through the public API with host buffers ----
     # The targets and rotations stream from pinned host memory in chunks; the
     # copy of chunk k+1 overlaps the extract / backward / insert of chunk k.
@@ -551,6 +597,7 @@ def main():
                                                       if world > 1 else ""),
                        "deterministic": det},
             "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "fused_mse": fused,
             # extract, backward, rotation-gradient finish, insert splat, insert finalize
             # (+ absmax pre-passes and the fixed-point add-back when deterministic)
             "gpu_launches": (8 if det else 5) * args.steps,

@@ -122,6 +122,25 @@ int tt_extract_central_slices_rfft_3d_backward(const void *volume_rfft,
                                                size_t workspace_bytes,
                                                const tt_slice_params *p, void *stream);
 
+/* Fused extraction + mean squared error + backward, for fitting a volume
+ * and/or orientations to target slices:
+ *   *loss = mean over the n * img_h * (img_w/2+1) complex elements of
+ *           |extract(volume_rfft, R) - targets|^2            (device float)
+ * and, for the loss itself as the objective (upstream gradient 1),
+ * grad_volume (nullable, ACCUMULATED into) and grad_rotation (nullable, (n,3,3)
+ * in the rotation dtype, overwritten) — the gradients
+ * tt_extract_central_slices_rfft_3d_backward computes for G = 2 (S - T) / M,
+ * without writing S or reading G: the sample is rebuilt from the corner
+ * values the rotation gradient loads anyway.  The loss and the rotation
+ * gradient are reduced in a fixed order.  targets: complex64 (n, img_h, img_w/2+1).
+ * Workspace: tt_central_slice_mse_workspace_bytes.  No deterministic mode.
+ * The reference has no fused loss; this replaces extract_central_slices_rfft_3d
+ * + a torch MSE + its autograd backward. */
+size_t tt_central_slice_mse_workspace_bytes(const tt_slice_params *p);
+int tt_central_slice_mse(const void *volume_rfft, const void *rotation_matrices, const void *targets,
+                         float *loss, void *grad_volume, void *grad_rotation, void *workspace,
+                         size_t workspace_bytes, const tt_slice_params *p, void *stream);
+
 /* Size of the built-in scratch array used by
  * tt_extract_central_slices_rfft_3d_backward_noalloc (per GPU, for the life of
  * the process). */

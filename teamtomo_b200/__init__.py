@@ -5,7 +5,7 @@ the 3D interpolation API of torch-image-interpolation, running on
 hand-written sm_100a CUDA kernels through the C ABI in include/teamtomo_b200.h.
 """
 
-from . import distributed, streaming, torch_fourier_slice, torch_image_interpolation
+from . import distributed, losses, streaming, torch_fourier_slice, torch_image_interpolation
 from .torch_fourier_slice import (
     backproject_2d_to_3d,
     backproject_2d_to_3d_multichannel,
@@ -22,6 +22,7 @@ __version__ = "0.1.0"
 
 __all__ = [
     "distributed",
+    "losses",
     "streaming",
     "torch_fourier_slice",
     "torch_image_interpolation",

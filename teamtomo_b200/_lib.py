@@ -69,6 +69,8 @@ SIGNATURES = {
         [_vp, _vp, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_extract_central_slices_rfft_3d_backward_noalloc": (
         [_vp, _vp, _vp, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_central_slice_mse_workspace_bytes": ([ctypes.POINTER(SliceParams)], _sz),
+    "tt_central_slice_mse": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_central_slices_rfft_3d": (
         [_vp, _i32, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_accumulator_bytes": ([_i32, _i64, _i64, _i64, _i64], _sz),

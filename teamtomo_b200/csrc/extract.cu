@@ -72,9 +72,81 @@ struct DvTarget {
     }
 };
 
-// Backward of one slice pixel; acc receives the pixel's 6 contributions to
-// d/dR_zyx (rows z, y, x x columns y, x — column 0 multiplies the zero z
-// frequency of a central slice).
+// d/dvolume scatter of G' over the grid_sample corners of one pixel.
+template <bool FIXED>
+__device__ __forceinline__ void scatter_dv(const DvTarget<FIXED>& dv, const SliceGeom& g, const Corners& k,
+                                           float2 gv) {
+#pragma unroll
+    for (int bz = 0; bz < 2; bz++) {
+        if (bz && !k.zin) continue;
+        const float wz = bz ? k.az1 : k.az0;
+#pragma unroll
+        for (int by = 0; by < 2; by++) {
+            if (by && !k.yin) continue;
+            const float wzy = (by ? k.ay1 : k.ay0) * wz;
+            const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
+#pragma unroll
+            for (int bx = 0; bx < 2; bx++) {
+                if (bx && !k.xin) continue;
+                const float w = (bx ? k.ax1 : k.ax0) * wzy;
+                if (w != 0.0f) dv.add(base + bx, gv, w);
+            }
+        }
+    }
+}
+
+// The eight corner values of a pixel; corners past the last index read as
+// zero, as in grid_sample.
+__device__ __forceinline__ void load_corners(const float2* __restrict__ vol, const SliceGeom& g, const Corners& k,
+                                             float2 v[2][2][2]) {
+#pragma unroll
+    for (int bz = 0; bz < 2; bz++)
+#pragma unroll
+        for (int by = 0; by < 2; by++) {
+            const bool row_ok = (!bz || k.zin) && (!by || k.yin);
+            const int64_t base = vox_index(g, k.z0 + (row_ok ? bz : 0), k.y0 + (row_ok ? by : 0), k.x0);
+#pragma unroll
+            for (int bx = 0; bx < 2; bx++) {
+                const bool ok = row_ok && (!bx || k.xin);
+                v[bz][by][bx] = ok ? __ldg(vol + base + bx) : make_float2(0.f, 0.f);
+            }
+        }
+}
+
+// The pixel's 6 contributions to d/dR_zyx (rows z, y, x x columns y, x —
+// column 0 multiplies the zero z frequency of a central slice) from its
+// corner values: the trilinear gradient from differences of neighbouring
+// voxels (subtracting first keeps it accurate where the volume varies
+// slowly), then Re(conj(G') dV/dc) chained through dc/dp and the redirect sign.
+__device__ __forceinline__ void drot_terms(const float2 v[2][2][2], const Corners& k, float2 gv, bool cj,
+                                           const SliceGeom& g, float qy, float qx, float acc[6]) {
+    float2 gz = make_float2(0.f, 0.f), gy = gz, gx = gz;
+    const float wzs[2] = {k.az0, k.az1}, wys[2] = {k.ay0, k.ay1}, wxs[2] = {k.ax0, k.ax1};
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            const float wyx = wys[a] * wxs[b], wzx = wzs[a] * wxs[b], wzy = wzs[a] * wys[b];
+            gz.x = fmaf(wyx, v[1][a][b].x - v[0][a][b].x, gz.x);
+            gz.y = fmaf(wyx, v[1][a][b].y - v[0][a][b].y, gz.y);
+            gy.x = fmaf(wzx, v[a][1][b].x - v[a][0][b].x, gy.x);
+            gy.y = fmaf(wzx, v[a][1][b].y - v[a][0][b].y, gy.y);
+            gx.x = fmaf(wzy, v[a][b][1].x - v[a][b][0].x, gx.x);
+            gx.y = fmaf(wzy, v[a][b][1].y - v[a][b][0].y, gx.y);
+        }
+    const float sg = cj ? -1.f : 1.f;
+    const float p0 = fmaf(gv.x, gz.x, gv.y * gz.y) * g.dcdp0 * sg;
+    const float p1 = fmaf(gv.x, gy.x, gv.y * gy.y) * g.dcdp1 * sg;
+    const float p2 = fmaf(gv.x, gx.x, gv.y * gx.y) * g.dcdp2 * sg;
+    acc[0] = p0 * qy;
+    acc[1] = p0 * qx;
+    acc[2] = p1 * qy;
+    acc[3] = p1 * qx;
+    acc[4] = p2 * qy;
+    acc[5] = p2 * qx;
+}
+
+// Backward of one slice pixel; acc receives the pixel's 6 contributions to d/dR_zyx.
 template <bool WANT_DV, bool WANT_DR, bool FIXED>
 __device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const float* m,
                                           const float2* __restrict__ grad, const DvTarget<FIXED>& dv,
@@ -85,68 +157,56 @@ __device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const 
     const Corners k = make_corners(g, c);
     float2 gv = __ldcs(grad + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
     if (cj) gv.y = -gv.y;  // G' = conj(G) where the sample was conjugated
-    if (WANT_DV) {
+    if (WANT_DV) scatter_dv(dv, g, k, gv);
+    if (WANT_DR) {
+        float2 v[2][2][2];
+        load_corners(vol, g, k, v);
+        drot_terms(v, k, gv, cj, g, qy, qx, acc);
+    }
+}
+
+// Fused extraction + squared-error loss + backward of one pixel: the sample S
+// is rebuilt from the corner values the rotation gradient needs anyway (same
+// operation order as extract_fwd_kernel), r = S - T, the loss term |r|^2, and
+// G = scale * r (scale = 2 / M for the mean) feeds the two gradients.  Pixels
+// whose sample is zero (outside fftfreq_max or the volume) add |T|^2 and no
+// gradient.
+template <bool WANT_DV, bool WANT_DR>
+__device__ __forceinline__ void mse_point(const float2* __restrict__ vol, const float* m,
+                                          const float2* __restrict__ target, const DvTarget<false>& dv,
+                                          const SliceGeom& g, int64_t s, int iy, int ix, float scale, float acc[6],
+                                          double& loss) {
+    const float2 t = __ldcs(target + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+    float qy, qx, c[3];
+    bool cj = false;
+    if (!extract_geometry(g, m, iy, ix, qy, qx, cj, c)) {
+        loss += (double)t.x * t.x + (double)t.y * t.y;
+        return;
+    }
+    const Corners k = make_corners(g, c);
+    float2 v[2][2][2];
+    load_corners(vol, g, k, v);
+    float2 sv = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int bz = 0; bz < 2; bz++) {
-            if (bz && !k.zin) continue;
-            const float wz = bz ? k.az1 : k.az0;
+    for (int bz = 0; bz < 2; bz++) {
+        const float wz = bz ? k.az1 : k.az0;
 #pragma unroll
-            for (int by = 0; by < 2; by++) {
-                if (by && !k.yin) continue;
-                const float wzy = (by ? k.ay1 : k.ay0) * wz;
-                const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
-#pragma unroll
-                for (int bx = 0; bx < 2; bx++) {
-                    if (bx && !k.xin) continue;
-                    const float w = (bx ? k.ax1 : k.ax0) * wzy;
-                    if (w != 0.0f) dv.add(base + bx, gv, w);
-                }
-            }
+        for (int by = 0; by < 2; by++) {
+            const float wzy = (by ? k.ay1 : k.ay0) * wz;
+            const float w0 = k.ax0 * wzy, w1 = k.ax1 * wzy;
+            sv.x = fmaf(v[bz][by][0].x, w0, sv.x);
+            sv.y = fmaf(v[bz][by][0].y, w0, sv.y);
+            sv.x = fmaf(v[bz][by][1].x, w1, sv.x);
+            sv.y = fmaf(v[bz][by][1].y, w1, sv.y);
         }
     }
-    if (WANT_DR) {
-        // trilinear gradient from differences of neighbouring voxels (subtracting
-        // first keeps it accurate where the volume varies slowly); corners past the
-        // last index read as zero, as in grid_sample
-        float2 v[2][2][2];
-#pragma unroll
-        for (int bz = 0; bz < 2; bz++)
-#pragma unroll
-            for (int by = 0; by < 2; by++) {
-                const bool row_ok = (!bz || k.zin) && (!by || k.yin);
-                const int64_t base = vox_index(g, k.z0 + (row_ok ? bz : 0), k.y0 + (row_ok ? by : 0), k.x0);
-#pragma unroll
-                for (int bx = 0; bx < 2; bx++) {
-                    const bool ok = row_ok && (!bx || k.xin);
-                    v[bz][by][bx] = ok ? __ldg(vol + base + bx) : make_float2(0.f, 0.f);
-                }
-            }
-        float2 gz = make_float2(0.f, 0.f), gy = gz, gx = gz;
-        const float wzs[2] = {k.az0, k.az1}, wys[2] = {k.ay0, k.ay1}, wxs[2] = {k.ax0, k.ax1};
-#pragma unroll
-        for (int a = 0; a < 2; a++)
-#pragma unroll
-            for (int b = 0; b < 2; b++) {
-                const float wyx = wys[a] * wxs[b], wzx = wzs[a] * wxs[b], wzy = wzs[a] * wys[b];
-                gz.x = fmaf(wyx, v[1][a][b].x - v[0][a][b].x, gz.x);
-                gz.y = fmaf(wyx, v[1][a][b].y - v[0][a][b].y, gz.y);
-                gy.x = fmaf(wzx, v[a][1][b].x - v[a][0][b].x, gy.x);
-                gy.y = fmaf(wzx, v[a][1][b].y - v[a][0][b].y, gy.y);
-                gx.x = fmaf(wzy, v[a][b][1].x - v[a][b][0].x, gx.x);
-                gx.y = fmaf(wzy, v[a][b][1].y - v[a][b][0].y, gx.y);
-            }
-        // Re(conj(G') dV/dc), chained through dc/dp and the redirect sign
-        const float sg = cj ? -1.f : 1.f;
-        const float p0 = fmaf(gv.x, gz.x, gv.y * gz.y) * g.dcdp0 * sg;
-        const float p1 = fmaf(gv.x, gy.x, gv.y * gy.y) * g.dcdp1 * sg;
-        const float p2 = fmaf(gv.x, gx.x, gv.y * gx.y) * g.dcdp2 * sg;
-        acc[0] = p0 * qy;
-        acc[1] = p0 * qx;
-        acc[2] = p1 * qy;
-        acc[3] = p1 * qx;
-        acc[4] = p2 * qy;
-        acc[5] = p2 * qx;
-    }
+    if (cj) sv.y = -sv.y;
+    const float rx = sv.x - t.x, ry = sv.y - t.y;
+    loss += (double)rx * rx + (double)ry * ry;
+    float2 gv = make_float2(rx * scale, ry * scale);
+    if (cj) gv.y = -gv.y;
+    if (WANT_DV) scatter_dv(dv, g, k, gv);
+    if (WANT_DR) drot_terms(v, k, gv, cj, g, qy, qx, acc);
 }
 
 // One block per (slice, tile).  WANT_DR: the block's partial sums of the 6
@@ -184,6 +244,60 @@ extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
             for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][threadIdx.x];
             part[((int64_t)s * tiles + tile) * 6 + threadIdx.x] = (float)v;
         }
+    }
+}
+
+// Fused extraction + mean squared error + backward: one block per (slice,
+// tile).  Block partials of the loss (double) go to loss_part[s * tiles + tile]
+// and, with WANT_DR, those of d/dR_zyx to part[(s * tiles + tile) * 6 + k].
+template <bool WANT_DV, bool WANT_DR>
+__global__ void __launch_bounds__(kExtractThreads)
+slice_mse_kernel(const float2* __restrict__ vol, const void* __restrict__ rot, const float2* __restrict__ target,
+                 float2* __restrict__ dvol, float* __restrict__ part, double* __restrict__ loss_part, float scale,
+                 SliceGeom g, int tiles) {
+    __shared__ float m[9];
+    __shared__ double red[kExtractThreads / 32][7];
+    const int64_t s = blockIdx.x / tiles;
+    const int tile = blockIdx.x - (int)(s * tiles);
+    load_rotation(m, rot, s, g, true);
+    __syncthreads();
+    float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    double loss = 0.0;
+    const DvTarget<false> dv{dvol, nullptr, 0.0};
+    int iy, ix;
+    if (tile_pixel(g, tile, iy, ix)) mse_point<WANT_DV, WANT_DR>(vol, m, target, dv, g, s, iy, ix, scale, acc, loss);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+        const double v = warp_sum_d(k < 6 ? (double)acc[k] : loss);
+        if (lane == 0) red[warp][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 7) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][threadIdx.x];
+        const int64_t b = (int64_t)s * tiles + tile;
+        if (threadIdx.x == 6)
+            loss_part[b] = v;
+        else if (WANT_DR)
+            part[b * 6 + threadIdx.x] = (float)v;
+    }
+}
+
+// loss = inv_m * sum of the block partials, summed in a fixed order by one block.
+__global__ void __launch_bounds__(1024) mse_loss_finish_kernel(const double* __restrict__ loss_part, int64_t count,
+                                                               double inv_m, float* __restrict__ loss) {
+    __shared__ double red[32];
+    double v = 0.0;
+    for (int64_t i = threadIdx.x; i < count; i += blockDim.x) v += loss_part[i];
+    v = warp_sum_d(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        v = warp_sum_d(v);
+        if (threadIdx.x == 0) *loss = (float)(v * inv_m);
     }
 }
 
@@ -315,6 +429,66 @@ static int launch_backward(const float2* v, const void* rot, const float2* gr, f
 }  // namespace tt
 
 using namespace tt;
+
+static size_t mse_workspace_bytes(int64_t n, int tiles) {
+    return (size_t)(n * tiles) * sizeof(double) + partial_bytes(n, tiles);
+}
+
+extern "C" size_t tt_central_slice_mse_workspace_bytes(const tt_slice_params* p) {
+    if (!p || p->n <= 0 || p->img_h < 1 || p->img_w < 1) return 0;
+    return mse_workspace_bytes(p->n, tiles_per_slice((int)p->img_h, (int)(p->img_w / 2 + 1)));
+}
+
+extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotation_matrices, const void* targets,
+                                    float* loss, void* grad_volume, void* grad_rotation, void* workspace,
+                                    size_t workspace_bytes, const tt_slice_params* p, void* stream) {
+    if (int e = validate_params(p)) return e;
+    if (p->deterministic)
+        return fail(TT_ERR_INVALID, "central_slice_mse: no deterministic mode (the gradient scale is known only "
+                                    "after the loss); use the extraction backward");
+    if (p->n == 0) return fail(TT_ERR_INVALID, "central_slice_mse: no slices (the mean is undefined)");
+    if (!volume_rfft || !rotation_matrices || !targets || !loss)
+        return fail(TT_ERR_INVALID, "central_slice_mse: NULL pointer argument");
+    SliceGeom g = make_geom(*p);
+    const int tiles = extract_tiles(g);
+    const int64_t blocks = (int64_t)g.n * tiles;
+    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "central_slice_mse: too many blocks");
+    const size_t need = mse_workspace_bytes(g.n, tiles);
+    if (!workspace || workspace_bytes < need)
+        return fail(TT_ERR_WORKSPACE, "central_slice_mse: workspace of %zu bytes needed, got %zu", need,
+                    workspace_bytes);
+    double* loss_part = (double*)workspace;
+    float* part = (float*)((char*)workspace + (size_t)blocks * sizeof(double));
+    const double m = (double)g.n * g.img_h * g.wr;
+    const float scale = (float)(2.0 / m);
+    const float2* v = (const float2*)volume_rfft;
+    const float2* t = (const float2*)targets;
+    float2* dv = (float2*)grad_volume;
+    cudaStream_t st = as_stream(stream);
+    const unsigned nb = (unsigned)blocks;
+    if (dv && grad_rotation)
+        slice_mse_kernel<true, true><<<nb, kExtractThreads, 0, st>>>(v, rotation_matrices, t, dv, part, loss_part,
+                                                                    scale, g, tiles);
+    else if (dv)
+        slice_mse_kernel<true, false><<<nb, kExtractThreads, 0, st>>>(v, rotation_matrices, t, dv, part, loss_part,
+                                                                     scale, g, tiles);
+    else if (grad_rotation)
+        slice_mse_kernel<false, true><<<nb, kExtractThreads, 0, st>>>(v, rotation_matrices, t, dv, part, loss_part,
+                                                                     scale, g, tiles);
+    else
+        slice_mse_kernel<false, false><<<nb, kExtractThreads, 0, st>>>(v, rotation_matrices, t, dv, part,
+                                                                      loss_part, scale, g, tiles);
+    if (int e = check_launch("slice_mse_kernel")) return e;
+    mse_loss_finish_kernel<<<1, 1024, 0, st>>>(loss_part, blocks, 1.0 / m, loss);
+    if (int e = check_launch("mse_loss_finish_kernel")) return e;
+    if (grad_rotation) {
+        const int64_t total = (int64_t)g.n * 9;
+        drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rotation_matrices, grad_rotation,
+                                                                            g, tiles);
+        if (int e = check_launch("drot_finish_kernel")) return e;
+    }
+    return TT_OK;
+}
 
 extern "C" int tt_extract_central_slices_rfft_3d(const void* volume_rfft, const void* rotation_matrices,
                                                  void* slices_out, const tt_slice_params* p, void* stream) {

@@ -266,3 +266,24 @@ def test_streaming_host_checks():
         next(streaming.prefetch_to_device([torch.zeros(3), torch.zeros(4)], 2, "cpu"))
     with pytest.raises(ValueError, match="data_bound"):
         streaming.InsertionAccumulator((8, 8, 8), "cpu", deterministic=True)
+
+
+def test_fused_mse_validation():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    fake = ctypes.c_void_p(16)
+    p = _params()
+    need = L.tt_central_slice_mse_workspace_bytes(ctypes.byref(p))
+    tiles = ((9 + 7) // 8) * ((16 + 31) // 32)
+    assert need == 4 * tiles * 8 + 4 * tiles * 6 * 4
+    assert L.tt_central_slice_mse(fake, fake, fake, fake, None, None, fake, 8, ctypes.byref(p),
+                                  None) == _lib.TT_ERR_WORKSPACE
+    assert L.tt_central_slice_mse(fake, fake, fake, None, None, None, fake, need, ctypes.byref(p),
+                                  None) == _lib.TT_ERR_INVALID
+    p = _params(deterministic=1)
+    assert L.tt_central_slice_mse(fake, fake, fake, fake, None, None, fake, need, ctypes.byref(p),
+                                  None) == _lib.TT_ERR_INVALID
+    p = _params(n=0)
+    assert L.tt_central_slice_mse(fake, fake, fake, fake, None, None, fake, need, ctypes.byref(p),
+                                  None) == _lib.TT_ERR_INVALID
