@@ -51,13 +51,15 @@ WORKLOAD = ("extract_central_slices_rfft_3d fwd + MSE vs noisy targets + bwd (d/
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--box", type=int, default=N_BOX)
     ap.add_argument("--slices", type=int, default=N_SLICES)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fused", action="store_true", help="skip the fused-MSE leg")
+    ap.add_argument("--no-torch-gpu", action="store_true", help="skip timing the reference's torch code on the GPU")
+    ap.add_argument("--torch-gpu-sample", type=int, default=512, help="slices timed on the reference's torch path")
     ap.add_argument("--e2e-chunk", type=int, default=256, help="slices per streamed chunk in the e2e leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1024, help="slices per CPU-baseline sample")
@@ -122,7 +124,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (FileNotFoundError, OSError):
@@ -234,6 +236,54 @@ def reference_arm(args):
 # ----------------------------------------------------------------------------
 # GPU arm
 # ----------------------------------------------------------------------------
+
+def torch_gpu_reference(dev, n, V0, R0, T, sample, chunk=128):
+    """The reference's own torch code (baseline/_ref, unmodified, placed there
+    by baseline/install_reference.py) run on the GPU for the same step:
+    extraction, the same MSE, its autograd backward for d/drotation, and the
+    insertion of the targets (partial volumes summed), chunked over slices.
+    Its autograd w.r.t. the volume expands the volume per sample (4.5 TB at
+    128^3 x 64 slices), so d/dvolume is left out of this leg."""
+    import torch
+
+    ref_dir = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref_dir, "torch_fourier_slice")):
+        return {"unavailable": "baseline/_ref missing (run baseline/install_reference.py where the reference is)"}
+    if ref_dir not in sys.path:
+        sys.path.insert(0, ref_dir)
+    from torch_fourier_slice import extract_central_slices_rfft_3d as ref_extract
+    from torch_fourier_slice import insert_central_slices_rfft_3d as ref_insert
+
+    shape = (n, n, n)
+    sample = min(sample, R0.shape[0])
+    Rs = R0[:sample].detach().double()  # a float32 leaf would be zeroed in place by the reference and raise
+
+    def step():
+        vol_sum = None
+        for s0 in range(0, sample, chunk):
+            R = Rs[s0:s0 + chunk].clone().requires_grad_(True)
+            S = ref_extract(V0, shape, R)
+            loss = (S - T[s0:s0 + chunk]).abs().square().mean()
+            loss.backward()
+            vol, w = ref_insert(T[s0:s0 + chunk], shape, R.detach())
+            vol_sum = vol if vol_sum is None else vol_sum + vol
+        return vol_sum
+
+    step()
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 2
+    a.record()
+    for _ in range(reps):
+        step()
+    b.record()
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b) / reps
+    return {"value": sample / (ms / 1e3), "unit": UNIT, "ms_per_sample": ms,
+            "sample": f"{sample} of the 4096 slices, chunks of {chunk}, volume without grad",
+            "excluded": "d/dvolume (the reference's autograd expands the volume per sample)",
+            "code": "reference torch_fourier_slice, unmodified, CUDA tensors"}
+
 
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -582,6 +632,14 @@ def main():
                "d2h_bytes_per_step": d2h, "steps": e2e_steps, "chunk_slices": args.e2e_chunk,
                "overlap": "H2D of chunk k+1 on a copy stream during compute of chunk k"}
 
+    torch_gpu = None
+    if rank == 0 and world == 1 and not args.no_torch_gpu:
+        with torch.no_grad():
+            V_ref = V.detach().clone()
+        torch_gpu = torch_gpu_reference(dev, n, V_ref, R0, T, args.torch_gpu_sample)
+        if "value" in torch_gpu:
+            torch_gpu["ours_over_torch_gpu"] = round(value / torch_gpu["value"], 1)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_baseline(n, args.cpu_sample)
@@ -597,7 +655,7 @@ def main():
                                                       if world > 1 else ""),
                        "deterministic": det},
             "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "fused_mse": fused,
+            "fused_mse": fused, "torch_gpu_reference": torch_gpu,
             # extract, backward, rotation-gradient finish, insert splat, insert finalize
             # (+ absmax pre-passes and the fixed-point add-back when deterministic)
             "gpu_launches": (8 if det else 5) * args.steps,
