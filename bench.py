@@ -65,7 +65,8 @@ def parse_args():
     ap.add_argument("--cpu-sample", type=int, default=1024, help="slices per CPU-baseline sample")
     ap.add_argument("--deterministic", action="store_true",
                     help="64-bit fixed-point insertion and volume gradient (bit-reproducible)")
-    ap.add_argument("--workload", choices=["differentiation", "batched"], default="differentiation",
+    ap.add_argument("--workload", choices=["differentiation", "batched", "project", "backproject", "fullscale"],
+                    default="differentiation",
                     help="differentiation: the 256^3 extract+insert+bwd step (headline); batched: 32 "
                          "uneven CTF-weighted volumes in one graph-captured launch per stage")
     return ap.parse_args()
@@ -387,12 +388,162 @@ def batched_workload(args):
     return 0
 
 
+def _ref_module():
+    """The reference's torch_fourier_slice from baseline/_ref, or None."""
+    ref_dir = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref_dir, "torch_fourier_slice")):
+        return None
+    if ref_dir not in sys.path:
+        sys.path.insert(0, ref_dir)
+    import torch_fourier_slice
+
+    return torch_fourier_slice
+
+
+def _time_device(fn, steps, warmup, dev):
+    import torch
+
+    for _ in range(max(warmup, 0)):
+        fn()
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        fn()
+    b.record()
+    torch.cuda.synchronize(dev)
+    return a.elapsed_time(b) / steps
+
+
+def config_workload(args):
+    """The other configurations of the path, one JSON line each:
+    project     project_3d_to_2d of a 64^3 Gaussian-blob volume at 100 rotations (pad 2.0)
+    backproject backproject_2d_to_3d of 10,000 128^2 noisy projections (SNR 0.1), pad 1.0 and 2.0
+    fullscale   CTF-weighted insertion of 200,000 320^2 noisy images (SNR 0.05, defocus U(0.8, 2.5) um)
+                into a 320^3 volume, then 100,000-orientation extraction with forward + backward
+                (fused MSE against the images), generated on the GPU chunk by chunk (82 GB of images)
+    Each times our path with CUDA events and, where the reference can run on this GPU, the
+    reference's own torch code (baseline/_ref) on a bounded sample."""
+    import torch
+
+    import teamtomo_b200 as tt
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    ref = _ref_module()
+    peak, peak_kind = load_peaks()
+    clocks = ClockSampler(dev.index)
+    out = {"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
+    if args.workload == "project":
+        n, k = 64, 100
+        vol = blob_volume_torch(n, 1001, dev)
+        R = torch.tensor(rotations(k, 1001), device=dev)
+        clocks.start()
+        ms = _time_device(lambda: tt.project_3d_to_2d(vol, R), args.steps, args.warmup, dev)
+        clk = clocks.stop()
+        ref_ms = (_time_device(lambda: ref.project_3d_to_2d(vol, R), 5, 2, dev) if ref else None)
+        out.update({"metric": "slices/s project_3d_to_2d 64^3 pad 2.0", "value": k / (ms / 1e3), "unit": "slices/s",
+                    "ms_per_step": ms, "config": {"workload": "project 64^3 x 100 rotations, pad 2.0"},
+                    "torch_gpu_reference": None if ref is None else {"value": k / (ref_ms / 1e3), "ms": ref_ms},
+                    "clocks": clk, "gpu_launches": 4 * args.steps})
+    elif args.workload == "backproject":
+        n, k = 128, 10_000
+        vol = blob_volume_torch(n, 1002, dev)
+        R = torch.tensor(rotations(k, 1002), device=dev)
+        with torch.no_grad():
+            proj = torch.cat([tt.project_3d_to_2d(vol, R[i:i + 1000]) for i in range(0, k, 1000)])
+            gen = torch.Generator(device=dev).manual_seed(1002)
+            noise = torch.randn(proj.shape, device=dev, generator=gen) * (proj.var() / 0.1).sqrt()
+            imgs = (proj + noise).contiguous()
+        del proj, noise
+        res = {}
+        clocks.start()
+        for pf in (1.0, 2.0):
+            ms = _time_device(lambda: tt.backproject_2d_to_3d(imgs, R, pad_factor=pf), args.steps, args.warmup,
+                              dev)
+            res[f"pad{pf:g}"] = {"value": k / (ms / 1e3), "ms_per_step": ms}
+        clk = clocks.stop()
+        refres = None
+        if ref is not None:
+            m = 1000  # bounded sample of the reference
+            refres = {}
+            for pf in (1.0, 2.0):
+                rms = _time_device(lambda: ref.backproject_2d_to_3d(imgs[:m], R[:m], pad_factor=pf), 2, 1, dev)
+                refres[f"pad{pf:g}"] = {"value": m / (rms / 1e3), "sample": m}
+        out.update({"metric": "images/s backproject_2d_to_3d 10,000 x 128^2", "value": res["pad1"]["value"],
+                    "unit": "images/s", "ms_per_step": res["pad1"]["ms_per_step"],
+                    "config": {"workload": "backproject 10,000 x 128^2 (SNR 0.1); value at pad 1.0 "
+                               "(128x128x65 volume), pad 2.0 beside it"},
+                    "pads": res, "torch_gpu_reference": refres, "clocks": clk, "gpu_launches": 5 * args.steps})
+    else:
+        n, n_img, n_ext, chunk = 320, 200_000, 100_000, 10_000
+        vol_real = blob_volume_torch(n, 1005, dev)
+        V = rfft_volume_torch(vol_real)
+        shape = (n, n, n)
+        from teamtomo_b200 import batched
+
+        def images(i0, m):
+            """Chunk [i0, i0+m): rotations, CTF rows, noisy CTF-modulated slices of the map."""
+            R = torch.tensor(rotations(m, 50_000 + i0), device=dev)
+            rng = np.random.default_rng(60_000 + i0)
+            ctf = batched.ctf_params(rng.uniform(0.8, 2.5, m), voltage_kv=300.0, spherical_aberration_mm=2.7,
+                                     amplitude_contrast=0.07, pixel_size_a=1.0, device=dev)
+            with torch.no_grad():
+                S = batched.extract_central_slices_rfft_3d_batched([V], [R], ctf=[ctf])[0]
+                gen = torch.Generator(device=dev).manual_seed(70_000 + i0)
+                S = S + torch.randn(S.shape, dtype=S.dtype, device=dev, generator=gen) * (
+                    S.abs().square().mean() / 0.05).sqrt()
+            return R, ctf, S
+
+        torch.cuda.synchronize(dev)
+        ins_ms = ext_ms = 0.0
+        vol_sum = w_sum = None
+        clocks.start()
+        for i0 in range(0, n_img, chunk):
+            R, ctf, S = images(i0, chunk)
+            torch.cuda.synchronize(dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            (v, w), = batched.insert_central_slices_rfft_3d_batched([S], [R], ctf=[ctf])
+            vol_sum = v if vol_sum is None else vol_sum.add_(v)
+            w_sum = w if w_sum is None else w_sum.add_(w)
+            b.record()
+            torch.cuda.synchronize(dev)
+            ins_ms += a.elapsed_time(b)
+        Vfit = (vol_sum / torch.clamp(w_sum, min=1.0)).detach().requires_grad_(True)
+        for i0 in range(0, n_ext, chunk):
+            R, ctf, S = images(i0, chunk)
+            Rg = R.float().requires_grad_(True)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            tt.losses.central_slice_mse(Vfit, shape, Rg, S).backward()
+            b.record()
+            torch.cuda.synchronize(dev)
+            ext_ms += a.elapsed_time(b)
+        clk = clocks.stop()
+        out.update({"metric": "images/s CTF-weighted insertion, 320^3, 200,000 images; then slices/s extract "
+                              "fwd+bwd, 100,000 orientations",
+                    "value": n_img / (ins_ms / 1e3), "unit": "images/s", "ms_per_step": ins_ms + ext_ms,
+                    "steps": 1, "warmup": 0,
+                    "extract_fwd_bwd": {"value": n_ext / (ext_ms / 1e3), "unit": "slices/s", "ms": ext_ms},
+                    "insert_ms": ins_ms,
+                    "config": {"workload": "full scale: 320^3 complex64 rfft volume (320x320x161), "
+                               f"images generated on the GPU in chunks of {chunk} (not timed)",
+                               "images": n_img, "orientations": n_ext},
+                    "torch_gpu_reference": None, "clocks": clk, "gpu_launches": n_img // chunk * 3 + n_ext // chunk * 3})
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
     if args.workload == "batched":
         return batched_workload(args)
+    if args.workload in ("project", "backproject", "fullscale"):
+        return config_workload(args)
 
     import torch
     import torch.distributed as dist
