@@ -269,6 +269,36 @@ int tt_insert_fixed_finalize(const void *accumulator, int32_t complex128, int64_
                              int64_t d, int64_t h, int64_t w_rfft, const uint32_t *absmax_bits,
                              int64_t max_slices, void *volume_rfft, void *weights, void *stream);
 
+/* ---- multichannel slices (c volumes, one set of rotations) -------------
+ * Each pixel's geometry is computed once and applied to every channel.
+ * Volumes (channels, vol_d, vol_h, vol_w) complex64; slices
+ * (n, channels, img_h, img_w/2+1) complex64 — the reference's (..., c, h, w)
+ * layout.  Replace the per-channel loops of
+ * extract_central_slices_rfft_3d_multichannel (_extract_central_slices_rfft_3d.py:225-367)
+ * and insert_central_slices_rfft_3d_multichannel (_insert_central_slices_rfft_3d.py:109-210). */
+int tt_extract_central_slices_rfft_3d_multichannel(const void *volume_rfft, int64_t channels,
+                                                   const void *rotation_matrices, void *slices_out,
+                                                   const tt_slice_params *p, void *stream);
+/* grad_volume (channels, ...) ACCUMULATED into; grad_rotation summed over the
+ * channels (workspace: tt_extract_backward_workspace_bytes with
+ * p->deterministic = 0; no deterministic mode here). */
+int tt_extract_central_slices_rfft_3d_multichannel_backward(
+    const void *volume_rfft, int64_t channels, const void *rotation_matrices,
+    const void *grad_slices, void *grad_volume, void *grad_rotation, void *workspace,
+    size_t workspace_bytes, const tt_slice_params *p, void *stream);
+/* Splat of (n, channels, h, w/2+1) complex64 slices into `channels` caller-zeroed
+ * float accumulators (tt_insert_accumulator_bytes(0, channels, ...)); the
+ * interpolation weights go to channel 0, which tt_insert_finalize reads. */
+int tt_insert_accumulate_multichannel(const void *image_rfft, int64_t channels,
+                                      const void *rotation_matrices, void *accumulator,
+                                      const tt_slice_params *p, void *stream);
+/* Backward of the multichannel insertion w.r.t. the slices (per channel as
+ * tt_insert_central_slices_rfft_3d_backward), complex64; grad_image overwritten. */
+int tt_insert_central_slices_rfft_3d_multichannel_backward(const void *grad_volume, int64_t channels,
+                                                           const void *rotation_matrices,
+                                                           void *grad_image,
+                                                           const tt_slice_params *p, void *stream);
+
 /* ---- batched, CTF-weighted slices over many volumes -------------------
  * Many volumes of uneven box size, each with its own rotations and optional
  * per-image CTF, in ONE persistent launch whose blocks take slices from a
@@ -342,8 +372,9 @@ int tt_pad_fftshift_2d(const void *images, int32_t is_f64, int64_t m, int64_t d,
                        void *out, void *stream);
 
 /* Friedel completion + division by max(weights, 1) + ifftshift along (d, h)
- * of `channels` insertion accumulators (tt_insert_accumulate, not finalized)
- * into complex volumes out (channels, d, h, w_rfft) (backproject.py:66-79). */
+ * of `channels` insertion accumulators (tt_insert_accumulate, not finalized;
+ * the weights are read from channel 0) into complex volumes out
+ * (channels, d, h, w_rfft) (backproject.py:66-79). */
 int tt_backproject_normalize(const void *accumulator, int32_t complex128, int64_t channels,
                              int64_t d, int64_t h, int64_t w_rfft, void *out, void *stream);
 

@@ -83,6 +83,13 @@ SIGNATURES = {
     "tt_insert_fixed_accumulator_bytes": ([_i64, _i64, _i64, _i64], _sz),
     "tt_insert_fixed_accumulate": ([_vp, _i32, _vp, _vp, _vp, _i64, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_fixed_finalize": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _vp], _i32),
+    "tt_extract_central_slices_rfft_3d_multichannel": ([_vp, _i64, _vp, _vp, ctypes.POINTER(SliceParams), _vp],
+                                                       _i32),
+    "tt_extract_central_slices_rfft_3d_multichannel_backward": (
+        [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_insert_accumulate_multichannel": ([_vp, _i64, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_insert_central_slices_rfft_3d_multichannel_backward": (
+        [_vp, _i64, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_batch_workspace_bytes": ([], _sz),
     "tt_extract_central_slices_rfft_3d_batched": (
         [ctypes.POINTER(BatchVolume), _i32, _i32, _vp, _sz, _vp], _i32),

@@ -23,6 +23,7 @@
 #include "capi_util.cuh"
 #include "fixed_point.cuh"
 #include "slice_common.cuh"
+#include "slice_grad.cuh"
 #include "slice_ops.cuh"
 
 namespace tt {
@@ -53,97 +54,6 @@ extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     }
     // streaming store: the slices are written once and should not evict the volume from L2
     __stcs(out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, r);
-}
-
-// Volume-gradient target: float2 atomics, or (FIXED, the deterministic mode)
-// two 64-bit fixed-point words per voxel at scale `scale`.
-template <bool FIXED>
-struct DvTarget {
-    float2* dvol;
-    unsigned long long* fixed;
-    double scale;
-    __device__ __forceinline__ void add(int64_t vi, float2 gv, float w) const {
-        if (FIXED) {
-            fixed_add(fixed + 2 * vi, (double)gv.x * (double)w * scale);
-            fixed_add(fixed + 2 * vi + 1, (double)gv.y * (double)w * scale);
-        } else {
-            atomicAdd(dvol + vi, make_float2(gv.x * w, gv.y * w));
-        }
-    }
-};
-
-// d/dvolume scatter of G' over the grid_sample corners of one pixel.
-template <bool FIXED>
-__device__ __forceinline__ void scatter_dv(const DvTarget<FIXED>& dv, const SliceGeom& g, const Corners& k,
-                                           float2 gv) {
-#pragma unroll
-    for (int bz = 0; bz < 2; bz++) {
-        if (bz && !k.zin) continue;
-        const float wz = bz ? k.az1 : k.az0;
-#pragma unroll
-        for (int by = 0; by < 2; by++) {
-            if (by && !k.yin) continue;
-            const float wzy = (by ? k.ay1 : k.ay0) * wz;
-            const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
-#pragma unroll
-            for (int bx = 0; bx < 2; bx++) {
-                if (bx && !k.xin) continue;
-                const float w = (bx ? k.ax1 : k.ax0) * wzy;
-                if (w != 0.0f) dv.add(base + bx, gv, w);
-            }
-        }
-    }
-}
-
-// The eight corner values of a pixel; corners past the last index read as
-// zero, as in grid_sample.
-__device__ __forceinline__ void load_corners(const float2* __restrict__ vol, const SliceGeom& g, const Corners& k,
-                                             float2 v[2][2][2]) {
-#pragma unroll
-    for (int bz = 0; bz < 2; bz++)
-#pragma unroll
-        for (int by = 0; by < 2; by++) {
-            const bool row_ok = (!bz || k.zin) && (!by || k.yin);
-            const int64_t base = vox_index(g, k.z0 + (row_ok ? bz : 0), k.y0 + (row_ok ? by : 0), k.x0);
-#pragma unroll
-            for (int bx = 0; bx < 2; bx++) {
-                const bool ok = row_ok && (!bx || k.xin);
-                v[bz][by][bx] = ok ? __ldg(vol + base + bx) : make_float2(0.f, 0.f);
-            }
-        }
-}
-
-// The pixel's 6 contributions to d/dR_zyx (rows z, y, x x columns y, x —
-// column 0 multiplies the zero z frequency of a central slice) from its
-// corner values: the trilinear gradient from differences of neighbouring
-// voxels (subtracting first keeps it accurate where the volume varies
-// slowly), then Re(conj(G') dV/dc) chained through dc/dp and the redirect sign.
-__device__ __forceinline__ void drot_terms(const float2 v[2][2][2], const Corners& k, float2 gv, bool cj,
-                                           const SliceGeom& g, float qy, float qx, float acc[6]) {
-    float2 gz = make_float2(0.f, 0.f), gy = gz, gx = gz;
-    const float wzs[2] = {k.az0, k.az1}, wys[2] = {k.ay0, k.ay1}, wxs[2] = {k.ax0, k.ax1};
-#pragma unroll
-    for (int a = 0; a < 2; a++)
-#pragma unroll
-        for (int b = 0; b < 2; b++) {
-            const float wyx = wys[a] * wxs[b], wzx = wzs[a] * wxs[b], wzy = wzs[a] * wys[b];
-            gz.x = fmaf(wyx, v[1][a][b].x - v[0][a][b].x, gz.x);
-            gz.y = fmaf(wyx, v[1][a][b].y - v[0][a][b].y, gz.y);
-            gy.x = fmaf(wzx, v[a][1][b].x - v[a][0][b].x, gy.x);
-            gy.y = fmaf(wzx, v[a][1][b].y - v[a][0][b].y, gy.y);
-            gx.x = fmaf(wzy, v[a][b][1].x - v[a][b][0].x, gx.x);
-            gx.y = fmaf(wzy, v[a][b][1].y - v[a][b][0].y, gx.y);
-        }
-    const float sg = cj ? -1.f : 1.f;
-    const float p0 = fmaf(gv.x, gz.x, gv.y * gz.y) * g.dcdp0 * sg;
-    const float p1 = fmaf(gv.x, gy.x, gv.y * gy.y) * g.dcdp1 * sg;
-    const float p2 = fmaf(gv.x, gx.x, gv.y * gx.y) * g.dcdp2 * sg;
-    acc[0] = p0 * qy;
-    acc[1] = p0 * qx;
-    acc[2] = p1 * qy;
-    acc[3] = p1 * qx;
-    acc[4] = p2 * qy;
-    acc[5] = p2 * qx;
 }
 
 // Backward of one slice pixel; acc receives the pixel's 6 contributions to d/dR_zyx.
@@ -379,6 +289,13 @@ __global__ void dv_fixed_add_kernel(const long long* __restrict__ fixed, float2*
 }
 
 static size_t partial_bytes(int64_t n, int tiles) { return (size_t)(n * tiles * 6) * sizeof(float); }
+
+int launch_drot_finish(const float* part, const void* rot, void* drot, const SliceGeom& g, int tiles,
+                       cudaStream_t st) {
+    const int64_t total = (int64_t)g.n * 9;
+    drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rot, drot, g, tiles);
+    return check_launch("drot_finish_kernel");
+}
 
 // Fixed-point volume gradient of the deterministic mode: 256-byte header
 // (absmax word) + 2 words per voxel, ahead of the rotation partials.

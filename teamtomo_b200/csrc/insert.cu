@@ -133,18 +133,6 @@ __global__ void mirror_x0_kernel(typename Acc<R>::C* __restrict__ vol, R* __rest
 // splat's own float32 weights, conjugated where the point was redirected.
 // One thread per slice pixel; every pixel is written (zero when dropped).
 template <typename R>
-__device__ __forceinline__ typename Acc<R>::C completed_grad(const typename Acc<R>::C* __restrict__ gvol,
-                                                            const SliceGeom& g, int z, int y, int x) {
-    typename Acc<R>::C a = gvol[vox_index(g, z, y, x)];
-    if (x == 0 && !(z == g.D / 2 && y == g.H / 2)) {
-        const typename Acc<R>::C b = gvol[vox_index(g, (g.D - z) % g.D, (g.H - y) % g.H, 0)];
-        a.x += b.x;
-        a.y -= b.y;
-    }
-    return a;
-}
-
-template <typename R>
 __global__ void __launch_bounds__(kTileThreads)
 insert_bwd_kernel(const typename Acc<R>::C* __restrict__ gvol, const void* __restrict__ rot,
                   typename Acc<R>::C* __restrict__ gimg, SliceGeom g, int tiles) {

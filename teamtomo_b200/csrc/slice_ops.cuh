@@ -271,6 +271,20 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
     }
 }
 
+// dL/dacc at voxel (z, y, x) for upstream dL/dvolume G: the adjoint of the
+// Friedel completion, G[v] + conj(G[m v]) on the x = 0 plane unless v is DC.
+template <typename R>
+__device__ __forceinline__ typename Acc<R>::C completed_grad(const typename Acc<R>::C* __restrict__ gvol,
+                                                            const SliceGeom& g, int z, int y, int x) {
+    typename Acc<R>::C a = gvol[vox_index(g, z, y, x)];
+    if (x == 0 && !(z == g.D / 2 && y == g.H / 2)) {
+        const typename Acc<R>::C b = gvol[vox_index(g, (g.D - z) % g.D, (g.H - y) % g.H, 0)];
+        a.x += b.x;
+        a.y -= b.y;
+    }
+    return a;
+}
+
 // Splat into the float (re, im, w, 0) accumulator.
 template <typename R>
 __device__ __forceinline__ void insert_point(const typename Acc<R>::C* __restrict__ img, const float* m,

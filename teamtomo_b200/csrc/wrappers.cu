@@ -105,16 +105,18 @@ __global__ void normalize_unshift_kernel(const typename C2<R>::A* __restrict__ a
     const int64_t i = r / (h * w), j = (r / w) % h, k = r % w;
     const int64_t z = wrap(i + d / 2, d), y = wrap(j + h / 2, h);  // source (shifted) voxel
     const int64_t src = (z * h + y) * w + k;
+    // the interpolation weights live in channel 0 (the channels share them)
     const typename C2<R>::A a = acc[ch * per + src];
-    R re = a.x, im = a.y, wt = a.z;
+    R re = a.x, im = a.y, wt = acc[src].z;
     if (k == 0) {
         const int64_t zm = (d - z) % d, ym = (h - y) % h;
         const bool m_dc = (zm == d / 2) && (ym == h / 2);
         if (!m_dc) {
-            const typename C2<R>::A u = acc[ch * per + (zm * h + ym) * w];
+            const int64_t msrc = (zm * h + ym) * w;
+            const typename C2<R>::A u = acc[ch * per + msrc];
             re += u.x;
             im -= u.y;
-            wt += u.z;
+            wt += acc[msrc].z;
         }
     }
     const R den = wt < (R)1 ? (R)1 : wt;

@@ -21,7 +21,12 @@ import torch
 from .. import _lib
 from . import _wrappers
 from ._params import rotation_arg
-from .slice_insertion import _InsertCentralSlices, insert_accumulate, new_accumulator
+from .slice_insertion import (
+    _InsertCentralSlices,
+    insert_accumulate,
+    insert_accumulate_multichannel,
+    new_accumulator,
+)
 
 
 def _pad_amount(n: int, pad_factor: float) -> int:
@@ -56,10 +61,15 @@ def _backproject(images, rotation_matrices, pad_factor, fftfreq_max, zyx_matrice
         real = torch.fft.irfftn(dft, dim=(-3, -2, -1))
         out = _wrappers.backproject_finish(real, p)
         return out if channels else out[0]
-    acc = new_accumulator(shape, spec.dtype == torch.complex128, dev, channels=c)
-    for ch in range(c):
-        insert_accumulate(spec[:, ch].contiguous(), R, shape, acc[ch], fftfreq_max, zyx_matrices,
-                          images_unshifted=True)
+    c128 = spec.dtype == torch.complex128
+    acc = new_accumulator(shape, c128, dev, channels=c)
+    if c > 1 and not c128:
+        insert_accumulate_multichannel(spec.contiguous(), R, shape, acc, fftfreq_max, zyx_matrices,
+                                       images_unshifted=True)
+    else:
+        for ch in range(c):
+            insert_accumulate(spec[:, ch].contiguous(), R, shape, acc[ch], fftfreq_max, zyx_matrices,
+                              images_unshifted=True)
     dft = _wrappers.backproject_normalize(acc)
     # irfftn without an output size, as the reference (odd boxes lose one x column)
     real = torch.fft.irfftn(dft, dim=(-3, -2, -1))

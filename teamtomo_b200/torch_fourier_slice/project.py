@@ -14,7 +14,7 @@ import torch
 
 from . import _wrappers
 from ._params import rotation_arg, slice_params
-from .slice_extraction import _ExtractCentralSlices
+from .slice_extraction import _ExtractCentralSlices, _ExtractMultichannel
 
 
 def _pad_amount(n: int, pad_factor: float) -> int:
@@ -62,10 +62,23 @@ def project_3d_to_2d_multichannel(
     fftfreq_max: float | None = None,
     zyx_matrices: bool = False,
 ) -> torch.Tensor:
-    """(c, d, d, d) -> (..., c, d, d): every channel projected with the same rotations."""
-    projections = [
-        project_3d_to_2d(volume[c], rotation_matrices, pad_factor=pad_factor,
-                         fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices)
-        for c in range(volume.shape[0])
-    ]
-    return torch.stack(projections, dim=-3)
+    """(c, d, d, d) -> (..., c, d, d): every channel projected with the same
+    rotations, one multichannel extraction for all channels."""
+    c, d, h, w = volume.shape[-4:]
+    if len({d, h, w}) != 1:
+        raise ValueError("all dimensions of volume must be equal.")
+    if pad_factor < 1.0:
+        raise ValueError("pad_factor must be >= 1.0")
+    p = _pad_amount(d, pad_factor) if pad_factor > 1.0 else 0
+    n_pad = d + 2 * p
+    shape = (n_pad, n_pad, n_pad)
+    fft_in = torch.stack([_wrappers.project_prepare(volume[ch], p) for ch in range(c)])
+    dft = torch.fft.rfftn(fft_in, dim=(-3, -2, -1)).contiguous()
+    R, stack = rotation_arg(rotation_matrices, volume.device)
+    params = slice_params(n=R.shape[0], image_shape=shape, volume=dft[0], rotation=R,
+                          fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                          rot_tolerance=1e-8, volume_unshifted=True, slices_unshifted=True)
+    slices = _ExtractMultichannel.apply(dft, R, params, (R.shape[0], c, n_pad, n_pad // 2 + 1))
+    images = torch.fft.irfftn(slices, dim=(-2, -1))
+    out = _wrappers.recentre_crop_2d(images.reshape(-1, *images.shape[-2:]), p)
+    return out.reshape(*stack, c, *out.shape[-2:])

@@ -55,6 +55,45 @@ class _ExtractCentralSlices(torch.autograd.Function):
         return dvol, drot, None, None
 
 
+class _ExtractMultichannel(torch.autograd.Function):
+    """(c, d, h, w//2+1) volumes -> (n, c, h, w//2+1) slices with one
+    geometry pass per pixel; backward: d/dvolume per channel, d/drotation
+    summed over the channels."""
+
+    @staticmethod
+    def forward(ctx, volumes, rotation_matrices, params, out_shape):
+        if not (volumes.is_contiguous() and rotation_matrices.is_contiguous()):
+            raise ValueError("extraction needs C-contiguous volume and rotation tensors")
+        dev = volumes.device
+        out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
+        L = _lib.load()
+        _lib.check(L.tt_extract_central_slices_rfft_3d_multichannel(
+            _lib.ptr(volumes), volumes.shape[0], _lib.ptr(rotation_matrices), _lib.ptr(out), params,
+            _lib.stream_of(dev)), "extract_central_slices_rfft_3d_multichannel")
+        ctx.params = params
+        ctx.save_for_backward(volumes, rotation_matrices)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        volumes, R = ctx.saved_tensors
+        want_v, want_r = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        if not (want_v or want_r):
+            return None, None, None, None
+        dev = volumes.device
+        grad = _lib.dense(grad.to(torch.complex64))
+        L = _lib.load()
+        dvol = torch.zeros_like(volumes) if want_v else None
+        drot = torch.empty_like(R) if want_r else None
+        nbytes = int(L.tt_extract_backward_workspace_bytes(ctx.params)) if want_r else 0
+        ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev) if want_r else None
+        _lib.check(L.tt_extract_central_slices_rfft_3d_multichannel_backward(
+            _lib.ptr(volumes), volumes.shape[0], _lib.ptr(R), _lib.ptr(grad), _lib.ptr(dvol), _lib.ptr(drot),
+            _lib.ptr(ws), nbytes, ctx.params, _lib.stream_of(dev)),
+            "extract_central_slices_rfft_3d_multichannel backward")
+        return dvol, drot, None, None
+
+
 def extract_backward(volume_rfft, rotation_matrices, grad, params, want_volume=True,
                      want_rotation=True):
     """Fused backward: (d/dvolume, d/drotation) for upstream slice gradient ``grad``."""
@@ -159,8 +198,23 @@ def extract_central_slices_rfft_3d_multichannel(
 ) -> torch.Tensor:  # (..., c, h, w)
     """Multichannel extraction (_extract_central_slices_rfft_3d.py:225-367):
     ``(c, d, d, d//2+1)`` -> ``(..., c, h, w//2+1)``, the same rotations for
-    every channel."""
+    every channel, each pixel's geometry computed once for all channels (the
+    deterministic mode runs the channels one by one)."""
     assert volume_rfft.ndim == 4, "Input volume_rfft must be 4D tensor."
+    if not resolve_deterministic(deterministic):
+        _lib.require_cuda(volume_rfft)
+        if volume_rfft.dtype != torch.complex64:
+            raise RuntimeError(
+                f"extract_central_slices_rfft_3d supports complex64 volumes (got {volume_rfft.dtype})")
+        vols = _lib.dense(volume_rfft)
+        R, stack = rotation_arg(rotation_matrices, vols.device)
+        h, w = int(image_shape[-2]), int(image_shape[-1])
+        c = vols.shape[0]
+        params = slice_params(n=R.shape[0], image_shape=image_shape, volume=vols[0], rotation=R,
+                              fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices, x_tolerance=x_tolerance,
+                              rot_tolerance=rot_tolerance)
+        out = _ExtractMultichannel.apply(vols, R, params, (R.shape[0], c, h, w // 2 + 1))
+        return out.reshape(*stack, c, h, w // 2 + 1)
     slices = [
         extract_central_slices_rfft_3d(volume_rfft[c], image_shape, rotation_matrices,
                                        fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,

@@ -188,6 +188,40 @@ def insert_backward(grad_volume, R, volume_shape, fftfreq_max=None, zyx_matrices
     return out
 
 
+def insert_accumulate_multichannel(images, R, volume_shape, acc, fftfreq_max=None, zyx_matrices=False,
+                                   images_unshifted=False):
+    """Add the splat of (n, c, h, w//2+1) complex64 slices into c float
+    accumulators (c, d, h, w//2+1, 4) — weights in channel 0."""
+    if not (images.is_contiguous() and R.is_contiguous() and acc.is_contiguous()):
+        raise ValueError("insertion needs C-contiguous slices, rotations and accumulator")
+    params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=None, rotation=R,
+                          fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                          slices_unshifted=images_unshifted, vol_dims=rfft_shape(volume_shape))
+    L = _lib.load()
+    _lib.check(L.tt_insert_accumulate_multichannel(_lib.ptr(images), images.shape[1], _lib.ptr(R), _lib.ptr(acc),
+                                                   params, _lib.stream_of(acc.device)),
+               "insert_central_slices_rfft_3d_multichannel")
+
+
+def insert_backward_multichannel(grad_volumes, R, volume_shape, fftfreq_max=None, zyx_matrices=False,
+                                 images_unshifted=False) -> torch.Tensor:
+    """dL/dslices (n, c, h, w//2+1) of a multichannel insertion for upstream
+    dL/dvolumes (c, d, h, w//2+1), complex64."""
+    dev = grad_volumes.device
+    grad_volumes = _lib.dense(grad_volumes)
+    c = grad_volumes.shape[0]
+    d, h, w = rfft_shape(volume_shape)
+    out = torch.empty((R.shape[0], c, h, w), dtype=torch.complex64, device=dev)
+    params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=None, rotation=R,
+                          fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
+                          slices_unshifted=images_unshifted, vol_dims=(d, h, w))
+    L = _lib.load()
+    _lib.check(L.tt_insert_central_slices_rfft_3d_multichannel_backward(
+        _lib.ptr(grad_volumes), c, _lib.ptr(R), _lib.ptr(out), params, _lib.stream_of(dev)),
+        "insert_central_slices_rfft_3d_multichannel backward")
+    return out
+
+
 class _InsertCentralSlices(torch.autograd.Function):
     """(n, c, h, w//2+1) slices -> ((c, d, h, w//2+1) volumes, weights),
     differentiable w.r.t. the slices (not the rotations, which are constants
@@ -196,10 +230,18 @@ class _InsertCentralSlices(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, images, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, unshifted=False):
-        chans = [_lib.dense(images[:, ch]) for ch in range(images.shape[1])]
+        c = images.shape[1]
         c128 = images.dtype == torch.complex128
-        volumes, weights = _splat(chans, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, c128,
-                                  images.device, unshifted)
+        if c > 1 and not c128 and not deterministic:
+            # one geometry pass per pixel for all channels
+            acc = new_accumulator(volume_shape, False, images.device, channels=c)
+            insert_accumulate_multichannel(_lib.dense(images), R, volume_shape, acc, fftfreq_max, zyx_matrices,
+                                           unshifted)
+            volumes, weights = insert_finalize(acc, False)
+        else:
+            chans = [_lib.dense(images[:, ch]) for ch in range(c)]
+            volumes, weights = _splat(chans, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, c128,
+                                      images.device, unshifted)
         ctx.mark_non_differentiable(weights)
         ctx.save_for_backward(R)
         ctx.args = (volume_shape, fftfreq_max, zyx_matrices, unshifted)
@@ -210,8 +252,11 @@ class _InsertCentralSlices(torch.autograd.Function):
         if grad_volumes is None or not ctx.needs_input_grad[0]:
             return None, None, None, None, None, None, None
         (R,) = ctx.saved_tensors
-        grads = torch.stack([insert_backward(grad_volumes[ch], R, *ctx.args)
-                             for ch in range(grad_volumes.shape[0])], dim=1)
+        c = grad_volumes.shape[0]
+        if c > 1 and grad_volumes.dtype == torch.complex64:
+            grads = insert_backward_multichannel(grad_volumes, R, *ctx.args)
+        else:
+            grads = torch.stack([insert_backward(grad_volumes[ch], R, *ctx.args) for ch in range(c)], dim=1)
         return grads, None, None, None, None, None, None
 
 
