@@ -269,6 +269,28 @@ int tt_insert_fixed_finalize(const void *accumulator, int32_t complex128, int64_
                              int64_t d, int64_t h, int64_t w_rfft, const uint32_t *absmax_bits,
                              int64_t max_slices, void *volume_rfft, void *weights, void *stream);
 
+/* ---- central lines of 2D images -----------------------------------------
+ * image_rfft: complex64 (img_h, img_w_rfft), fftshifted along h (the rfft of an
+ * (h, w) image); rotation_matrices (n, 2, 2) float32 or float64 (rotation_f64),
+ * acting on xy column vectors unless yx_matrices; lines_out complex64
+ * (n, w/2+1), fully written (zeros beyond fftfreq_max / outside the image).
+ * Replaces extract_central_slices_rfft_2d (_extract_central_slices_rfft_2d.py:9-84);
+ * the reference raises for any fftfreq_max (its mask is taken over the (w, 2)
+ * coordinate grid), here it zeroes the samples with frequency > fftfreq_max. */
+int tt_extract_central_lines_rfft_2d(const void *image_rfft, int64_t img_h, int64_t img_w_rfft,
+                                     const void *rotation_matrices, int32_t rotation_f64, int64_t n,
+                                     int64_t h, int64_t w, int32_t has_fftfreq_max, float fftfreq_max,
+                                     int32_t yx_matrices, void *lines_out, void *stream);
+/* Backward: grad_image (img_h, img_w_rfft) ACCUMULATED into (nullable),
+ * grad_rotation (n, 2, 2) in the rotation dtype, overwritten (nullable);
+ * grad_lines in PyTorch's complex-gradient convention. */
+int tt_extract_central_lines_rfft_2d_backward(const void *image_rfft, int64_t img_h, int64_t img_w_rfft,
+                                              const void *rotation_matrices, int32_t rotation_f64,
+                                              int64_t n, int64_t h, int64_t w, int32_t has_fftfreq_max,
+                                              float fftfreq_max, int32_t yx_matrices,
+                                              const void *grad_lines, void *grad_image,
+                                              void *grad_rotation, void *stream);
+
 /* ---- multichannel slices (c volumes, one set of rotations) -------------
  * Each pixel's geometry is computed once and applied to every channel.
  * Volumes (channels, vol_d, vol_h, vol_w) complex64; slices

@@ -100,12 +100,16 @@ static void to_dft_coords(const coord_scale *s, const float p[3], float c[3]) {
 }
 
 /* array coordinate -> grid_sample coordinate -> unnormalised source index,
- * clipped to [0, n-1] (padding_mode='border', align_corners=True). */
-static float roundtrip_index(float c, int64_t n) {
+ * clipped to [0, n-1] (padding_mode='border', align_corners=True).  *grad_ok:
+ * the clip passes a coordinate gradient, i.e. the unclipped index lies
+ * strictly inside (0, n-1) — on the border itself grid_sample's backward
+ * treats the point as clipped and gives that axis zero gradient. */
+static float roundtrip_index(float c, int64_t n, int *grad_ok) {
     float fn = (float)n;
     float half = 0.5f * fn - 0.5f;
     float g = c / half - 1.0f;
     float ix = ((g + 1.0f) / 2.0f) * (fn - 1.0f);
+    *grad_ok = ix > 0.0f && ix < fn - 1.0f;
     if (ix < 0.0f) ix = 0.0f;
     if (ix > fn - 1.0f) ix = fn - 1.0f;
     return ix;
@@ -124,13 +128,14 @@ typedef struct {
     /* d w / d(ix, iy, iz) for each corner */
     float gx[8], gy[8], gz[8];
     float ix, iy, iz;
+    int ok_x, ok_y, ok_z; /* the coordinate gradient passes the border clip */
 } tri_corners;
 
 static void grid_sample_corners(const float c[3], int64_t D, int64_t H, int64_t W,
                                 tri_corners *t) {
-    float iz = roundtrip_index(c[0], D);
-    float iy = roundtrip_index(c[1], H);
-    float ix = roundtrip_index(c[2], W);
+    float iz = roundtrip_index(c[0], D, &t->ok_z);
+    float iy = roundtrip_index(c[1], H, &t->ok_y);
+    float ix = roundtrip_index(c[2], W, &t->ok_x);
     float x0 = floorf(ix), y0 = floorf(iy), z0 = floorf(iz);
     float x1 = x0 + 1.0f, y1 = y0 + 1.0f, z1 = z0 + 1.0f;
     float ax0 = x1 - ix, ax1 = ix - x0;
@@ -296,10 +301,11 @@ int orc_extract_grad(const float *vol, int64_t D, int64_t H, int64_t W, const fl
                     }
                 }
                 if (drot) {
-                    /* the clip of padding_mode='border' passes no gradient at a
-                     * clipped coordinate; inside points are never clipped */
+                    /* the clip of padding_mode='border' passes no gradient along an
+                     * axis whose source index lies on the border (0 or n-1) */
                     double sg = cj ? -1.0 : 1.0;
-                    double dp[3] = {dz * dcdp[0] * sg, dy * dcdp[1] * sg, dx * dcdp[2] * sg};
+                    double dp[3] = {dz * dcdp[0] * sg * t.ok_z, dy * dcdp[1] * sg * t.ok_y,
+                                    dx * dcdp[2] * sg * t.ok_x};
                     for (int i = 0; i < 3; i++)
                         for (int j = 0; j < 3; j++) acc[i * 3 + j] += dp[i] * (double)q[j];
                 }

@@ -321,6 +321,84 @@ def insert_grad_images(grad_volume, volume_shape, rotation_matrices, fftfreq_max
 
 
 # ----------------------------------------------------------------------------
+# central lines of 2D images (numpy, float32 arithmetic)
+# ----------------------------------------------------------------------------
+
+def _source_index_np(c, n):
+    """grid_sample's array -> grid -> array round trip (align_corners, border clip)."""
+    f32 = np.float32
+    half = f32(0.5) * f32(n) - f32(0.5)
+    g = (c / half).astype(f32) - f32(1)
+    ix = ((g + f32(1)) * f32(0.5)).astype(f32) * f32(n - 1)
+    return np.clip(ix.astype(f32), f32(0), f32(n - 1))
+
+
+def extract_lines_2d(image_rfft, image_shape, rotation_matrices, fftfreq_max=None, yx_matrices=False):
+    """Restatement of extract_central_slices_rfft_2d
+    (_extract_central_slices_rfft_2d.py:9-84): central lines (..., w//2+1) of
+    an fftshifted (h, w//2+1) rfft, bilinear grid_sample sampling, strict
+    x' < 0 redirect; samples with frequency > fftfreq_max are zero."""
+    f32 = np.float32
+    img = np.asarray(image_rfft).astype(np.complex64)
+    H, W = img.shape
+    h, w = (int(x) for x in image_shape)
+    R = np.asarray(rotation_matrices)
+    stack = R.shape[:-2]
+    r = R.astype(f32).reshape(-1, 2, 2)
+    if not yx_matrices:
+        r = r[:, ::-1, ::-1]
+    wr = w // 2 + 1
+    qx = np.arange(wr, dtype=f32) * f32(1.0 / w)
+    py = (r[:, 0, 1][:, None] * qx[None, :]).astype(f32)
+    px = (r[:, 1, 1][:, None] * qx[None, :]).astype(f32)
+    cj = px < 0
+    py = np.where(cj, -py, py)
+    px = np.where(cj, -px, px)
+    iw0 = f32(1) - f32(1.0) / f32(h)
+    cy = (((py + f32(0.5)).astype(f32) / iw0).astype(f32) * f32(h - 1)).astype(f32)
+    cx = ((px * f32(2)).astype(f32) * f32(wr - 1)).astype(f32)
+    inside = (cy >= 0) & (cy <= H - 1) & (cx >= 0) & (cx <= W - 1)
+    if fftfreq_max is not None:
+        inside &= (qx <= f32(fftfreq_max))[None, :]
+    iy = _source_index_np(cy, H)
+    ix = _source_index_np(cx, W)
+    y0 = np.floor(iy).astype(np.int64)
+    x0 = np.floor(ix).astype(np.int64)
+    ay1 = (iy - y0).astype(np.float64)
+    ax1 = (ix - x0).astype(np.float64)
+    out = np.zeros(py.shape, np.complex128)
+    for by in (0, 1):
+        for bx in (0, 1):
+            yy, xx = y0 + by, x0 + bx
+            ok = inside & (yy < H) & (xx < W)
+            wgt = (ay1 if by else 1 - ay1) * (ax1 if bx else 1 - ax1)
+            out += np.where(ok, wgt * img[np.clip(yy, 0, H - 1), np.clip(xx, 0, W - 1)], 0)
+    out = np.where(cj, np.conj(out), out)
+    out = np.where(inside, out, 0)
+    return out.astype(np.complex64).reshape(*stack, wr)
+
+
+def project_2d_to_1d(image, rotation_matrices, pad_factor=2.0, fftfreq_max=None, yx_matrices=False):
+    """Restatement of torch_fourier_slice.project_2d_to_1d (project.py): pad,
+    premultiply by sinc^2, 2D rfft, central lines, 1D irfft without an output
+    size, recentre, unpad."""
+    img = np.asarray(image, np.float64)
+    d = img.shape[-1]
+    p = int((d * (pad_factor - 1.0)) // 2) if pad_factor > 1.0 else 0
+    if p:
+        img = np.pad(img, p)
+    n = img.shape[-1]
+    f = np.fft.fftshift(np.fft.fftfreq(n))
+    img = img * np.sinc(np.sqrt(f[:, None] ** 2 + f[None, :] ** 2)) ** 2
+    dft = np.fft.fftshift(np.fft.rfftn(np.fft.fftshift(img)), axes=(0,))
+    lines = extract_lines_2d(dft, (n, n), rotation_matrices, fftfreq_max=fftfreq_max, yx_matrices=yx_matrices)
+    proj = np.fft.ifftshift(np.fft.irfft(lines.astype(np.complex128), axis=-1), axes=-1)
+    if p:
+        proj = proj[..., p:-p]
+    return proj.astype(np.float32)
+
+
+# ----------------------------------------------------------------------------
 # deterministic insertion: 64-bit fixed point (numpy, bit-exact restatement of
 # the CUDA fixed-point mode; the reference has no such mode, so it is pinned
 # through its float outputs)

@@ -9,10 +9,12 @@ from . import distributed, losses, streaming, torch_fourier_slice, torch_image_i
 from .torch_fourier_slice import (
     backproject_2d_to_3d,
     backproject_2d_to_3d_multichannel,
+    extract_central_slices_rfft_2d,
     extract_central_slices_rfft_3d,
     extract_central_slices_rfft_3d_multichannel,
     insert_central_slices_rfft_3d,
     insert_central_slices_rfft_3d_multichannel,
+    project_2d_to_1d,
     project_3d_to_2d,
     project_3d_to_2d_multichannel,
 )
@@ -28,10 +30,12 @@ __all__ = [
     "torch_image_interpolation",
     "backproject_2d_to_3d",
     "backproject_2d_to_3d_multichannel",
+    "extract_central_slices_rfft_2d",
     "extract_central_slices_rfft_3d",
     "extract_central_slices_rfft_3d_multichannel",
     "insert_central_slices_rfft_3d",
     "insert_central_slices_rfft_3d_multichannel",
+    "project_2d_to_1d",
     "project_3d_to_2d",
     "project_3d_to_2d_multichannel",
     "sample_image_3d",

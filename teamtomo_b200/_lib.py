@@ -90,6 +90,10 @@ SIGNATURES = {
     "tt_insert_accumulate_multichannel": ([_vp, _i64, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_central_slices_rfft_3d_multichannel_backward": (
         [_vp, _i64, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_extract_central_lines_rfft_2d": ([_vp, _i64, _i64, _vp, _i32, _i64, _i64, _i64, _i32, _f32, _i32, _vp, _vp],
+                                         _i32),
+    "tt_extract_central_lines_rfft_2d_backward": (
+        [_vp, _i64, _i64, _vp, _i32, _i64, _i64, _i64, _i32, _f32, _i32, _vp, _vp, _vp, _vp], _i32),
     "tt_batch_workspace_bytes": ([], _sz),
     "tt_extract_central_slices_rfft_3d_batched": (
         [ctypes.POINTER(BatchVolume), _i32, _i32, _vp, _sz, _vp], _i32),

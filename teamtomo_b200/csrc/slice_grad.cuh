@@ -90,9 +90,10 @@ __device__ __forceinline__ void drot_terms(const float2 v[2][2][2], const Corner
             gx.y = fmaf(wzy, v[a][b][1].y - v[a][b][0].y, gx.y);
         }
     const float sg = cj ? -1.f : 1.f;
-    const float p0 = fmaf(gv.x, gz.x, gv.y * gz.y) * g.dcdp0 * sg;
-    const float p1 = fmaf(gv.x, gy.x, gv.y * gy.y) * g.dcdp1 * sg;
-    const float p2 = fmaf(gv.x, gx.x, gv.y * gx.y) * g.dcdp2 * sg;
+    // an axis whose source index is on the border gets no gradient (grid_sample's clip)
+    const float p0 = k.gz ? fmaf(gv.x, gz.x, gv.y * gz.y) * g.dcdp0 * sg : 0.0f;
+    const float p1 = k.gy ? fmaf(gv.x, gy.x, gv.y * gy.y) * g.dcdp1 * sg : 0.0f;
+    const float p2 = k.gx ? fmaf(gv.x, gx.x, gv.y * gx.y) * g.dcdp2 * sg : 0.0f;
     acc[0] = p0 * qy;
     acc[1] = p0 * qx;
     acc[2] = p1 * qy;

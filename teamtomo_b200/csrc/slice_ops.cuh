@@ -13,9 +13,12 @@ namespace tt {
 // grid_sample's source index of array coordinate c on an axis of n samples:
 // c -> grid coordinate c / (0.5 n - 0.5) - 1 (grid_sample_utils.py:6-26) ->
 // ((g + 1) / 2) * (n - 1) (align_corners=True), clipped to [0, n-1].
-__device__ __forceinline__ float source_index(float c, float half, float nm1) {
+// grad_ok: the border clip passes a coordinate gradient — grid_sample's
+// backward treats an index on the border itself (0 or n-1) as clipped.
+__device__ __forceinline__ float source_index(float c, float half, float nm1, bool& grad_ok) {
     const float gc = __fsub_rn(__fdiv_rn(c, half), 1.0f);
     const float ix = __fmul_rn(__fmul_rn(__fadd_rn(gc, 1.0f), 0.5f), nm1);
+    grad_ok = ix > 0.0f && ix < nm1;
     return fminf(fmaxf(ix, 0.0f), nm1);
 }
 
@@ -23,15 +26,16 @@ struct Corners {
     int z0, y0, x0;
     float ax0, ax1, ay0, ay1, az0, az1;  // per-axis weights of the low/high corner
     bool zin, yin, xin;                  // high corner inside the array
+    bool gz, gy, gx;                     // the axis passes a coordinate gradient (not on the border)
 };
 
 // grid_sample trilinear corner set of an inside array coordinate c (the
 // round trip decides the cell at integer kinks, where the derivative jumps).
 __device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float c[3]) {
-    const float iz = source_index(c[0], 0.5f * (float)g.D - 0.5f, g.ub0);
-    const float iy = source_index(c[1], 0.5f * (float)g.H - 0.5f, g.ub1);
-    const float ix = source_index(c[2], 0.5f * (float)g.W - 0.5f, g.ub2);
     Corners k;
+    const float iz = source_index(c[0], 0.5f * (float)g.D - 0.5f, g.ub0, k.gz);
+    const float iy = source_index(c[1], 0.5f * (float)g.H - 0.5f, g.ub1, k.gy);
+    const float ix = source_index(c[2], 0.5f * (float)g.W - 0.5f, g.ub2, k.gx);
     const float fz = floorf(iz), fy = floorf(iy), fx = floorf(ix);
     k.z0 = (int)fz;
     k.y0 = (int)fy;

@@ -23,6 +23,7 @@ Cases (reference test each one mirrors):
   ctf_*          torch-ctf calculate_ctf_2d grids
   insgrad_*      reference autograd of insert_central_slices_rfft_3d w.r.t. the images
   bpgrad_*       reference autograd of backproject_2d_to_3d w.r.t. the images
+  lines_*, linesgrad_*, proj1d_*   extract_central_slices_rfft_2d (+ its autograd), project_2d_to_1d
 """
 
 from __future__ import annotations
@@ -273,6 +274,43 @@ def main():
         g[f"bpgrad_{name}_images"], g[f"bpgrad_{name}_rot"] = imgs.detach().numpy(), rots
         g[f"bpgrad_{name}_G"], g[f"bpgrad_{name}_pad"] = G.numpy(), np.array(pf)
         g[f"bpgrad_{name}_out"] = imgs.grad.numpy()
+
+    # ---------------- d/drotation at axis-aligned rotations (points on the border) ----------------
+    n = 16
+    vol = rfft_volume(blob_volume(n, 31))
+    rots = special_rotations()
+    G = torch.randn(len(rots), n, n // 2 + 1, dtype=torch.complex64, generator=torch.Generator().manual_seed(31))
+    R = torch.tensor(rots, requires_grad=True)
+    (extract_central_slices_rfft_3d(vol, (n, n, n), R) * G.conj()).real.sum().backward()
+    g["grad_axes_volume"], g["grad_axes_rot"], g["grad_axes_G"] = vol.numpy(), rots, G.numpy()
+    g["grad_axes_out"] = R.grad.numpy()
+
+    # ---------------- central lines of 2D images ----------------
+    from torch_fourier_slice import extract_central_slices_rfft_2d, project_2d_to_1d
+
+    gen = torch.Generator().manual_seed(29)
+    th = torch.tensor(np.concatenate([np.linspace(0, 2 * np.pi, 13, endpoint=False), [np.pi / 2, np.pi]]))
+    rot2 = torch.stack([torch.stack([torch.cos(th), -torch.sin(th)], -1),
+                        torch.stack([torch.sin(th), torch.cos(th)], -1)], -2)  # (15, 2, 2) float64
+    names = []
+    for h, yx in ((16, False), (17, False), (16, True)):
+        img = torch.randn(h, h // 2 + 1, dtype=torch.complex64, generator=gen)
+        name = f"h{h}" + ("_yx" if yx else "")
+        g[f"lines_{name}_image"], g[f"lines_{name}_rot"] = img.numpy(), rot2.numpy()
+        g[f"lines_{name}_yx"] = np.array(int(yx))
+        g[f"lines_{name}_out"] = extract_central_slices_rfft_2d(img, (h, h), rot2, yx_matrices=yx).numpy()
+        names.append(name)
+    g["lines_cases"] = np.array(names)
+    R = rot2.clone().requires_grad_(True)
+    img = torch.randn(16, 9, dtype=torch.complex64, generator=gen).requires_grad_(True)
+    G = torch.randn(15, 9, dtype=torch.complex64, generator=gen)
+    (extract_central_slices_rfft_2d(img, (16, 16), R) * G.conj()).real.sum().backward()
+    g["linesgrad_image"], g["linesgrad_G"] = img.detach().numpy(), G.numpy()
+    g["linesgrad_drot"], g["linesgrad_dimage"] = R.grad.numpy(), img.grad.numpy()
+    for name, d, pf in (("even", 32, 2.0), ("odd", 17, 1.5)):
+        im = torch.randn(d, d, generator=gen)
+        g[f"proj1d_{name}_image"], g[f"proj1d_{name}_pad"] = im.numpy(), np.array(pf)
+        g[f"proj1d_{name}_out"] = project_2d_to_1d(im, rot2.float(), pad_factor=pf).numpy()
 
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {os.path.getsize(OUT) / 1e6:.2f} MB, {len(g)} arrays")

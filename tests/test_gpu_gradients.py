@@ -186,3 +186,18 @@ def test_gradient_through_lazy_conjugate():
     out = tt().extract_central_slices_rfft_3d(vol.conj(), (n, n, n), rots)
     ref = tt().extract_central_slices_rfft_3d(vol.conj().resolve_conj(), (n, n, n), rots)
     assert torch.equal(out, ref)
+
+
+def test_grad_rotation_on_the_border_matches_reference_autograd(golden):
+    vol = cuda(golden["grad_axes_volume"])
+    n = vol.shape[0]
+    R = cuda(golden["grad_axes_rot"]).requires_grad_(True)
+    _loss(tt().extract_central_slices_rfft_3d(vol, (n, n, n), R), cuda(golden["grad_axes_G"])).backward()
+    assert rel_l2(R.grad.cpu().numpy(), golden["grad_axes_out"]) < RTOL
+    # the fused MSE kernel shares the rule
+    T = torch.zeros((R.shape[0], n, n // 2 + 1), dtype=torch.complex64, device="cuda")
+    R2 = cuda(golden["grad_axes_rot"]).requires_grad_(True)
+    R3 = cuda(golden["grad_axes_rot"]).requires_grad_(True)
+    tt().losses.central_slice_mse(vol, (n, n, n), R2, T).backward()
+    (tt().extract_central_slices_rfft_3d(vol, (n, n, n), R3) - T).abs().square().mean().backward()
+    assert rel_l2(R2.grad.cpu().numpy(), R3.grad.cpu().numpy()) < RTOL

@@ -176,3 +176,30 @@ def test_insert_image_gradient_matches_reference_autograd(golden, oracle):
         tol = 1e-12 if imgs.dtype == np.complex128 else 1e-6
         assert rel_l2(out, ref) < tol, name
         assert np.array_equal(out == 0, ref == 0), name  # same pixels receive no gradient
+
+
+def test_lines_2d_match_reference(golden, oracle):
+    for name in golden["lines_cases"]:
+        name = str(name)
+        img = golden[f"lines_{name}_image"]
+        h = img.shape[0]
+        out = oracle.extract_lines_2d(img, (h, h), golden[f"lines_{name}_rot"],
+                                      yx_matrices=bool(int(golden[f"lines_{name}_yx"])))
+        ref = golden[f"lines_{name}_out"]
+        assert out.shape == ref.shape
+        assert rel_l2(out, ref) < 1e-6, name
+    for name in ("even", "odd"):
+        im = golden[f"proj1d_{name}_image"]
+        out = oracle.project_2d_to_1d(im, golden["lines_h16_rot"], pad_factor=float(golden[f"proj1d_{name}_pad"]))
+        ref = golden[f"proj1d_{name}_out"]
+        assert out.shape == ref.shape, name
+        assert rel_l2(out, ref) < 1e-5, name
+
+
+def test_rotation_gradient_on_the_border_matches_reference(golden, oracle):
+    """Axis-aligned rotations put whole pixel columns on the x = 0 border,
+    where grid_sample's backward passes no coordinate gradient."""
+    vol = golden["grad_axes_volume"]
+    n = vol.shape[0]
+    _, drot = oracle.extract_grad(vol, (n, n, n), golden["grad_axes_rot"], golden["grad_axes_G"], want_dvol=False)
+    assert rel_l2(drot, golden["grad_axes_out"]) < 1e-5
