@@ -374,6 +374,18 @@ int tt_insert_into_image_3d(const void *values, int32_t dtype, const float *coor
                             void *image, int64_t channels, int64_t d, int64_t h, int64_t w,
                             void *weights, int32_t weights_f64, int32_t nearest, void *stream);
 
+/* Affine resampling: out (n_matrices, od, oh, ow, channels) of the image's
+ * dtype = image sampled at M (z, y, x, 1) for every output voxel (z, y, x),
+ * matrices_zyx (n_matrices, 4, 4) float32 already in zyx order; coordinates in
+ * float32 with the reference's operation order, then trilinear / nearest as
+ * tt_sample_image_3d.  Replaces affine_transform_image_3d
+ * (torch_transform_image/transforms_3d.py:10-40: coordinate_grid, matmul,
+ * sample_image_3d) without materialising the coordinate grid. */
+int tt_affine_transform_image_3d(const void *image, int32_t dtype, int64_t channels, int64_t d,
+                                 int64_t h, int64_t w, const float *matrices_zyx, int64_t n_matrices,
+                                 int64_t od, int64_t oh, int64_t ow, int32_t nearest, void *out,
+                                 void *stream);
+
 /* ---- elementwise passes around the FFTs of the real-space wrappers ------
  * is_f64 selects float64 (else float32) real data; complex128 likewise. */
 

@@ -320,6 +320,35 @@ def insert_grad_images(grad_volume, volume_shape, rotation_matrices, fftfreq_max
     return out
 
 
+def affine_transform_image_3d(image, matrices, interpolation, output_shape=None, zyx_matrices=False):
+    """Restatement of torch_transform_image.affine_transform_image_3d
+    (transforms_3d.py:10-40): float32 homogeneous coordinates M (z, y, x, 1)
+    with each product rounded and the sums taken left to right, then
+    sample_image_3d."""
+    f32 = np.float32
+    img = np.asarray(image)
+    d, h, w = (int(s) for s in (output_shape if output_shape else img.shape[-3:]))
+    M = np.array(matrices, dtype=f32, copy=True)
+    if not zyx_matrices:
+        M[..., :3, :3] = M[..., :3, :3][..., ::-1, ::-1]
+        M[..., :3, 3] = M[..., :3, 3][..., ::-1]
+    z, y, x = (a.astype(f32) for a in np.indices((d, h, w)))
+    cols = (z, y, x, np.ones_like(z))
+    stack = M.shape[:-2]
+    Mf = M.reshape(-1, 4, 4)
+    outs = []
+    for m in Mf:
+        c = np.zeros((d, h, w, 3), f32)
+        for i in range(3):
+            acc = (m[i, 0] * cols[0]).astype(f32)
+            for j in (1, 2, 3):
+                acc = (acc + (m[i, j] * cols[j]).astype(f32)).astype(f32)
+            c[..., i] = acc
+        real = np.float64 if img.dtype in (np.float64, np.complex128) else f32
+        outs.append(sample_image_3d(img, c.astype(real), interpolation))
+    return np.stack(outs).reshape(*stack, *outs[0].shape)
+
+
 # ----------------------------------------------------------------------------
 # central lines of 2D images (numpy, float32 arithmetic)
 # ----------------------------------------------------------------------------

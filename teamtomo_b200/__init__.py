@@ -5,7 +5,14 @@ the 3D interpolation API of torch-image-interpolation, running on
 hand-written sm_100a CUDA kernels through the C ABI in include/teamtomo_b200.h.
 """
 
-from . import distributed, losses, streaming, torch_fourier_slice, torch_image_interpolation
+from . import (
+    distributed,
+    losses,
+    streaming,
+    torch_fourier_slice,
+    torch_image_interpolation,
+    torch_transform_image,
+)
 from .torch_fourier_slice import (
     backproject_2d_to_3d,
     backproject_2d_to_3d_multichannel,
@@ -28,6 +35,7 @@ __all__ = [
     "streaming",
     "torch_fourier_slice",
     "torch_image_interpolation",
+    "torch_transform_image",
     "backproject_2d_to_3d",
     "backproject_2d_to_3d_multichannel",
     "extract_central_slices_rfft_2d",

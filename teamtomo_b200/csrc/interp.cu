@@ -22,13 +22,10 @@ __device__ __forceinline__ void atomic_add_real(T* p, T v) {
     atomicAdd(p, v);
 }
 
+// One sample of the (C, D, H, W) image at (cz, cy, cx) into o[0 .. C*E).
 template <typename T, int E>
-__global__ void sample3d_kernel(const T* __restrict__ img, int64_t C, int D, int H, int W,
-                                const T* __restrict__ coords, int64_t n, T* __restrict__ out, int nearest) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const T cz = coords[i * 3 + 0], cy = coords[i * 3 + 1], cx = coords[i * 3 + 2];
-    T* o = out + i * C * E;
+__device__ __forceinline__ void sample_point(const T* __restrict__ img, int64_t C, int D, int H, int W, T cz, T cy,
+                                             T cx, T* __restrict__ o, int nearest) {
     const bool inside = cz >= (T)0 && cz <= (T)(D - 1) && cy >= (T)0 && cy <= (T)(H - 1) && cx >= (T)0 &&
                         cx <= (T)(W - 1);
     const int64_t plane = (int64_t)D * H * W;
@@ -66,6 +63,39 @@ __global__ void sample3d_kernel(const T* __restrict__ img, int64_t C, int D, int
 #pragma unroll
         for (int e = 0; e < E; e++) o[ch * E + e] = acc[e];
     }
+}
+
+template <typename T, int E>
+__global__ void sample3d_kernel(const T* __restrict__ img, int64_t C, int D, int H, int W,
+                                const T* __restrict__ coords, int64_t n, T* __restrict__ out, int nearest) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    sample_point<T, E>(img, C, D, H, W, coords[i * 3 + 0], coords[i * 3 + 1], coords[i * 3 + 2], out + i * C * E,
+                       nearest);
+}
+
+// affine_transform_image_3d (torch_transform_image/transforms_3d.py:10-40):
+// output voxel (z, y, x) of matrix m samples the image at M_m (z, y, x, 1),
+// M in zyx order, computed in float32 with the reference's operation order
+// (((m0 z + m1 y) + m2 x) + m3 1, each product rounded) so that nearest
+// sampling picks the same voxels.  One thread per (matrix, output voxel).
+template <typename T, int E>
+__global__ void affine3d_kernel(const T* __restrict__ img, int64_t C, int D, int H, int W,
+                                const float* __restrict__ mats, int64_t nm, int od, int oh, int ow,
+                                T* __restrict__ out, int nearest) {
+    const int64_t vox = (int64_t)od * oh * ow;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nm * vox) return;
+    const int64_t mi = idx / vox, r = idx - mi * vox;
+    const float z = (float)(r / ((int64_t)oh * ow)), y = (float)((r / ow) % oh), x = (float)(r % ow);
+    const float* M = mats + mi * 16;
+    float c[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+        c[i] = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(M[i * 4 + 0], z), __fmul_rn(M[i * 4 + 1], y)),
+                                   __fmul_rn(M[i * 4 + 2], x)),
+                         __fmul_rn(M[i * 4 + 3], 1.0f));
+    sample_point<T, E>(img, C, D, H, W, (T)c[0], (T)c[1], (T)c[2], out + idx * C * E, nearest);
 }
 
 template <typename T, int E, typename WT>
@@ -168,4 +198,39 @@ extern "C" int tt_insert_into_image_3d(const void* values, int32_t dtype, const 
     }
 #undef TT_INSERT_CASE
     return check_launch("insert3d_kernel");
+}
+
+extern "C" int tt_affine_transform_image_3d(const void* image, int32_t dtype, int64_t channels, int64_t d, int64_t h,
+                                            int64_t w, const float* matrices_zyx, int64_t n_matrices, int64_t od,
+                                            int64_t oh, int64_t ow, int32_t nearest, void* out, void* stream) {
+    if (n_matrices == 0 || od * oh * ow == 0) return TT_OK;
+    if (!image || !matrices_zyx || !out || channels < 1 || d < 1 || h < 1 || w < 1 || n_matrices < 0 || od < 0 ||
+        oh < 0 || ow < 0)
+        return fail(TT_ERR_INVALID, "affine_transform_image_3d: bad arguments");
+    if (dtype < 0 || dtype > 3) return fail(TT_ERR_INVALID, "affine_transform_image_3d: dtype must be 0-3");
+    const int64_t total = n_matrices * od * oh * ow;
+    const unsigned b = nblocks(total, 256);
+    cudaStream_t st = as_stream(stream);
+    switch (dtype) {
+        case 0:
+            affine3d_kernel<float, 1><<<b, 256, 0, st>>>((const float*)image, channels, (int)d, (int)h, (int)w,
+                                                         matrices_zyx, n_matrices, (int)od, (int)oh, (int)ow,
+                                                         (float*)out, nearest);
+            break;
+        case 1:
+            affine3d_kernel<double, 1><<<b, 256, 0, st>>>((const double*)image, channels, (int)d, (int)h, (int)w,
+                                                          matrices_zyx, n_matrices, (int)od, (int)oh, (int)ow,
+                                                          (double*)out, nearest);
+            break;
+        case 2:
+            affine3d_kernel<float, 2><<<b, 256, 0, st>>>((const float*)image, channels, (int)d, (int)h, (int)w,
+                                                         matrices_zyx, n_matrices, (int)od, (int)oh, (int)ow,
+                                                         (float*)out, nearest);
+            break;
+        default:
+            affine3d_kernel<double, 2><<<b, 256, 0, st>>>((const double*)image, channels, (int)d, (int)h, (int)w,
+                                                          matrices_zyx, n_matrices, (int)od, (int)oh, (int)ow,
+                                                          (double*)out, nearest);
+    }
+    return check_launch("affine3d_kernel");
 }

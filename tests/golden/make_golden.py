@@ -24,6 +24,7 @@ Cases (reference test each one mirrors):
   insgrad_*      reference autograd of insert_central_slices_rfft_3d w.r.t. the images
   bpgrad_*       reference autograd of backproject_2d_to_3d w.r.t. the images
   lines_*, linesgrad_*, proj1d_*   extract_central_slices_rfft_2d (+ its autograd), project_2d_to_1d
+  affine_*       torch_transform_image.affine_transform_image_3d
 """
 
 from __future__ import annotations
@@ -311,6 +312,29 @@ def main():
         im = torch.randn(d, d, generator=gen)
         g[f"proj1d_{name}_image"], g[f"proj1d_{name}_pad"] = im.numpy(), np.array(pf)
         g[f"proj1d_{name}_out"] = project_2d_to_1d(im, rot2.float(), pad_factor=pf).numpy()
+
+    # ---------------- affine_transform_image_3d (torch-transform-image) ----------------
+    for pkg in ("torch-transform-image", "torch-affine-utils"):
+        sys.path.insert(0, os.path.join(REF, "packages", "primitives", pkg, "src"))
+    from torch_transform_image import affine_transform_image_3d
+
+    gen = torch.Generator().manual_seed(37)
+    rot = torch.tensor(special_ortho_group.rvs(3, size=3, random_state=37), dtype=torch.float32)
+    M = torch.eye(4).repeat(3, 1, 1)
+    M[:, :3, :3] = rot
+    M[:, :3, 3] = torch.tensor([[1.5, -2.0, 0.25], [0.0, 3.0, -1.0], [2.0, 2.0, 2.0]])
+    for name, img in (("real", torch.randn(9, 10, 11, generator=gen)),
+                      ("complex", torch.randn(9, 10, 11, dtype=torch.complex64, generator=gen)),
+                      ("multi", torch.randn(2, 9, 10, 11, generator=gen))):
+        g[f"affine_{name}_image"] = img.numpy()
+        for mode in ("trilinear", "nearest"):  # the reference takes one (4, 4) matrix per call
+            g[f"affine_{name}_{mode}_out"] = np.stack(
+                [affine_transform_image_3d(img, M[i], interpolation=mode).numpy() for i in range(3)])
+    g["affine_matrices"] = M.numpy()
+    g["affine_shape_zyx_out"] = affine_transform_image_3d(g_img := torch.randn(8, 8, 8, generator=gen), M[0],
+                                                          interpolation="trilinear", output_shape=(6, 7, 5),
+                                                          zyx_matrices=True).numpy()
+    g["affine_shape_zyx_image"] = g_img.numpy()
 
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {os.path.getsize(OUT) / 1e6:.2f} MB, {len(g)} arrays")

@@ -203,3 +203,20 @@ def test_rotation_gradient_on_the_border_matches_reference(golden, oracle):
     n = vol.shape[0]
     _, drot = oracle.extract_grad(vol, (n, n, n), golden["grad_axes_rot"], golden["grad_axes_G"], want_dvol=False)
     assert rel_l2(drot, golden["grad_axes_out"]) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["real", "complex", "multi"])
+@pytest.mark.parametrize("mode", ["trilinear", "nearest"])
+def test_affine_transform_matches_reference(golden, oracle, name, mode):
+    out = oracle.affine_transform_image_3d(golden[f"affine_{name}_image"], golden["affine_matrices"], mode)
+    ref = golden[f"affine_{name}_{mode}_out"]
+    assert out.shape == ref.shape
+    assert rel_l2(out, ref) < 1e-6
+    if mode == "nearest":
+        assert np.array_equal(out, ref)
+
+
+def test_affine_transform_output_shape_zyx(golden, oracle):
+    out = oracle.affine_transform_image_3d(golden["affine_shape_zyx_image"], golden["affine_matrices"][0],
+                                           "trilinear", output_shape=(6, 7, 5), zyx_matrices=True)
+    assert rel_l2(out, golden["affine_shape_zyx_out"]) < 1e-6
