@@ -365,6 +365,17 @@ int tt_sample_image_3d(const void *image, int32_t dtype, int64_t channels, int64
                        int64_t w, const void *coordinates, int64_t n, void *out, int32_t nearest,
                        void *stream);
 
+/* Backward of tt_sample_image_3d for upstream grad_out (n, channels):
+ * grad_image (channels, d, h, w) ACCUMULATED into (nullable), grad_coordinates
+ * (n, 3) overwritten (nullable), in PyTorch's complex-gradient convention;
+ * coordinate gradients follow grid_sample's backward (zero on the border of
+ * an axis and outside; none for nearest).  Replaces the autograd graph of
+ * sample_image_3d (grid_sample backward). */
+int tt_sample_image_3d_backward(const void *image, int32_t dtype, int64_t channels, int64_t d,
+                                int64_t h, int64_t w, const void *coordinates, int64_t n,
+                                const void *grad_out, void *grad_image, void *grad_coordinates,
+                                int32_t nearest, void *stream);
+
 /* Splats values (n, channels) at float32 coordinates (n, 3) into image and
  * weights (d, h, w; float32, or float64 when weights_f64), ACCUMULATED into:
  * trilinear (floor/ceil corners, float32 weights) or nearest (rint, weight 1);

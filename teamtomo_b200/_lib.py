@@ -100,6 +100,7 @@ SIGNATURES = {
     "tt_insert_central_slices_rfft_3d_batched": (
         [ctypes.POINTER(BatchVolume), _i32, _i32, _vp, _sz, _vp], _i32),
     "tt_sample_image_3d": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i32, _vp], _i32),
+    "tt_sample_image_3d_backward": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _vp, _i32, _vp], _i32),
     "tt_insert_into_image_3d": (
         [_vp, _i32, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _i32, _i32, _vp], _i32),
     "tt_affine_transform_image_3d": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _i64, _i64, _i64, _i32, _vp,

@@ -74,6 +74,80 @@ __global__ void sample3d_kernel(const T* __restrict__ img, int64_t C, int D, int
                        nearest);
 }
 
+// Backward of sample3d_kernel: d/dimage (ACCUMULATED, atomics) and
+// d/dcoordinates (overwritten), PyTorch's complex-gradient convention.
+// Trilinear: the same corners and weights; the coordinate gradient per axis is
+// Re(conj(G) dS/dc) summed over the channels, zero where grid_sample's border
+// clip stops it (a source index of exactly 0 or n-1 on that axis).  Nearest:
+// the gradient goes to the sampled voxel; coordinates get none.
+template <typename T>
+__device__ __forceinline__ bool coord_grad_passes(T c, int n) {
+    // grid_sample's round trip of the coordinate: c -> c / (0.5 n - 0.5) - 1 -> ((g + 1) / 2) (n - 1)
+    const T half = (T)0.5 * (T)n - (T)0.5;
+    const T raw = ((c / half - (T)1 + (T)1) * (T)0.5) * (T)(n - 1);
+    return raw > (T)0 && raw < (T)(n - 1);
+}
+
+template <typename T, int E>
+__global__ void sample3d_bwd_kernel(const T* __restrict__ img, int64_t C, int D, int H, int W,
+                                    const T* __restrict__ coords, int64_t n, const T* __restrict__ grad,
+                                    T* __restrict__ gimg, T* __restrict__ gcoord, int nearest) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const T cz = coords[i * 3 + 0], cy = coords[i * 3 + 1], cx = coords[i * 3 + 2];
+    const T* gi = grad + i * C * E;
+    T dz = (T)0, dy = (T)0, dx = (T)0;
+    const bool inside = cz >= (T)0 && cz <= (T)(D - 1) && cy >= (T)0 && cy <= (T)(H - 1) && cx >= (T)0 &&
+                        cx <= (T)(W - 1);
+    const int64_t plane = (int64_t)D * H * W;
+    if (inside && nearest) {
+        if (gimg) {
+            const int z = (int)nearbyint((double)cz), y = (int)nearbyint((double)cy), x = (int)nearbyint((double)cx);
+            const int64_t vi = ((int64_t)z * H + y) * W + x;
+            for (int64_t ch = 0; ch < C; ch++)
+#pragma unroll
+                for (int e = 0; e < E; e++) atomicAdd(gimg + (ch * plane + vi) * E + e, gi[ch * E + e]);
+        }
+    } else if (inside) {
+        const T fz = floor(cz), fy = floor(cy), fx = floor(cx);
+        const int z0 = (int)fz, y0 = (int)fy, x0 = (int)fx;
+        const T az[2] = {(fz + (T)1) - cz, cz - fz};
+        const T ay[2] = {(fy + (T)1) - cy, cy - fy};
+        const T ax[2] = {(fx + (T)1) - cx, cx - fx};
+        const T sgn[2] = {(T)-1, (T)1};
+        for (int64_t ch = 0; ch < C; ch++) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int bz = (k >> 2) & 1, by = (k >> 1) & 1, bx = k & 1;
+                const int z = z0 + bz, y = y0 + by, x = x0 + bx;
+                if (z >= D || y >= H || x >= W) continue;
+                const int64_t vi = ch * plane + ((int64_t)z * H + y) * W + x;
+                if (gimg) {
+                    const T wgt = ax[bx] * ay[by] * az[bz];
+#pragma unroll
+                    for (int e = 0; e < E; e++) atomicAdd(gimg + vi * E + e, gi[ch * E + e] * wgt);
+                }
+                if (gcoord) {
+                    T gv = (T)0;  // Re(conj(G) v)
+#pragma unroll
+                    for (int e = 0; e < E; e++) gv += gi[ch * E + e] * img[vi * E + e];
+                    dz += gv * sgn[bz] * ay[by] * ax[bx];
+                    dy += gv * az[bz] * sgn[by] * ax[bx];
+                    dx += gv * az[bz] * ay[by] * sgn[bx];
+                }
+            }
+        }
+        if (!coord_grad_passes(cz, D)) dz = (T)0;
+        if (!coord_grad_passes(cy, H)) dy = (T)0;
+        if (!coord_grad_passes(cx, W)) dx = (T)0;
+    }
+    if (gcoord) {
+        gcoord[i * 3 + 0] = dz;
+        gcoord[i * 3 + 1] = dy;
+        gcoord[i * 3 + 2] = dx;
+    }
+}
+
 // affine_transform_image_3d (torch_transform_image/transforms_3d.py:10-40):
 // output voxel (z, y, x) of matrix m samples the image at M_m (z, y, x, 1),
 // M in zyx order, computed in float32 with the reference's operation order
@@ -233,4 +307,40 @@ extern "C" int tt_affine_transform_image_3d(const void* image, int32_t dtype, in
                                                           (double*)out, nearest);
     }
     return check_launch("affine3d_kernel");
+}
+
+extern "C" int tt_sample_image_3d_backward(const void* image, int32_t dtype, int64_t channels, int64_t d, int64_t h,
+                                           int64_t w, const void* coordinates, int64_t n, const void* grad_out,
+                                           void* grad_image, void* grad_coordinates, int32_t nearest, void* stream) {
+    if (n == 0) return TT_OK;
+    if (!image || !coordinates || !grad_out || channels < 1 || d < 1 || h < 1 || w < 1 || n < 0)
+        return fail(TT_ERR_INVALID, "sample_image_3d backward: bad arguments");
+    if (dtype < 0 || dtype > 3) return fail(TT_ERR_INVALID, "sample_image_3d backward: dtype must be 0-3");
+    if (!grad_image && !grad_coordinates) return TT_OK;
+    const unsigned b = nblocks(n, 256);
+    cudaStream_t st = as_stream(stream);
+    switch (dtype) {
+        case 0:
+            sample3d_bwd_kernel<float, 1><<<b, 256, 0, st>>>((const float*)image, channels, (int)d, (int)h, (int)w,
+                                                             (const float*)coordinates, n, (const float*)grad_out,
+                                                             (float*)grad_image, (float*)grad_coordinates, nearest);
+            break;
+        case 1:
+            sample3d_bwd_kernel<double, 1><<<b, 256, 0, st>>>((const double*)image, channels, (int)d, (int)h,
+                                                              (int)w, (const double*)coordinates, n,
+                                                              (const double*)grad_out, (double*)grad_image,
+                                                              (double*)grad_coordinates, nearest);
+            break;
+        case 2:
+            sample3d_bwd_kernel<float, 2><<<b, 256, 0, st>>>((const float*)image, channels, (int)d, (int)h, (int)w,
+                                                             (const float*)coordinates, n, (const float*)grad_out,
+                                                             (float*)grad_image, (float*)grad_coordinates, nearest);
+            break;
+        default:
+            sample3d_bwd_kernel<double, 2><<<b, 256, 0, st>>>((const double*)image, channels, (int)d, (int)h,
+                                                              (int)w, (const double*)coordinates, n,
+                                                              (const double*)grad_out, (double*)grad_image,
+                                                              (double*)grad_coordinates, nearest);
+    }
+    return check_launch("sample3d_bwd_kernel");
 }

@@ -2,7 +2,10 @@
 
 ``sample_image_3d`` and ``insert_into_image_3d`` keep the reference
 signatures and semantics (torch_image_interpolation/image_interpolation_3d.py:11-101
-and :104-275) and run on sm_100a gather / scatter kernels.
+and :104-275) and run on sm_100a gather / scatter kernels.  ``sample_image_3d``
+is differentiable w.r.t. the image and the coordinates, as the reference's
+grid_sample is (one backward kernel: a d/dimage scatter and the trilinear
+coordinate gradient; no per-sample copy of the image).
 """
 
 from __future__ import annotations
@@ -24,6 +27,37 @@ def _code(dtype: torch.dtype) -> int:
     return _DTYPE_CODES[dtype]
 
 
+class _SampleImage3d(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, img, coords, nearest):
+        C, D, H, W = img.shape
+        n = coords.shape[0]
+        out = torch.empty((n, C), dtype=img.dtype, device=img.device)
+        L = _lib.load()
+        _lib.check(L.tt_sample_image_3d(_lib.ptr(img), _code(img.dtype), C, D, H, W, _lib.ptr(coords), n,
+                                        _lib.ptr(out), int(nearest), _lib.stream_of(img.device)), "sample_image_3d")
+        ctx.save_for_backward(img, coords)
+        ctx.nearest = nearest
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        img, coords = ctx.saved_tensors
+        want_i, want_c = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        if not (want_i or want_c):
+            return None, None, None
+        C, D, H, W = img.shape
+        grad = _lib.dense(grad.to(img.dtype))
+        gimg = torch.zeros_like(img) if want_i else None
+        gc = torch.empty_like(coords) if want_c else None
+        L = _lib.load()
+        _lib.check(L.tt_sample_image_3d_backward(_lib.ptr(img), _code(img.dtype), C, D, H, W, _lib.ptr(coords),
+                                                 coords.shape[0], _lib.ptr(grad), _lib.ptr(gimg), _lib.ptr(gc),
+                                                 int(ctx.nearest), _lib.stream_of(img.device)),
+                   "sample_image_3d backward")
+        return gimg, gc, None
+
+
 def sample_image_3d(
     image: torch.Tensor,
     coordinates: torch.Tensor,
@@ -38,19 +72,14 @@ def sample_image_3d(
     if interpolation not in ("nearest", "trilinear"):
         raise ValueError(f"interpolation must be 'nearest' or 'trilinear', got {interpolation!r}")
     _lib.require_cuda(image)
-    code = _code(image.dtype)
+    _code(image.dtype)  # validates the dtype
     multi = image.ndim == 4
     img = _lib.dense(image if multi else image[None])
     C, D, H, W = img.shape
     coords = torch.as_tensor(coordinates).to(image.device)
     batch = coords.shape[:-1]
     c = _lib.dense(coords.reshape(-1, 3).to(_REAL[image.dtype]))
-    n = c.shape[0]
-    out = torch.empty((n, C), dtype=image.dtype, device=image.device)
-    L = _lib.load()
-    _lib.check(L.tt_sample_image_3d(_lib.ptr(img), code, C, D, H, W, _lib.ptr(c), n,
-                                    _lib.ptr(out), int(interpolation == "nearest"),
-                                    _lib.stream_of(image.device)), "sample_image_3d")
+    out = _SampleImage3d.apply(img, c, interpolation == "nearest")
     out = out.reshape(*batch, C)
     return out if multi else out[..., 0]
 

@@ -25,6 +25,7 @@ Cases (reference test each one mirrors):
   bpgrad_*       reference autograd of backproject_2d_to_3d w.r.t. the images
   lines_*, linesgrad_*, proj1d_*   extract_central_slices_rfft_2d (+ its autograd), project_2d_to_1d
   affine_*       torch_transform_image.affine_transform_image_3d
+  sgrad_*        sample_image_3d autograd w.r.t. the image and the coordinates
 """
 
 from __future__ import annotations
@@ -335,6 +336,23 @@ def main():
                                                           interpolation="trilinear", output_shape=(6, 7, 5),
                                                           zyx_matrices=True).numpy()
     g["affine_shape_zyx_image"] = g_img.numpy()
+
+    # ---------------- sample_image_3d autograd (image and coordinates) ----------------
+    gen = torch.Generator().manual_seed(41)
+    rng2 = np.random.default_rng(41)
+    for name, shape, dt in (("real", (7, 8, 9), torch.float32), ("complex", (7, 8, 9), torch.complex64),
+                            ("multi", (3, 7, 8, 9), torch.float32)):
+        img = torch.randn(shape, dtype=dt, generator=gen).requires_grad_(True)
+        hi = np.array(shape[-3:]) - 1
+        coords = rng2.uniform(-0.5, hi + 0.5, size=(6, 10, 3))
+        coords[0, :4] = np.array([[0, 2.5, 3.5], [hi[0], 1.5, 2.5], [2.5, hi[1], 0], [3.25, 4.5, hi[2]]])
+        c = torch.tensor(coords, dtype=torch.float32, requires_grad=True)
+        out = sample_image_3d(img, c, interpolation="trilinear")
+        G = torch.randn(out.shape, dtype=out.dtype, generator=gen)
+        (out * G.conj()).real.sum().backward()
+        g[f"sgrad_{name}_image"], g[f"sgrad_{name}_coords"], g[f"sgrad_{name}_G"] = (
+            img.detach().numpy(), c.detach().numpy(), G.numpy())
+        g[f"sgrad_{name}_dimage"], g[f"sgrad_{name}_dcoords"] = img.grad.numpy(), c.grad.numpy()
 
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {os.path.getsize(OUT) / 1e6:.2f} MB, {len(g)} arrays")

@@ -249,3 +249,17 @@ def test_backprojection_gradient_matches_reference_autograd(golden, name):
     assert rel_l2(rec.detach().cpu().numpy(), fused.cpu().numpy()) < 1e-6
     (rec * torch.as_tensor(golden[f"bpgrad_{name}_G"]).cuda()).sum().backward()
     assert rel_l2(imgs.grad.cpu().numpy(), golden[f"bpgrad_{name}_out"]) < 1e-5
+
+
+@pytest.mark.parametrize("name", ["real", "complex", "multi"])
+def test_sample_image_3d_gradients_match_reference_autograd(golden, name):
+    import teamtomo_b200 as tt
+
+    img = torch.as_tensor(golden[f"sgrad_{name}_image"]).cuda().requires_grad_(True)
+    c = torch.as_tensor(golden[f"sgrad_{name}_coords"]).cuda().requires_grad_(True)
+    out = tt.sample_image_3d(img, c)
+    (out * torch.as_tensor(golden[f"sgrad_{name}_G"]).cuda().conj()).real.sum().backward()
+    assert rel_l2(img.grad.cpu().numpy(), golden[f"sgrad_{name}_dimage"]) < 1e-6
+    assert rel_l2(c.grad.cpu().numpy(), golden[f"sgrad_{name}_dcoords"]) < 1e-5
+    # border and outside points: same zeros as grid_sample's backward
+    assert np.array_equal(c.grad.cpu().numpy() == 0, golden[f"sgrad_{name}_dcoords"] == 0)
