@@ -397,6 +397,14 @@ int tt_affine_transform_image_3d(const void *image, int32_t dtype, int64_t chann
                                  int64_t od, int64_t oh, int64_t ow, int32_t nearest, void *out,
                                  void *stream);
 
+/* Backward of tt_insert_into_image_3d w.r.t. the values: grad_values
+ * (n, channels) of the image's dtype, overwritten, = the upstream image
+ * gradient gathered with the insertion's own weights (zero for dropped points).
+ * Replaces the index_put_ backward of insert_into_image_3d. */
+int tt_insert_into_image_3d_backward(const void *grad_image, int32_t dtype, const float *coordinates,
+                                     int64_t n, int64_t channels, int64_t d, int64_t h, int64_t w,
+                                     int32_t nearest, void *grad_values, void *stream);
+
 /* ---- elementwise passes around the FFTs of the real-space wrappers ------
  * is_f64 selects float64 (else float32) real data; complex128 likewise. */
 

@@ -105,6 +105,7 @@ SIGNATURES = {
         [_vp, _i32, _vp, _i64, _vp, _i64, _i64, _i64, _i64, _vp, _i32, _i32, _vp], _i32),
     "tt_affine_transform_image_3d": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _i64, _i64, _i64, _i64, _i32, _vp,
                                       _vp], _i32),
+    "tt_insert_into_image_3d_backward": ([_vp, _i32, _vp, _i64, _i64, _i64, _i64, _i64, _i32, _vp, _vp], _i32),
     "tt_project_prepare": ([_vp, _i32, _i64, _i64, _vp, _vp], _i32),
     "tt_recentre_crop_2d": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp], _i32),
     "tt_pad_fftshift_2d": ([_vp, _i32, _i64, _i64, _i64, _vp, _vp], _i32),

@@ -210,6 +210,43 @@ __global__ void insert3d_kernel(const T* __restrict__ vals, const float* __restr
     }
 }
 
+// Backward of insert3d_kernel w.r.t. the values: each point gathers the
+// upstream image gradient at the voxels it was added to, with the same float32
+// weights (grad_values (n, channels) overwritten; zero for dropped points).
+template <typename T, int E>
+__global__ void insert3d_bwd_kernel(const T* __restrict__ gimg, const float* __restrict__ coords, int64_t n,
+                                    int64_t C, int D, int H, int W, T* __restrict__ gvals, int nearest) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float cz = coords[i * 3 + 0], cy = coords[i * 3 + 1], cx = coords[i * 3 + 2];
+    T* o = gvals + i * C * E;
+    for (int64_t k = 0; k < C * E; k++) o[k] = (T)0;
+    if (!(cz >= 0.0f && cz <= (float)D - 1.0f && cy >= 0.0f && cy <= (float)H - 1.0f && cx >= 0.0f &&
+          cx <= (float)W - 1.0f))
+        return;
+    const int64_t plane = (int64_t)D * H * W;
+    if (nearest) {
+        const int64_t vi = ((int64_t)rintf(cz) * H + (int64_t)rintf(cy)) * W + (int64_t)rintf(cx);
+        for (int64_t ch = 0; ch < C; ch++)
+#pragma unroll
+            for (int e = 0; e < E; e++) o[ch * E + e] = gimg[(ch * plane + vi) * E + e];
+        return;
+    }
+    const float z0 = floorf(cz), y0 = floorf(cy), x0 = floorf(cx);
+    const int iz[2] = {(int)z0, (int)ceilf(cz)}, iy[2] = {(int)y0, (int)ceilf(cy)}, ix[2] = {(int)x0, (int)ceilf(cx)};
+    const float tz = cz - z0, ty = cy - y0, tx = cx - x0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        const int bz = (k >> 2) & 1, by = (k >> 1) & 1, bx = k & 1;
+        const float w = ((bz ? tz : 1.0f - tz) * (by ? ty : 1.0f - ty)) * (bx ? tx : 1.0f - tx);
+        if (w == 0.0f) continue;
+        const int64_t vi = ((int64_t)iz[bz] * H + iy[by]) * W + ix[bx];
+        for (int64_t ch = 0; ch < C; ch++)
+#pragma unroll
+            for (int e = 0; e < E; e++) o[ch * E + e] += gimg[(ch * plane + vi) * E + e] * (T)w;
+    }
+}
+
 inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace tt
@@ -343,4 +380,33 @@ extern "C" int tt_sample_image_3d_backward(const void* image, int32_t dtype, int
                                                               (double*)grad_coordinates, nearest);
     }
     return check_launch("sample3d_bwd_kernel");
+}
+
+extern "C" int tt_insert_into_image_3d_backward(const void* grad_image, int32_t dtype, const float* coordinates,
+                                                int64_t n, int64_t channels, int64_t d, int64_t h, int64_t w,
+                                                int32_t nearest, void* grad_values, void* stream) {
+    if (n == 0) return TT_OK;
+    if (!grad_image || !coordinates || !grad_values || channels < 1 || d < 1 || h < 1 || w < 1 || n < 0)
+        return fail(TT_ERR_INVALID, "insert_into_image_3d backward: bad arguments");
+    if (dtype < 0 || dtype > 3) return fail(TT_ERR_INVALID, "insert_into_image_3d backward: dtype must be 0-3");
+    const unsigned b = nblocks(n, 256);
+    cudaStream_t st = as_stream(stream);
+    switch (dtype) {
+        case 0:
+            insert3d_bwd_kernel<float, 1><<<b, 256, 0, st>>>((const float*)grad_image, coordinates, n, channels,
+                                                             (int)d, (int)h, (int)w, (float*)grad_values, nearest);
+            break;
+        case 1:
+            insert3d_bwd_kernel<double, 1><<<b, 256, 0, st>>>((const double*)grad_image, coordinates, n, channels,
+                                                              (int)d, (int)h, (int)w, (double*)grad_values, nearest);
+            break;
+        case 2:
+            insert3d_bwd_kernel<float, 2><<<b, 256, 0, st>>>((const float*)grad_image, coordinates, n, channels,
+                                                             (int)d, (int)h, (int)w, (float*)grad_values, nearest);
+            break;
+        default:
+            insert3d_bwd_kernel<double, 2><<<b, 256, 0, st>>>((const double*)grad_image, coordinates, n, channels,
+                                                              (int)d, (int)h, (int)w, (double*)grad_values, nearest);
+    }
+    return check_launch("insert3d_bwd_kernel");
 }

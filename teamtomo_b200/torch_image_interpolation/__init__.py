@@ -113,23 +113,51 @@ def insert_into_image_3d(
         return image, weights
     if weights.dtype not in (torch.float32, torch.float64):
         raise ValueError(f"weights must be float32 or float64, got {weights.dtype}")
-    code = _code(image.dtype)
     C = image.shape[0] if multi else 1
-    vals = _lib.dense(values.to(image.device).reshape(-1, C))
+    vals = values.to(image.device).reshape(-1, C)
     c = coordinates.to(image.device).reshape(-1, 3).float().contiguous()
-    img = image if image.is_contiguous() else image.contiguous()
-    wts = weights if weights.is_contiguous() else weights.contiguous()
-    L = _lib.load()
-    _lib.check(L.tt_insert_into_image_3d(_lib.ptr(vals), code, _lib.ptr(c), c.shape[0],
-                                         _lib.ptr(img), C, d, h, w, _lib.ptr(wts),
-                                         int(wts.dtype == torch.float64),
-                                         int(interpolation == "nearest"),
-                                         _lib.stream_of(image.device)), "insert_into_image_3d")
-    if img is not image:
-        image.copy_(img)
-    if wts is not weights:
-        weights.copy_(wts)
+    if image.is_contiguous() and weights.is_contiguous():
+        return _InsertIntoImage3d.apply(vals, c, image, weights, C, interpolation == "nearest")
+    img, wts = image.contiguous(), weights.contiguous()
+    _InsertIntoImage3d.apply(vals, c, img, wts, C, interpolation == "nearest")
+    image.copy_(img)
+    weights.copy_(wts)
     return image, weights
+
+
+class _InsertIntoImage3d(torch.autograd.Function):
+    """In-place splat into (image, weights); differentiable w.r.t. the values
+    (the reference's index_put_ backward: a gather with the same weights).
+    The coordinates get no gradient."""
+
+    @staticmethod
+    def forward(ctx, vals, coords, image, weights, C, nearest):
+        d, h, w = image.shape[-3:]
+        v = _lib.dense(vals)
+        L = _lib.load()
+        _lib.check(L.tt_insert_into_image_3d(_lib.ptr(v), _code(image.dtype), _lib.ptr(coords), coords.shape[0],
+                                             _lib.ptr(image), C, d, h, w, _lib.ptr(weights),
+                                             int(weights.dtype == torch.float64), int(nearest),
+                                             _lib.stream_of(image.device)), "insert_into_image_3d")
+        ctx.mark_dirty(image, weights)
+        ctx.mark_non_differentiable(weights)
+        ctx.save_for_backward(coords)
+        ctx.meta = (C, d, h, w, nearest, image.dtype, vals.shape)
+        return image, weights
+
+    @staticmethod
+    def backward(ctx, grad_image, grad_weights):
+        (coords,) = ctx.saved_tensors
+        C, d, h, w, nearest, dtype, vshape = ctx.meta
+        gv = None
+        if ctx.needs_input_grad[0] and grad_image is not None:
+            g = _lib.dense(grad_image.to(dtype))
+            gv = torch.empty(vshape, dtype=dtype, device=g.device)
+            L = _lib.load()
+            _lib.check(L.tt_insert_into_image_3d_backward(_lib.ptr(g), _code(dtype), _lib.ptr(coords),
+                                                          coords.shape[0], C, d, h, w, int(nearest), _lib.ptr(gv),
+                                                          _lib.stream_of(g.device)), "insert_into_image_3d backward")
+        return gv, None, grad_image, None, None, None
 
 
 __all__ = ["sample_image_3d", "insert_into_image_3d"]

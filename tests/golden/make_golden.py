@@ -26,6 +26,7 @@ Cases (reference test each one mirrors):
   lines_*, linesgrad_*, proj1d_*   extract_central_slices_rfft_2d (+ its autograd), project_2d_to_1d
   affine_*       torch_transform_image.affine_transform_image_3d
   sgrad_*        sample_image_3d autograd w.r.t. the image and the coordinates
+  igrad_*        insert_into_image_3d autograd w.r.t. the values
 """
 
 from __future__ import annotations
@@ -353,6 +354,18 @@ def main():
         g[f"sgrad_{name}_image"], g[f"sgrad_{name}_coords"], g[f"sgrad_{name}_G"] = (
             img.detach().numpy(), c.detach().numpy(), G.numpy())
         g[f"sgrad_{name}_dimage"], g[f"sgrad_{name}_dcoords"] = img.grad.numpy(), c.grad.numpy()
+
+    # ---------------- insert_into_image_3d autograd w.r.t. the values ----------------
+    for name, dt, mode in (("f32", torch.float32, "trilinear"), ("c64", torch.complex64, "trilinear"),
+                           ("f32", torch.float32, "nearest")):
+        vals = torch.randn((5, 12), dtype=dt, generator=gen).requires_grad_(True)
+        coords = torch.tensor(rng2.uniform(-0.5, 9.5, size=(5, 12, 3)), dtype=torch.float32)
+        img, _ = insert_into_image_3d(vals, coords, torch.zeros((9, 10, 11), dtype=dt), interpolation=mode)
+        G = torch.randn(img.shape, dtype=dt, generator=gen)
+        (img * G.conj()).real.sum().backward()
+        key = f"igrad_{name}_{mode}"
+        g[f"{key}_values"], g[f"{key}_coords"], g[f"{key}_G"] = vals.detach().numpy(), coords.numpy(), G.numpy()
+        g[f"{key}_dvalues"] = vals.grad.numpy()
 
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {os.path.getsize(OUT) / 1e6:.2f} MB, {len(g)} arrays")

@@ -263,3 +263,17 @@ def test_sample_image_3d_gradients_match_reference_autograd(golden, name):
     assert rel_l2(c.grad.cpu().numpy(), golden[f"sgrad_{name}_dcoords"]) < 1e-5
     # border and outside points: same zeros as grid_sample's backward
     assert np.array_equal(c.grad.cpu().numpy() == 0, golden[f"sgrad_{name}_dcoords"] == 0)
+
+
+@pytest.mark.parametrize("key", ["f32_trilinear", "c64_trilinear", "f32_nearest"])
+def test_insert_into_image_3d_value_gradient_matches_reference(golden, key):
+    import teamtomo_b200 as tt
+
+    k = f"igrad_{key}"
+    vals = torch.as_tensor(golden[f"{k}_values"]).cuda().requires_grad_(True)
+    img = torch.zeros((9, 10, 11), dtype=vals.dtype, device="cuda")
+    out, w = tt.insert_into_image_3d(vals, torch.as_tensor(golden[f"{k}_coords"]).cuda(), img,
+                                     interpolation=key.split("_")[1])
+    assert out is img and not w.requires_grad
+    (out * torch.as_tensor(golden[f"{k}_G"]).cuda().conj()).real.sum().backward()
+    assert rel_l2(vals.grad.cpu().numpy(), golden[f"{k}_dvalues"]) < 1e-6
