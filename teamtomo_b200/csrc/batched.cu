@@ -95,10 +95,12 @@ batched_slices_kernel(const __grid_constant__ BatchParams bp, unsigned long long
         const CtfConst* ccp = bv.ctf ? &cc : nullptr;
         for (int tile = 0; tile < bv.tiles; tile++) {
             int iy, ix;
-            if (!tile_pixel_t<TX>(bv.g, tile, iy, ix)) continue;
+            const bool has_pixel = tile_pixel_t<TX>(bv.g, tile, iy, ix);
             if (INSERT) {
-                insert_point<float>(bv.slices, m, bv.acc, bv.g, s, iy, ix, ccp);
+                // every lane takes part: lane pairs share a pixel's x-corners
+                insert_point_paired(bv.slices, m, bv.acc, bv.g, s, has_pixel, iy, ix, ccp);
             } else {
+                if (!has_pixel) continue;
                 float qy, qx, c[3];
                 bool cj = false;
                 float2 r = make_float2(0.0f, 0.0f);

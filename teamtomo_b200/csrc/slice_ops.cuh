@@ -279,15 +279,15 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
 // reduce the x-low and the x-high corner of the same pixel in the same
 // instruction (adjacent voxels, usually one 32-byte L2 sector), serving pixels
 // j and j + 16 in two rounds; the pixel data move by warp shuffles.  Same
-// pixels, corners, weights ((fz * fy) * fx) and values as insert_point.  Must
-// be called by all 32 lanes of the warp (has_pixel false where the tile
-// overhangs the slice).
+// pixels, corners, weights ((fz * fy) * fx), CTF weighting and values as
+// insert_point.  Must be called by all 32 lanes of the warp (has_pixel false
+// where the tile overhangs the slice).
 __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ img, const float* m,
                                                     float4* __restrict__ acc, const SliceGeom& g, int64_t s,
-                                                    bool has_pixel, int iy, int ix) {
+                                                    bool has_pixel, int iy, int ix, const CtfConst* ctf = nullptr) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, bx = lane & 1;
-    float dre = 0.f, dim = 0.f, tx = 0.f;
+    float dre = 0.f, dim = 0.f, tx = 0.f, wscale = 1.f;
     int x0 = 0, x1 = 0;
     int64_t rowbase[4] = {0, 0, 0, 0};
     float wzy[4] = {0.f, 0.f, 0.f, 0.f};
@@ -301,6 +301,12 @@ __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ i
             if (insert_cell(g, m, qy, qx, cj, k)) {
                 dre = d.x;
                 dim = cj ? -d.y : d.y;
+                if (ctf) {
+                    const float cv = ctf_value(*ctf, qy, qx);
+                    dre *= cv;
+                    dim *= cv;
+                    wscale = cv * cv;
+                }
                 tx = k.tx;
                 x0 = k.ix0;
                 x1 = k.ix1;
@@ -317,7 +323,7 @@ __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ i
     for (int half = 0; half < 2; half++) {
         const int src = (lane >> 1) + 16 * half;
         const float sre = __shfl_sync(full, dre, src), sim = __shfl_sync(full, dim, src);
-        const float stx = __shfl_sync(full, tx, src);
+        const float stx = __shfl_sync(full, tx, src), sws = __shfl_sync(full, wscale, src);
         // every lane runs every shuffle (full mask), then picks its corner
         const int sx0 = __shfl_sync(full, x0, src), sx1 = __shfl_sync(full, x1, src);
         const int sx = bx ? sx1 : sx0;
@@ -327,7 +333,7 @@ __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ i
             const float swzy = __shfl_sync(full, wzy[zy], src);
             const long long sbase = __shfl_sync(full, (long long)rowbase[zy], src);
             const float w = swzy * fx;
-            if (w != 0.0f) acc_add(acc + sbase + sx, sre * w, sim * w, w);
+            if (w != 0.0f) acc_add(acc + sbase + sx, sre * w, sim * w, w * sws);
         }
     }
 }
