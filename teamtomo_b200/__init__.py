@@ -6,6 +6,8 @@ hand-written sm_100a CUDA kernels through the C ABI in include/teamtomo_b200.h.
 """
 
 from . import (
+    autotune,
+    batched,
     distributed,
     losses,
     streaming,
@@ -30,6 +32,8 @@ from .torch_image_interpolation import insert_into_image_3d, sample_image_3d
 __version__ = "0.1.0"
 
 __all__ = [
+    "autotune",
+    "batched",
     "distributed",
     "losses",
     "streaming",

@@ -41,6 +41,24 @@ def sinc2_grid_3(n0: int, n1: int, n2: int, device, dtype=torch.float32) -> torc
     return (torch.sinc(r) ** 2).to(dtype)
 
 
+def irfftn_last(x: torch.Tensor, ndim: int) -> torch.Tensor:
+    """``irfftn`` over the last ``ndim`` axes (no output size), evaluated the way
+    torch's CPU FFT evaluates it: inverse complex FFTs along the leading axes,
+    then a 1D inverse real FFT along the last axis that ignores the imaginary
+    parts of its DC and Nyquist bins.  Sampled central slices (and inserted
+    volumes) are not exactly Hermitian, and for such inputs cuFFT's
+    multi-dimensional complex-to-real transform differs from the CPU result
+    by ~1e-4; this form matches it."""
+    if ndim > 1:
+        x = torch.fft.ifftn(x, dim=tuple(range(-ndim, -1)))
+    m = x.shape[-1]
+    keep = torch.ones(m, dtype=x.real.dtype, device=x.device)
+    keep[0] = 0
+    keep[m - 1] = 0  # the Nyquist bin of the default (even) output length
+    x = torch.complex(x.real, x.imag * keep)
+    return torch.fft.irfft(x, dim=-1)
+
+
 class _ProjectPrepare(torch.autograd.Function):
     @staticmethod
     def forward(ctx, volume, pad):

@@ -58,7 +58,7 @@ def _backproject(images, rotation_matrices, pad_factor, fftfreq_max, zyx_matrice
     if torch.is_grad_enabled() and images.requires_grad:
         vols, weights = _InsertCentralSlices.apply(spec, R, shape, fftfreq_max, zyx_matrices, False, True)
         dft = torch.fft.ifftshift(vols / torch.clamp(weights, min=1.0), dim=(-3, -2))
-        real = torch.fft.irfftn(dft, dim=(-3, -2, -1))
+        real = _wrappers.irfftn_last(dft, 3)
         out = _wrappers.backproject_finish(real, p)
         return out if channels else out[0]
     c128 = spec.dtype == torch.complex128
@@ -72,7 +72,7 @@ def _backproject(images, rotation_matrices, pad_factor, fftfreq_max, zyx_matrice
                               images_unshifted=True)
     dft = _wrappers.backproject_normalize(acc)
     # irfftn without an output size, as the reference (odd boxes lose one x column)
-    real = torch.fft.irfftn(dft, dim=(-3, -2, -1))
+    real = _wrappers.irfftn_last(dft, 3)
     out = _wrappers.backproject_finish(real, p)
     return out if channels else out[0]
 

@@ -18,6 +18,7 @@ import torch
 import torch.nn.functional as F
 
 from .. import _lib
+from ._wrappers import irfftn_last
 
 
 def _rotation_2d(rotation_matrices: torch.Tensor, device):
@@ -121,7 +122,7 @@ def project_2d_to_1d(
     dft = torch.fft.fftshift(dft, dim=(-2,))
     lines = extract_central_slices_rfft_2d(dft.to(torch.complex64), (n, n), rotation_matrices,
                                            fftfreq_max=fftfreq_max, yx_matrices=yx_matrices)
-    proj = torch.fft.ifftshift(torch.fft.irfftn(lines, dim=(-1,)), dim=(-1,))
+    proj = torch.fft.ifftshift(irfftn_last(lines, 1), dim=(-1,))
     if p:
         proj = F.pad(proj, pad=[-p] * 2)
     return proj

@@ -50,7 +50,7 @@ def project_3d_to_2d(
     slices = _ExtractCentralSlices.apply(dft, R, params, (R.shape[0], n_pad, n_pad // 2 + 1))
     # irfftn without an output size, as the reference: an odd padded box
     # gives images one column narrower (2 * (n_pad // 2) wide)
-    images = torch.fft.irfftn(slices, dim=(-2, -1))
+    images = _wrappers.irfftn_last(slices, 2)
     out = _wrappers.recentre_crop_2d(images, p)
     return out.reshape(*stack, *out.shape[-2:])
 
@@ -79,6 +79,6 @@ def project_3d_to_2d_multichannel(
                           fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
                           rot_tolerance=1e-8, volume_unshifted=True, slices_unshifted=True)
     slices = _ExtractMultichannel.apply(dft, R, params, (R.shape[0], c, n_pad, n_pad // 2 + 1))
-    images = torch.fft.irfftn(slices, dim=(-2, -1))
+    images = _wrappers.irfftn_last(slices, 2)
     out = _wrappers.recentre_crop_2d(images.reshape(-1, *images.shape[-2:]), p)
     return out.reshape(*stack, c, *out.shape[-2:])
