@@ -296,6 +296,15 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def xp_launches(n_pixels, volume, purposes=("forward", "grad")):
+    """1 when an extraction of n_pixels slice pixels (forward, or rotation
+    gradient / fused MSE) gathers from an x-paired copy of the volume (one
+    pack launch), else 0."""
+    from teamtomo_b200.torch_fourier_slice._xpairs import use_xpairs
+
+    return int(any(use_xpairs(n_pixels, volume, p) for p in purposes))
+
+
 def load_traffic():
     path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
@@ -531,7 +540,11 @@ def config_workload(args):
                     "config": {"workload": "full scale: 320^3 complex64 rfft volume (320x320x161), "
                                f"images generated on the GPU in chunks of {chunk} (not timed)",
                                "images": n_img, "orientations": n_ext},
-                    "torch_gpu_reference": None, "clocks": clk, "gpu_launches": n_img // chunk * 3 + n_ext // chunk * 3})
+                    "torch_gpu_reference": None, "clocks": clk,
+                    # insertion: splat, finalize, sum; fused MSE: loss kernel, loss and rotation finish
+                    # (+ the x-paired copy of the volume)
+                    "gpu_launches": n_img // chunk * 3
+                    + n_ext // chunk * (3 + xp_launches(chunk * n * (n // 2 + 1), Vfit, ("grad",)))})
     print(json.dumps(out))
     return 0
 
@@ -807,9 +820,10 @@ def main():
                        "deterministic": det},
             "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "fused_mse": fused, "torch_gpu_reference": torch_gpu,
-            # extract, backward, rotation-gradient finish, insert splat, insert finalize
-            # (+ absmax pre-passes and the fixed-point add-back when deterministic)
-            "gpu_launches": (8 if det else 5) * args.steps,
+            # extract (+ the x-paired copy of the volume it gathers from), backward,
+            # rotation-gradient finish, insert splat, insert finalize (+ absmax
+            # pre-passes and the fixed-point add-back when deterministic)
+            "gpu_launches": ((8 if det else 5) + xp_launches(ns * n * (n // 2 + 1), V)) * args.steps,
             "loss": float(loss.item()),
         }
         print(json.dumps(line))

@@ -60,6 +60,11 @@ typedef struct tt_slice_params {
     int32_t deterministic;         /* 1: insertion and the volume gradient accumulate in 64-bit
                                       fixed point, bit-identical for any launch order (the
                                       workspace queries grow accordingly) */
+    int32_t volume_xpairs;         /* 1: volume_rfft is the x-paired copy written by
+                                      tt_pack_volume_xpairs (extraction forward, backward and
+                                      tt_central_slice_mse only; other entry points refuse it).
+                                      Occupies the struct's former tail padding: 0 keeps the
+                                      plain layout, so zero-initialised structs are unchanged. */
 } tt_slice_params;
 
 /* Per-image contrast transfer function, the scalar arguments of torch-ctf's
@@ -99,6 +104,19 @@ int tt_extract_central_slices_rfft_3d(const void *volume_rfft, const void *rotat
  * and _insert_central_slices_rfft_3d.py:30-85, which the reference keeps internal. */
 int tt_slice_geometry(const void *rotation_matrices, int32_t mode, uint8_t *flags, float *coords,
                       const tt_slice_params *p, void *stream);
+
+/* x-paired copy of an rfft volume for the extraction gathers: entry (z, y, x)
+ * holds the complex64 pair (V[z, y, x], V[z, y, x + 1]) as four floats, the
+ * second zero in the last column, in the (z, y) order of the source (fftshifted,
+ * or plain when p->volume_unshifted).  A pixel's eight trilinear corners are
+ * then four 16-byte loads instead of eight 8-byte ones, which lowers the L1
+ * wavefronts of the scattered gathers.  Pass the copy as volume_rfft with
+ * p->volume_xpairs = 1; results are bit-identical to the plain layout.
+ * tt_volume_xpairs_bytes: p->vol_d * vol_h * vol_w * 16.  The source is
+ * complex64 (vol_d, vol_h, vol_w); xpairs must be 16-byte aligned.  The
+ * reference has no such layout (it samples with grid_sample on the volume). */
+size_t tt_volume_xpairs_bytes(const tt_slice_params *p);
+int tt_pack_volume_xpairs(const void *volume_rfft, void *xpairs, const tt_slice_params *p, void *stream);
 
 /* Bytes of workspace tt_extract_central_slices_rfft_3d_backward needs when a
  * rotation gradient or (p->deterministic) a volume gradient is requested

@@ -35,7 +35,7 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 // Validates the common slice parameters; vol_w must be the rfft width of a
 // real dimension and all sizes must fit the int32 index arithmetic used on
 // the per-slice grid.
-inline int validate_params(const tt_slice_params* p) {
+inline int validate_params(const tt_slice_params* p, bool allow_xpairs = false) {
     if (!p) return fail(TT_ERR_INVALID, "params is NULL");
     if (p->n < 0) return fail(TT_ERR_INVALID, "n must be >= 0 (got %lld)", (long long)p->n);
     if (p->img_d < 1 || p->img_h < 1 || p->img_w < 1)
@@ -47,6 +47,9 @@ inline int validate_params(const tt_slice_params* p) {
         return fail(TT_ERR_INVALID, "slice or volume too large");
     if (p->n > (1LL << 31) - 1) return fail(TT_ERR_INVALID, "too many slices");
     if (p->deterministic != 0 && p->deterministic != 1) return fail(TT_ERR_INVALID, "deterministic must be 0 or 1");
+    if (p->volume_xpairs != 0 && p->volume_xpairs != 1) return fail(TT_ERR_INVALID, "volume_xpairs must be 0 or 1");
+    if (p->volume_xpairs && !allow_xpairs)
+        return fail(TT_ERR_INVALID, "volume_xpairs: this entry point takes the plain volume layout");
     return TT_OK;
 }
 

@@ -35,8 +35,10 @@ __device__ __forceinline__ void load_rotation(float* sm, const void* rot, int64_
     if (threadIdx.x < 9) sm[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, apply_tol);
 }
 
+// VT: float2 (plain volume) or float4 (x-paired copy, tt_pack_volume_xpairs).
+template <typename VT>
 __global__ void __launch_bounds__(kExtractThreads)
-extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
+extract_fwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
                    float2* __restrict__ out, SliceGeom g, int tiles) {
     __shared__ float m[9];
     const int64_t s = blockIdx.x / tiles;
@@ -59,8 +61,8 @@ extract_fwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
 // Backward of one slice pixel; acc receives the pixel's 6 contributions to
 // d/dR_zyx.  Called by every lane of the warp (has_pixel false where the tile
 // overhangs the slice): the float d/dvolume scatter pairs lanes across the warp.
-template <bool WANT_DV, bool WANT_DR, bool FIXED>
-__device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const float* m,
+template <bool WANT_DV, bool WANT_DR, bool FIXED, typename VT>
+__device__ __forceinline__ void bwd_point(const VT* __restrict__ vol, const float* m,
                                           const float2* __restrict__ grad, const DvTarget<FIXED>& dv,
                                           const SliceGeom& g, int64_t s, bool has_pixel, int iy, int ix,
                                           float acc[6]) {
@@ -89,7 +91,8 @@ __device__ __forceinline__ void bwd_point(const float2* __restrict__ vol, const 
 }
 
 // Sample, residual and loss term of one pixel (mse_point); returns G'.
-__device__ __forceinline__ float2 mse_residual(const float2* __restrict__ vol, const SliceGeom& g, const Corners& k,
+template <typename VT>
+__device__ __forceinline__ float2 mse_residual(const VT* __restrict__ vol, const SliceGeom& g, const Corners& k,
                                                float2 t, bool cj, float scale, double& loss, float acc[6], float qy,
                                                float qx, bool want_dr) {
     float2 v[2][2][2];
@@ -124,8 +127,8 @@ __device__ __forceinline__ float2 mse_residual(const float2* __restrict__ vol, c
 // whose sample is zero (outside fftfreq_max or the volume) add |T|^2 and no
 // gradient.
 // Called by every lane of the warp (the d/dvolume scatter pairs lanes).
-template <bool WANT_DV, bool WANT_DR>
-__device__ __forceinline__ void mse_point(const float2* __restrict__ vol, const float* m,
+template <bool WANT_DV, bool WANT_DR, typename VT>
+__device__ __forceinline__ void mse_point(const VT* __restrict__ vol, const float* m,
                                           const float2* __restrict__ target, const DvTarget<false>& dv,
                                           const SliceGeom& g, int64_t s, bool has_pixel, int iy, int ix, float scale,
                                           float acc[6], double& loss) {
@@ -151,9 +154,9 @@ __device__ __forceinline__ void mse_point(const float2* __restrict__ vol, const 
 // non-zero entries of d/dR_zyx go to part[(s * tiles + tile) * 6 + k],
 // reduced in double within the block.  FIXED: the volume gradient goes to the
 // fixed-point words `fixed` at the scale set by *absmax and n.
-template <bool WANT_DV, bool WANT_DR, bool FIXED>
-__global__ void __launch_bounds__(kExtractThreads)
-extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
+template <bool WANT_DV, bool WANT_DR, bool FIXED, typename VT>
+__global__ void __launch_bounds__(kExtractThreads, FIXED ? 4 : 5)
+extract_bwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
                    const float2* __restrict__ grad, float2* __restrict__ dvol,
                    unsigned long long* __restrict__ fixed, const uint32_t* __restrict__ absmax,
                    float* __restrict__ part, SliceGeom g, int tiles) {
@@ -168,7 +171,7 @@ extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
     if (FIXED) dv.scale = fixed_data_scale(*absmax, ceil_log2(g.n));
     int iy, ix;
     const bool has_pixel = tile_pixel(g, tile, iy, ix);
-    bwd_point<WANT_DV, WANT_DR, FIXED>(vol, m, grad, dv, g, s, has_pixel, iy, ix, acc);
+    bwd_point<WANT_DV, WANT_DR, FIXED, VT>(vol, m, grad, dv, g, s, has_pixel, iy, ix, acc);
     if (WANT_DR) {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -189,9 +192,9 @@ extract_bwd_kernel(const float2* __restrict__ vol, const void* __restrict__ rot,
 // Fused extraction + mean squared error + backward: one block per (slice,
 // tile).  Block partials of the loss (double) go to loss_part[s * tiles + tile]
 // and, with WANT_DR, those of d/dR_zyx to part[(s * tiles + tile) * 6 + k].
-template <bool WANT_DV, bool WANT_DR>
+template <bool WANT_DV, bool WANT_DR, typename VT>
 __global__ void __launch_bounds__(kExtractThreads)
-slice_mse_kernel(const float2* __restrict__ vol, const void* __restrict__ rot, const float2* __restrict__ target,
+slice_mse_kernel(const VT* __restrict__ vol, const void* __restrict__ rot, const float2* __restrict__ target,
                  float2* __restrict__ dvol, float* __restrict__ part, double* __restrict__ loss_part, float scale,
                  SliceGeom g, int tiles) {
     __shared__ float m[9];
@@ -205,7 +208,7 @@ slice_mse_kernel(const float2* __restrict__ vol, const void* __restrict__ rot, c
     const DvTarget<false> dv{dvol, nullptr, 0.0};
     int iy, ix;
     const bool has_pixel = tile_pixel(g, tile, iy, ix);
-    mse_point<WANT_DV, WANT_DR>(vol, m, target, dv, g, s, has_pixel, iy, ix, scale, acc, loss);
+    mse_point<WANT_DV, WANT_DR, VT>(vol, m, target, dv, g, s, has_pixel, iy, ix, scale, acc, loss);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < 7; k++) {
@@ -336,8 +339,9 @@ static size_t fixed_dv_bytes(const tt_slice_params* p) {
 // Launches the backward and the rotation-gradient reduction; `part` holds
 // n * tiles * 6 floats when grad_rotation is set; `fixed` (deterministic
 // volume gradient) is the zeroed header + accumulator of fixed_dv_bytes.
-static int launch_backward(const float2* v, const void* rot, const float2* gr, float2* dv, void* grad_rotation,
-                           float* part, const SliceGeom& g, cudaStream_t st, void* fixed = nullptr) {
+template <typename VT>
+static int launch_backward_t(const VT* v, const void* rot, const float2* gr, float2* dv, void* grad_rotation,
+                             float* part, const SliceGeom& g, cudaStream_t st, void* fixed) {
     const int tiles = extract_tiles(g);
     const unsigned blocks = (unsigned)((int64_t)g.n * tiles);
     uint32_t* absmax = (uint32_t*)fixed;
@@ -345,23 +349,23 @@ static int launch_backward(const float2* v, const void* rot, const float2* gr, f
     if (dv && fixed) {
         if (int e = launch_fixed_absmax(gr, 0, (int64_t)g.n * g.img_h * g.wr * 2, absmax, st)) return e;
         if (grad_rotation)
-            extract_bwd_kernel<true, true, true><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, facc, absmax,
+            extract_bwd_kernel<true, true, true, VT><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, facc, absmax,
                                                                                     part, g, tiles);
         else
-            extract_bwd_kernel<true, false, true><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, facc, absmax,
+            extract_bwd_kernel<true, false, true, VT><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, facc, absmax,
                                                                                      part, g, tiles);
         if (int e = check_launch("extract_bwd_kernel")) return e;
         const int64_t vox = (int64_t)g.D * g.H * g.W;
         dv_fixed_add_kernel<<<(unsigned)((vox + 255) / 256), 256, 0, st>>>((const long long*)facc, dv, absmax,
                                                                            ceil_log2(g.n), vox);
     } else if (dv && grad_rotation) {
-        extract_bwd_kernel<true, true, false><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
+        extract_bwd_kernel<true, true, false, VT><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
                                                                                  part, g, tiles);
     } else if (dv) {
-        extract_bwd_kernel<true, false, false><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
+        extract_bwd_kernel<true, false, false, VT><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
                                                                                   part, g, tiles);
     } else {
-        extract_bwd_kernel<false, true, false><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
+        extract_bwd_kernel<false, true, false, VT><<<blocks, kExtractThreads, 0, st>>>(v, rot, gr, dv, nullptr, nullptr,
                                                                                   part, g, tiles);
     }
     if (int e = check_launch("extract_bwd_kernel")) return e;
@@ -371,6 +375,45 @@ static int launch_backward(const float2* v, const void* rot, const float2* gr, f
         if (int e = check_launch("drot_finish_kernel")) return e;
     }
     return TT_OK;
+}
+
+// `v` is the plain complex64 volume or, with g.vol_xpairs, its x-paired copy.
+static int launch_backward(const void* v, const void* rot, const float2* gr, float2* dv, void* grad_rotation,
+                           float* part, const SliceGeom& g, cudaStream_t st, void* fixed = nullptr) {
+    if (g.vol_xpairs)
+        return launch_backward_t((const float4*)v, rot, gr, dv, grad_rotation, part, g, st, fixed);
+    return launch_backward_t((const float2*)v, rot, gr, dv, grad_rotation, part, g, st, fixed);
+}
+
+// x-paired copy: xp[r * W + x] = (vol[r * W + x], vol[r * W + x + 1]), zero
+// past the last column.  Threads run along x (coalesced), rows in a grid-stride loop.
+__global__ void pack_xpairs_kernel(const float2* __restrict__ vol, float4* __restrict__ xp, int64_t rows, int W) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= W) return;
+    for (int64_t r = (int64_t)blockIdx.y * blockDim.y + threadIdx.y; r < rows; r += (int64_t)gridDim.y * blockDim.y) {
+        const int64_t i = r * W + x;
+        const float2 a = vol[i];
+        const float2 b = x + 1 < W ? vol[i + 1] : make_float2(0.0f, 0.0f);
+        xp[i] = make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
+template <typename VT>
+static int launch_mse(const VT* v, const void* rot, const float2* t, float2* dv, void* grad_rotation, float* part,
+                      double* loss_part, float scale, const SliceGeom& g, int tiles, unsigned nb, cudaStream_t st) {
+    if (dv && grad_rotation)
+        slice_mse_kernel<true, true, VT><<<nb, kExtractThreads, 0, st>>>(v, rot, t, dv, part, loss_part, scale, g,
+                                                                        tiles);
+    else if (dv)
+        slice_mse_kernel<true, false, VT><<<nb, kExtractThreads, 0, st>>>(v, rot, t, dv, part, loss_part, scale, g,
+                                                                         tiles);
+    else if (grad_rotation)
+        slice_mse_kernel<false, true, VT><<<nb, kExtractThreads, 0, st>>>(v, rot, t, dv, part, loss_part, scale, g,
+                                                                         tiles);
+    else
+        slice_mse_kernel<false, false, VT><<<nb, kExtractThreads, 0, st>>>(v, rot, t, dv, part, loss_part, scale, g,
+                                                                          tiles);
+    return check_launch("slice_mse_kernel");
 }
 
 }  // namespace tt
@@ -389,7 +432,7 @@ extern "C" size_t tt_central_slice_mse_workspace_bytes(const tt_slice_params* p)
 extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotation_matrices, const void* targets,
                                     float* loss, void* grad_volume, void* grad_rotation, void* workspace,
                                     size_t workspace_bytes, const tt_slice_params* p, void* stream) {
-    if (int e = validate_params(p)) return e;
+    if (int e = validate_params(p, true)) return e;
     if (p->deterministic)
         return fail(TT_ERR_INVALID, "central_slice_mse: no deterministic mode (the gradient scale is known only "
                                     "after the loss); use the extraction backward");
@@ -408,24 +451,15 @@ extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotatio
     float* part = (float*)((char*)workspace + (size_t)blocks * sizeof(double));
     const double m = (double)g.n * g.img_h * g.wr;
     const float scale = (float)(2.0 / m);
-    const float2* v = (const float2*)volume_rfft;
     const float2* t = (const float2*)targets;
     float2* dv = (float2*)grad_volume;
     cudaStream_t st = as_stream(stream);
     const unsigned nb = (unsigned)blocks;
-    if (dv && grad_rotation)
-        slice_mse_kernel<true, true><<<nb, kExtractThreads, 0, st>>>(v, rotation_matrices, t, dv, part, loss_part,
-                                                                    scale, g, tiles);
-    else if (dv)
-        slice_mse_kernel<true, false><<<nb, kExtractThreads, 0, st>>>(v, rotation_matrices, t, dv, part, loss_part,
-                                                                     scale, g, tiles);
-    else if (grad_rotation)
-        slice_mse_kernel<false, true><<<nb, kExtractThreads, 0, st>>>(v, rotation_matrices, t, dv, part, loss_part,
-                                                                     scale, g, tiles);
-    else
-        slice_mse_kernel<false, false><<<nb, kExtractThreads, 0, st>>>(v, rotation_matrices, t, dv, part,
-                                                                      loss_part, scale, g, tiles);
-    if (int e = check_launch("slice_mse_kernel")) return e;
+    if (int e = g.vol_xpairs ? launch_mse((const float4*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part,
+                                          loss_part, scale, g, tiles, nb, st)
+                             : launch_mse((const float2*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part,
+                                          loss_part, scale, g, tiles, nb, st))
+        return e;
     mse_loss_finish_kernel<<<1, 1024, 0, st>>>(loss_part, blocks, 1.0 / m, loss);
     if (int e = check_launch("mse_loss_finish_kernel")) return e;
     if (grad_rotation) {
@@ -439,7 +473,7 @@ extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotatio
 
 extern "C" int tt_extract_central_slices_rfft_3d(const void* volume_rfft, const void* rotation_matrices,
                                                  void* slices_out, const tt_slice_params* p, void* stream) {
-    if (int e = validate_params(p)) return e;
+    if (int e = validate_params(p, true)) return e;
     if (p->n == 0) return TT_OK;
     if (!volume_rfft || !rotation_matrices || !slices_out)
         return fail(TT_ERR_INVALID, "extract: NULL pointer argument");
@@ -447,14 +481,40 @@ extern "C" int tt_extract_central_slices_rfft_3d(const void* volume_rfft, const 
     const int tiles = extract_tiles(g);
     const int64_t blocks = (int64_t)g.n * tiles;
     if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract: too many blocks");
-    extract_fwd_kernel<<<(unsigned)blocks, kExtractThreads, 0, as_stream(stream)>>>(
-        (const float2*)volume_rfft, rotation_matrices, (float2*)slices_out, g, tiles);
+    if (g.vol_xpairs)
+        extract_fwd_kernel<<<(unsigned)blocks, kExtractThreads, 0, as_stream(stream)>>>(
+            (const float4*)volume_rfft, rotation_matrices, (float2*)slices_out, g, tiles);
+    else
+        extract_fwd_kernel<<<(unsigned)blocks, kExtractThreads, 0, as_stream(stream)>>>(
+            (const float2*)volume_rfft, rotation_matrices, (float2*)slices_out, g, tiles);
     return check_launch("extract_fwd_kernel");
+}
+
+extern "C" size_t tt_volume_xpairs_bytes(const tt_slice_params* p) {
+    if (!p || p->vol_d < 1 || p->vol_h < 1 || p->vol_w < 1) return 0;
+    return (size_t)(p->vol_d * p->vol_h * p->vol_w) * sizeof(float4);
+}
+
+extern "C" int tt_pack_volume_xpairs(const void* volume_rfft, void* xpairs, const tt_slice_params* p,
+                                     void* stream) {
+    if (int e = validate_params(p, true)) return e;
+    if (!volume_rfft || !xpairs) return fail(TT_ERR_INVALID, "pack_volume_xpairs: NULL pointer argument");
+    if ((reinterpret_cast<uintptr_t>(xpairs) & 15) != 0)
+        return fail(TT_ERR_INVALID, "pack_volume_xpairs: the x-paired copy must be 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(volume_rfft) & 7) != 0)
+        return fail(TT_ERR_INVALID, "pack_volume_xpairs: the volume must be 8-byte aligned");
+    const int64_t rows = p->vol_d * p->vol_h;
+    const int W = (int)p->vol_w;
+    const dim3 block(32, 8);
+    const int64_t gy = (rows + block.y - 1) / block.y;
+    const dim3 grid((unsigned)((W + 31) / 32), (unsigned)(gy < 65535 ? gy : 65535));
+    pack_xpairs_kernel<<<grid, block, 0, as_stream(stream)>>>((const float2*)volume_rfft, (float4*)xpairs, rows, W);
+    return check_launch("pack_xpairs_kernel");
 }
 
 extern "C" int tt_slice_geometry(const void* rotation_matrices, int32_t mode, uint8_t* flags, float* coords,
                                  const tt_slice_params* p, void* stream) {
-    if (int e = validate_params(p)) return e;
+    if (int e = validate_params(p, true)) return e;
     if (p->n == 0) return TT_OK;
     if (!rotation_matrices || !flags || !coords) return fail(TT_ERR_INVALID, "slice_geometry: NULL pointer argument");
     if (mode != 0 && mode != 1) return fail(TT_ERR_INVALID, "slice_geometry: mode must be 0 or 1");
@@ -475,7 +535,7 @@ extern "C" size_t tt_extract_backward_workspace_bytes(const tt_slice_params* p) 
 extern "C" int tt_extract_central_slices_rfft_3d_backward(
     const void* volume_rfft, const void* rotation_matrices, const void* grad_slices, void* grad_volume,
     void* grad_rotation, void* workspace, size_t workspace_bytes, const tt_slice_params* p, void* stream) {
-    if (int e = validate_params(p)) return e;
+    if (int e = validate_params(p, true)) return e;
     if (p->n == 0) return TT_OK;
     if (!volume_rfft || !rotation_matrices || !grad_slices)
         return fail(TT_ERR_INVALID, "extract backward: NULL pointer argument");
@@ -495,9 +555,8 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward(
         cudaError_t e = cudaMemsetAsync(workspace, 0, fixed, st);
         if (e != cudaSuccess) return fail(TT_ERR_CUDA, "extract backward: memset: %s", cudaGetErrorString(e));
     }
-    return launch_backward((const float2*)volume_rfft, rotation_matrices, (const float2*)grad_slices,
-                           (float2*)grad_volume, grad_rotation, (float*)((char*)workspace + fixed), g, st,
-                           fixed ? workspace : nullptr);
+    return launch_backward(volume_rfft, rotation_matrices, (const float2*)grad_slices, (float2*)grad_volume,
+                           grad_rotation, (float*)((char*)workspace + fixed), g, st, fixed ? workspace : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -554,7 +613,7 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward_noalloc(const void* vo
                                                                   const void* grad_slices, void* grad_volume,
                                                                   void* grad_rotation, const tt_slice_params* p,
                                                                   void* stream) {
-    if (int e = validate_params(p)) return e;
+    if (int e = validate_params(p, true)) return e;
     if (p->n == 0) return TT_OK;
     if (!volume_rfft || !rotation_matrices || !grad_slices)
         return fail(TT_ERR_INVALID, "noalloc backward: NULL pointer argument");
@@ -566,7 +625,7 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward_noalloc(const void* vo
     const int tiles = extract_tiles(g);
     if ((int64_t)g.n * tiles > 0x7fffffffLL) return fail(TT_ERR_INVALID, "noalloc backward: too many blocks");
     cudaStream_t st = as_stream(stream);
-    const float2* v = (const float2*)volume_rfft;
+    const void* v = volume_rfft;
     const float2* gr = (const float2*)grad_slices;
     float2* dv = (float2*)grad_volume;
     // the scratch holds n * tiles * 6 partial sums of the rotation gradient

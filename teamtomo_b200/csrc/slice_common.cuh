@@ -34,6 +34,7 @@ struct SliceGeom {
     int rot_f64;                   // rotation matrices are float64
     int vol_unshifted;             // volume is the plain rfftn output (no fftshift of z, y)
     int slice_unshifted;           // slices are stored ifftshifted along rows (irfft-ready)
+    int vol_xpairs;                // volume is the x-paired copy (float4 per voxel)
     float dcdp0, dcdp1, dcdp2;     // d(array coord)/d(frequency) per axis
 };
 
@@ -68,6 +69,7 @@ __host__ inline SliceGeom make_geom(const tt_slice_params& p) {
     g.rot_f64 = p.rotation_f64;
     g.vol_unshifted = p.volume_unshifted;
     g.slice_unshifted = p.slices_unshifted;
+    g.vol_xpairs = p.volume_xpairs;
     g.dcdp0 = g.s0 / g.iw0;
     g.dcdp1 = g.s1 / g.iw1;
     g.dcdp2 = 2.0f * g.sx;

@@ -88,8 +88,9 @@ __device__ __forceinline__ void scatter_dv_paired(float2* __restrict__ dvol, con
 }
 
 // The eight corner values of a pixel; corners past the last index read as
-// zero, as in grid_sample.
-__device__ __forceinline__ void load_corners(const float2* __restrict__ vol, const SliceGeom& g, const Corners& k,
+// zero, as in grid_sample.  VT: float2 (plain layout) or float4 (x-paired).
+template <typename VT>
+__device__ __forceinline__ void load_corners(const VT* __restrict__ vol, const SliceGeom& g, const Corners& k,
                                              float2 v[2][2][2]) {
 #pragma unroll
     for (int bz = 0; bz < 2; bz++)
@@ -97,11 +98,7 @@ __device__ __forceinline__ void load_corners(const float2* __restrict__ vol, con
         for (int by = 0; by < 2; by++) {
             const bool row_ok = (!bz || k.zin) && (!by || k.yin);
             const int64_t base = vox_index(g, k.z0 + (row_ok ? bz : 0), k.y0 + (row_ok ? by : 0), k.x0);
-#pragma unroll
-            for (int bx = 0; bx < 2; bx++) {
-                const bool ok = row_ok && (!bx || k.xin);
-                v[bz][by][bx] = ok ? __ldg(vol + base + bx) : make_float2(0.f, 0.f);
-            }
+            load_xrow(vol, base, row_ok, row_ok && k.xin, v[bz][by][0], v[bz][by][1]);
         }
 }
 

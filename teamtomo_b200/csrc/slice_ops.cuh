@@ -71,8 +71,27 @@ __device__ __forceinline__ bool extract_geometry(const SliceGeom& g, const float
     return inside_volume(g, c);
 }
 
-// Trilinear sample of the complex volume at corner set k.
-__device__ __forceinline__ float2 sample_trilinear(const float2* __restrict__ vol, const SliceGeom& g,
+// The two x-corners (x0, x0 + 1) of the volume row starting at voxel `base`:
+// v0 when lo, v1 when hi (hi implies lo), zero otherwise.  Plain layout: two
+// 8-byte gathers.
+__device__ __forceinline__ void load_xrow(const float2* __restrict__ vol, int64_t base, bool lo, bool hi,
+                                          float2& v0, float2& v1) {
+    v0 = lo ? __ldg(vol + base) : make_float2(0.0f, 0.0f);
+    v1 = hi ? __ldg(vol + base + 1) : make_float2(0.0f, 0.0f);
+}
+
+// x-paired layout (entry = (V[x], V[x + 1])): one 16-byte gather.
+__device__ __forceinline__ void load_xrow(const float4* __restrict__ vol, int64_t base, bool lo, bool hi,
+                                          float2& v0, float2& v1) {
+    const float4 q = lo ? __ldg(vol + base) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    v0 = make_float2(q.x, q.y);
+    v1 = hi ? make_float2(q.z, q.w) : make_float2(0.0f, 0.0f);
+}
+
+// Trilinear sample of the complex volume at corner set k; VT is float2 (plain
+// layout) or float4 (x-paired layout), with the same values and FMA order.
+template <typename VT>
+__device__ __forceinline__ float2 sample_trilinear(const VT* __restrict__ vol, const SliceGeom& g,
                                                    const Corners& k) {
     float2 r = make_float2(0.0f, 0.0f);
 #pragma unroll
@@ -84,12 +103,12 @@ __device__ __forceinline__ float2 sample_trilinear(const float2* __restrict__ vo
             if (by && !k.yin) continue;
             const float wzy = (by ? k.ay1 : k.ay0) * wz;
             const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
-            const float2 v0 = __ldg(vol + base);
+            float2 v0, v1;
+            load_xrow(vol, base, true, k.xin, v0, v1);
             const float w0 = k.ax0 * wzy;
             r.x = fmaf(v0.x, w0, r.x);
             r.y = fmaf(v0.y, w0, r.y);
             if (k.xin) {
-                const float2 v1 = __ldg(vol + base + 1);
                 const float w1 = k.ax1 * wzy;
                 r.x = fmaf(v1.x, w1, r.x);
                 r.y = fmaf(v1.y, w1, r.y);

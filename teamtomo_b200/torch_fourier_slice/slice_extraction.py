@@ -23,6 +23,7 @@ from __future__ import annotations
 import torch
 
 from .. import _lib
+from . import _xpairs
 from ._params import resolve_deterministic, rotation_arg, slice_params
 
 
@@ -35,23 +36,36 @@ class _ExtractCentralSlices(torch.autograd.Function):
         dev = volume_rfft.device
         out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
         L = _lib.load()
+        # large calls gather from an x-paired copy (bit-identical results)
+        xp = (_xpairs.pack(volume_rfft, params) if _xpairs.use_xpairs(out.numel(), volume_rfft, "forward")
+              else None)
         _lib.check(
-            L.tt_extract_central_slices_rfft_3d(_lib.ptr(volume_rfft), _lib.ptr(rotation_matrices),
-                                                _lib.ptr(out), params, _lib.stream_of(dev)),
+            L.tt_extract_central_slices_rfft_3d(_lib.ptr(xp if xp is not None else volume_rfft),
+                                                _lib.ptr(rotation_matrices), _lib.ptr(out),
+                                                _xpairs.with_xpairs(params, xp is not None),
+                                                _lib.stream_of(dev)),
             "extract_central_slices_rfft_3d",
         )
         ctx.params = params
-        ctx.save_for_backward(volume_rfft, rotation_matrices)
+        # the backward reads the volume only for d/drotation: keep the copy for it
+        keep_xp = xp is not None and ctx.needs_input_grad[1]
+        ctx.has_xp = keep_xp
+        ctx.save_for_backward(volume_rfft, rotation_matrices, *((xp,) if keep_xp else ()))
         return out
 
     @staticmethod
     def backward(ctx, grad):
-        volume_rfft, rotation_matrices = ctx.saved_tensors
+        saved = ctx.saved_tensors
+        volume_rfft, rotation_matrices = saved[0], saved[1]
         want_v, want_r = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         dvol = drot = None
         if want_v or want_r:
+            xp = saved[2] if ctx.has_xp else None
+            # the rotation gradient's gathers read the x-paired copy at any volume size
+            if xp is None and want_r and _xpairs.use_xpairs(grad.numel(), volume_rfft, "grad"):
+                xp = _xpairs.pack(volume_rfft, ctx.params)
             dvol, drot = extract_backward(volume_rfft, rotation_matrices, grad, ctx.params,
-                                          want_v, want_r)
+                                          want_v, want_r, xpairs=xp)
         return dvol, drot, None, None
 
 
@@ -95,11 +109,14 @@ class _ExtractMultichannel(torch.autograd.Function):
 
 
 def extract_backward(volume_rfft, rotation_matrices, grad, params, want_volume=True,
-                     want_rotation=True):
-    """Fused backward: (d/dvolume, d/drotation) for upstream slice gradient ``grad``."""
+                     want_rotation=True, xpairs=None):
+    """Fused backward: (d/dvolume, d/drotation) for upstream slice gradient
+    ``grad``.  ``xpairs``: the volume's x-paired copy (``_xpairs.pack``), read
+    by the rotation gradient's gathers in place of ``volume_rfft``."""
     dev = volume_rfft.device
     grad = _lib.dense(grad.to(torch.complex64))
     L = _lib.load()
+    params = _xpairs.with_xpairs(params, xpairs is not None)
     dvol = torch.zeros_like(volume_rfft) if want_volume else None
     drot = torch.empty_like(rotation_matrices) if want_rotation else None
     ws = None
@@ -109,7 +126,8 @@ def extract_backward(volume_rfft, rotation_matrices, grad, params, want_volume=T
         ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     _lib.check(
         L.tt_extract_central_slices_rfft_3d_backward(
-            _lib.ptr(volume_rfft), _lib.ptr(rotation_matrices), _lib.ptr(grad), _lib.ptr(dvol),
+            _lib.ptr(xpairs if xpairs is not None else volume_rfft), _lib.ptr(rotation_matrices),
+            _lib.ptr(grad), _lib.ptr(dvol),
             _lib.ptr(drot), _lib.ptr(ws), nbytes, params, _lib.stream_of(dev)),
         "extract_central_slices_rfft_3d backward",
     )

@@ -54,9 +54,58 @@ def _params(**kw):
 def test_param_struct_layout():
     from teamtomo_b200 import _lib
 
-    # 7 int64 + 11 four-byte fields, padded to the 8-byte alignment of the struct
+    # 7 int64 + 12 four-byte fields (the last one in what was the tail padding)
     assert ctypes.sizeof(_lib.SliceParams) == 104
     assert _lib.SliceParams.fftfreq_max.offset == 60 and _lib.SliceParams.deterministic.offset == 96
+    assert _lib.SliceParams.volume_xpairs.offset == 100
+
+
+def test_xpairs_flag_validation():
+    """volume_xpairs: accepted by the extraction entry points, refused by the
+    others and outside {0, 1}; the pack checks its pointers and alignment."""
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    fake = ctypes.c_void_p(16)
+    p = _params(volume_xpairs=1)
+    assert L.tt_volume_xpairs_bytes(ctypes.byref(p)) == 16 * 16 * 9 * 16
+    assert L.tt_insert_accumulate(fake, 0, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert b"volume_xpairs" in L.tt_last_error()
+    assert L.tt_insert_central_slices_rfft_3d(fake, 0, fake, fake, fake, fake, 1 << 30, ctypes.byref(p),
+                                              None) == _lib.TT_ERR_INVALID
+    assert L.tt_extract_central_slices_rfft_3d_multichannel(fake, 2, fake, fake, ctypes.byref(p),
+                                                            None) == _lib.TT_ERR_INVALID
+    # accepted (fails later, on the missing workspace, not on the flag)
+    assert L.tt_extract_central_slices_rfft_3d_backward(fake, fake, fake, None, fake, None, 0,
+                                                        ctypes.byref(p), None) == _lib.TT_ERR_WORKSPACE
+    p = _params(volume_xpairs=2)
+    assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    p = _params()
+    assert L.tt_pack_volume_xpairs(None, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert L.tt_pack_volume_xpairs(fake, ctypes.c_void_p(24), ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert b"16-byte" in L.tt_last_error()
+
+
+def test_xpairs_policy(monkeypatch):
+    from teamtomo_b200.torch_fourier_slice import _xpairs
+
+    vol = torch.zeros((16, 16, 9), dtype=torch.complex64)
+    monkeypatch.delenv("TT_VOLUME_XPAIRS", raising=False)
+    assert _xpairs.use_xpairs(2 * vol.numel(), vol) and not _xpairs.use_xpairs(2 * vol.numel() - 1, vol)
+    assert not _xpairs.use_xpairs(10**9, vol.to(torch.complex128))
+    assert not _xpairs.use_xpairs(10**9, vol, "forward")  # a CPU tensor: no L2 to fit
+    with pytest.raises(ValueError):
+        _xpairs.use_xpairs(1, vol, "backward")
+    monkeypatch.setenv("TT_VOLUME_XPAIRS", "0")
+    assert not _xpairs.use_xpairs(10**9, vol)
+    monkeypatch.setenv("TT_VOLUME_XPAIRS", "1")
+    assert _xpairs.use_xpairs(1, vol)
+    from teamtomo_b200 import _lib
+
+    p = _lib.SliceParams()
+    p.n, p.deterministic = 7, 1
+    q = _xpairs.with_xpairs(p, True)
+    assert (q.n, q.deterministic, q.volume_xpairs, p.volume_xpairs) == (7, 1, 1, 0)
 
 
 def test_validation_rejects_before_launch():
