@@ -36,8 +36,10 @@ __device__ __forceinline__ void load_rotation(float* sm, const void* rot, int64_
 }
 
 // VT: float2 (plain volume) or float4 (x-paired copy, tt_pack_volume_xpairs).
+// Eight resident blocks (32 registers, no spills): the gathers are latency-
+// bound at six (64 % warps active); full occupancy takes 8.5 % off the launch.
 template <typename VT>
-__global__ void __launch_bounds__(kExtractThreads)
+__global__ void __launch_bounds__(kExtractThreads, 8)
 extract_fwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
                    float2* __restrict__ out, SliceGeom g, int tiles) {
     __shared__ float m[9];

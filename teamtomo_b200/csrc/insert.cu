@@ -141,8 +141,9 @@ __global__ void mirror_x0_kernel(typename Acc<R>::C* __restrict__ vol, R* __rest
 // and each kept source pixel gathers sum_k w_k dL/dacc[corner k] with the
 // splat's own float32 weights, conjugated where the point was redirected.
 // One thread per slice pixel; every pixel is written (zero when dropped).
+// float: eight resident blocks (32 registers, no spills) for the gathers.
 template <typename R>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, sizeof(R) == 4 ? 8 : 1)
 insert_bwd_kernel(const typename Acc<R>::C* __restrict__ gvol, const void* __restrict__ rot,
                   typename Acc<R>::C* __restrict__ gimg, SliceGeom g, int tiles) {
     __shared__ float m[9];

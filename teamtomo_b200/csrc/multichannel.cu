@@ -19,8 +19,9 @@ __device__ __forceinline__ int64_t chan_pixel(const SliceGeom& g, int64_t s, int
     return (((int64_t)s * channels + ch) * g.img_h + slice_row(g, iy)) * g.wr + ix;
 }
 
-// Extraction: one thread per slice pixel, all channels.
-__global__ void __launch_bounds__(kTileThreads)
+// Extraction: one thread per slice pixel, all channels; eight resident blocks
+// (32 registers, no spills) for the gathers.
+__global__ void __launch_bounds__(kTileThreads, 8)
 extract_multi_fwd_kernel(const float2* __restrict__ vol, int64_t vstride, int channels,
                          const void* __restrict__ rot, float2* __restrict__ out, SliceGeom g, int tiles) {
     __shared__ float m[9];
