@@ -72,9 +72,14 @@ __device__ __forceinline__ void bwd_point(const VT* __restrict__ vol, const floa
     bool cj = false;
     const bool valid = has_pixel && extract_geometry(g, m, iy, ix, qy, qx, cj, c);
     Corners k{};
+    SourceIdx si{};
     float2 gv = make_float2(0.f, 0.f);
     if (valid) {
-        k = make_corners(g, c);
+        si = source_indices(g, c);
+        k = corners_at(g, si.z, si.y, si.x);
+        k.gz = si.gz;
+        k.gy = si.gy;
+        k.gx = si.gx;
         gv = __ldcs(grad + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
         if (cj) gv.y = -gv.y;  // G' = conj(G) where the sample was conjugated
     }
@@ -82,7 +87,7 @@ __device__ __forceinline__ void bwd_point(const VT* __restrict__ vol, const floa
         if (FIXED) {
             if (valid) scatter_dv(dv, g, k, gv);
         } else {
-            scatter_dv_paired(dv.dvol, g, k, gv, valid);
+            scatter_dv_paired(dv.dvol, g, si, gv, valid);
         }
     }
     if (WANT_DR && valid) {
@@ -139,17 +144,22 @@ __device__ __forceinline__ void mse_point(const VT* __restrict__ vol, const floa
     bool valid = false;
     float2 gv = make_float2(0.f, 0.f);
     Corners k{};
+    SourceIdx si{};
     if (has_pixel) {
         const float2 t = __ldcs(target + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
         valid = extract_geometry(g, m, iy, ix, qy, qx, cj, c);
         if (!valid) {
             loss += (double)t.x * t.x + (double)t.y * t.y;
         } else {
-            k = make_corners(g, c);
+            si = source_indices(g, c);
+            k = corners_at(g, si.z, si.y, si.x);
+            k.gz = si.gz;
+            k.gy = si.gy;
+            k.gx = si.gx;
             gv = mse_residual(vol, g, k, t, cj, scale, loss, acc, qy, qx, WANT_DR);
         }
     }
-    if (WANT_DV) scatter_dv_paired(dv.dvol, g, k, gv, valid);
+    if (WANT_DV) scatter_dv_paired(dv.dvol, g, si, gv, valid);
 }
 
 // One block per (slice, tile).  WANT_DR: the block's partial sums of the 6
@@ -175,12 +185,11 @@ extract_bwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
     const bool has_pixel = tile_pixel(g, tile, iy, ix);
     bwd_point<WANT_DV, WANT_DR, FIXED, VT>(vol, m, grad, dv, g, s, has_pixel, iy, ix, acc);
     if (WANT_DR) {
+        // warp totals in float (fixed order), then the warps in double
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-        for (int k = 0; k < 6; k++) {
-            const double v = warp_sum_d((double)acc[k]);
-            if (lane == 0) red[warp][k] = v;
-        }
+        const float v8[8] = {acc[0], acc[1], acc[2], acc[3], acc[4], acc[5], 0.f, 0.f};
+        const float t = warp_reduce8(v8);
+        if ((lane & 3) == 0 && (lane >> 2) < 6) red[warp][lane >> 2] = (double)t;
         __syncthreads();
         if (threadIdx.x < 6) {
             double v = 0.0;
@@ -211,12 +220,13 @@ slice_mse_kernel(const VT* __restrict__ vol, const void* __restrict__ rot, const
     int iy, ix;
     const bool has_pixel = tile_pixel(g, tile, iy, ix);
     mse_point<WANT_DV, WANT_DR, VT>(vol, m, target, dv, g, s, has_pixel, iy, ix, scale, acc, loss);
+    // rotation-gradient warp totals in float (fixed order), the loss in double
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 7; k++) {
-        const double v = warp_sum_d(k < 6 ? (double)acc[k] : loss);
-        if (lane == 0) red[warp][k] = v;
-    }
+    const float v8[8] = {acc[0], acc[1], acc[2], acc[3], acc[4], acc[5], 0.f, 0.f};
+    const float t = warp_reduce8(v8);
+    if ((lane & 3) == 0 && (lane >> 2) < 6) red[warp][lane >> 2] = (double)t;
+    const double lw = warp_sum_d(loss);
+    if (lane == 0) red[warp][6] = lw;
     __syncthreads();
     if (threadIdx.x < 7) {
         double v = 0.0;

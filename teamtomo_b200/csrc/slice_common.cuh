@@ -178,6 +178,26 @@ __device__ __forceinline__ float warp_sum(float v) {
     return v;
 }
 
+// Warp totals of eight values per lane by recursive halving (9 shuffles
+// instead of 8 x 5): at each step a lane keeps half of its values and adds
+// the partner's copy of that half.  Lane l returns the total of value l >> 2.
+__device__ __forceinline__ float warp_reduce8(const float v[8]) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+    float a[4], b[2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        a[i] = (h16 ? v[i + 4] : v[i]) + __shfl_xor_sync(full, h16 ? v[i] : v[i + 4], 16);
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+        b[i] = (h8 ? a[i + 2] : a[i]) + __shfl_xor_sync(full, h8 ? a[i] : a[i + 2], 8);
+    float c = (h4 ? b[1] : b[0]) + __shfl_xor_sync(full, h4 ? b[0] : b[1], 4);
+    c += __shfl_xor_sync(full, c, 2);
+    c += __shfl_xor_sync(full, c, 1);
+    return c;
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -54,35 +54,33 @@ __device__ __forceinline__ void scatter_dv(const DvTarget<FIXED>& dv, const Slic
 // and the x-high corner of the same pixel in the same instruction.  The two
 // corners are adjacent voxels, usually in one 32-byte L2 sector, so a warp's
 // reduction touches fewer sectors than with one pixel per lane (each pair of
-// lanes serves pixels j and j + 16 in two rounds; pixel data move by warp
-// shuffles).  Same corners, weights and values as scatter_dv.  Must be called
-// by all 32 lanes of the warp (valid = false for lanes without a pixel).
-__device__ __forceinline__ void scatter_dv_paired(float2* __restrict__ dvol, const SliceGeom& g, const Corners& k,
+// lanes serves pixels j and j + 16 in two rounds).  Only the pixel's G' and
+// its three source indices move by warp shuffles (5 per round; shuffles share
+// the L1 data pipe that limits the backward); each lane rebuilds the corner
+// set from the indices with the same arithmetic, so corners, weights and
+// values are those of scatter_dv.  Must be called by all 32 lanes of the warp
+// (valid = false for lanes without a pixel).
+__device__ __forceinline__ void scatter_dv_paired(float2* __restrict__ dvol, const SliceGeom& g, const SourceIdx& si,
                                                   float2 gv, bool valid) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, bx = lane & 1;
-    int64_t rowbase[4];
-    float wzy[4];
-#pragma unroll
-    for (int zy = 0; zy < 4; zy++) {
-        const int bz = zy >> 1, by = zy & 1;
-        const bool ok = valid && (!bz || k.zin) && (!by || k.yin);
-        wzy[zy] = ok ? (by ? k.ay1 : k.ay0) * (bz ? k.az1 : k.az0) : 0.0f;
-        rowbase[zy] = ok ? vox_index(g, k.z0 + bz, k.y0 + by, k.x0) : 0;
-    }
 #pragma unroll
     for (int half = 0; half < 2; half++) {
         const int src = (lane >> 1) + 16 * half;
         const float sgx = __shfl_sync(full, gv.x, src), sgy = __shfl_sync(full, gv.y, src);
-        const float sax0 = __shfl_sync(full, k.ax0, src), sax1 = __shfl_sync(full, k.ax1, src);
-        const int sxin = __shfl_sync(full, (int)k.xin, src);
-        const float wx = bx ? sax1 : sax0;
+        const float siz = __shfl_sync(full, valid ? si.z : -1.0f, src);  // < 0: no pixel
+        const float siy = __shfl_sync(full, si.y, src), six = __shfl_sync(full, si.x, src);
+        if (siz < 0.0f) continue;
+        const Corners k = corners_at(g, siz, siy, six);
+        if (bx && !k.xin) continue;
+        const float wx = bx ? k.ax1 : k.ax0;
 #pragma unroll
         for (int zy = 0; zy < 4; zy++) {
-            const float swzy = __shfl_sync(full, wzy[zy], src);
-            const long long sbase = __shfl_sync(full, (long long)rowbase[zy], src);
-            const float w = wx * swzy;
-            if ((!bx || sxin) && w != 0.0f) atomicAdd(dvol + sbase + bx, make_float2(sgx * w, sgy * w));
+            const int bz = zy >> 1, by = zy & 1;
+            if ((bz && !k.zin) || (by && !k.yin)) continue;
+            const float w = wx * ((by ? k.ay1 : k.ay0) * (bz ? k.az1 : k.az0));
+            if (w != 0.0f)
+                atomicAdd(dvol + vox_index(g, k.z0 + bz, k.y0 + by, k.x0) + bx, make_float2(sgx * w, sgy * w));
         }
     }
 }

@@ -29,13 +29,26 @@ struct Corners {
     bool gz, gy, gx;                     // the axis passes a coordinate gradient (not on the border)
 };
 
-// grid_sample trilinear corner set of an inside array coordinate c (the
-// round trip decides the cell at integer kinks, where the derivative jumps).
-__device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float c[3]) {
+// grid_sample source indices (z, y, x) of an inside array coordinate c, in
+// [0, n-1], and whether each axis passes a coordinate gradient.
+struct SourceIdx {
+    float z, y, x;
+    bool gz, gy, gx;
+};
+
+__device__ __forceinline__ SourceIdx source_indices(const SliceGeom& g, const float c[3]) {
+    SourceIdx si;
+    si.z = source_index(c[0], 0.5f * (float)g.D - 0.5f, g.ub0, si.gz);
+    si.y = source_index(c[1], 0.5f * (float)g.H - 0.5f, g.ub1, si.gy);
+    si.x = source_index(c[2], 0.5f * (float)g.W - 0.5f, g.ub2, si.gx);
+    return si;
+}
+
+// Trilinear corner set of source indices (iz, iy, ix); gz, gy, gx are left
+// false (make_corners sets them).
+__device__ __forceinline__ Corners corners_at(const SliceGeom& g, float iz, float iy, float ix) {
     Corners k;
-    const float iz = source_index(c[0], 0.5f * (float)g.D - 0.5f, g.ub0, k.gz);
-    const float iy = source_index(c[1], 0.5f * (float)g.H - 0.5f, g.ub1, k.gy);
-    const float ix = source_index(c[2], 0.5f * (float)g.W - 0.5f, g.ub2, k.gx);
+    k.gz = k.gy = k.gx = false;
     const float fz = floorf(iz), fy = floorf(iy), fx = floorf(ix);
     k.z0 = (int)fz;
     k.y0 = (int)fy;
@@ -49,6 +62,17 @@ __device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float 
     k.zin = k.z0 + 1 < g.D;
     k.yin = k.y0 + 1 < g.H;
     k.xin = k.x0 + 1 < g.W;
+    return k;
+}
+
+// grid_sample trilinear corner set of an inside array coordinate c (the
+// round trip decides the cell at integer kinks, where the derivative jumps).
+__device__ __forceinline__ Corners make_corners(const SliceGeom& g, const float c[3]) {
+    const SourceIdx si = source_indices(g, c);
+    Corners k = corners_at(g, si.z, si.y, si.x);
+    k.gz = si.gz;
+    k.gy = si.gy;
+    k.gx = si.gx;
     return k;
 }
 
