@@ -163,8 +163,9 @@ __device__ __forceinline__ void mse_point(const VT* __restrict__ vol, const floa
 }
 
 // One block per (slice, tile).  WANT_DR: the block's partial sums of the 6
-// non-zero entries of d/dR_zyx go to part[(s * tiles + tile) * 6 + k],
-// reduced in double within the block.  FIXED: the volume gradient goes to the
+// non-zero entries of d/dR_zyx go to part[(s * tiles + tile) * 6 + k]: warp
+// totals in float, then the eight warps in double, in a fixed order.  FIXED:
+// the volume gradient goes to the
 // fixed-point words `fixed` at the scale set by *absmax and n.
 template <bool WANT_DV, bool WANT_DR, bool FIXED, typename VT>
 __global__ void __launch_bounds__(kExtractThreads, FIXED ? 4 : 5)

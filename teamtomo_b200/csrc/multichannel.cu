@@ -47,7 +47,7 @@ extract_multi_fwd_kernel(const float2* __restrict__ vol, int64_t vstride, int ch
 }
 
 // Backward: d/dvolume per channel, d/drotation summed over the channels
-// (block partials reduced in double, as in the single-channel kernel).
+// (block partials reduced as in the single-channel kernel).
 template <bool WANT_DV, bool WANT_DR>
 __global__ void __launch_bounds__(kTileThreads)
 extract_multi_bwd_kernel(const float2* __restrict__ vol, int64_t vstride, int channels,
@@ -82,12 +82,11 @@ extract_multi_bwd_kernel(const float2* __restrict__ vol, int64_t vstride, int ch
         }
     }
     if (WANT_DR) {
+        // warp totals in float by recursive halving (fixed order), the warps in double
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-        for (int i = 0; i < 6; i++) {
-            const double v = warp_sum_d((double)acc[i]);
-            if (lane == 0) red[warp][i] = v;
-        }
+        const float v8[8] = {acc[0], acc[1], acc[2], acc[3], acc[4], acc[5], 0.f, 0.f};
+        const float t = warp_reduce8(v8);
+        if ((lane & 3) == 0 && (lane >> 2) < 6) red[warp][lane >> 2] = (double)t;
         __syncthreads();
         if (threadIdx.x < 6) {
             double v = 0.0;
