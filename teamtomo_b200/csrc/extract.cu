@@ -166,9 +166,11 @@ __device__ __forceinline__ void mse_point(const VT* __restrict__ vol, const floa
 // non-zero entries of d/dR_zyx go to part[(s * tiles + tile) * 6 + k]: warp
 // totals in float, then the eight warps in double, in a fixed order.  FIXED:
 // the volume gradient goes to the
-// fixed-point words `fixed` at the scale set by *absmax and n.
+// fixed-point words `fixed` at the scale set by *absmax and n.  Resident
+// blocks: 6 for the rotation gradient alone (39 registers), 5 with the volume
+// gradient (6 would spill into the L1 pipe that bounds it), 4 in fixed point.
 template <bool WANT_DV, bool WANT_DR, bool FIXED, typename VT>
-__global__ void __launch_bounds__(kExtractThreads, FIXED ? 4 : 5)
+__global__ void __launch_bounds__(kExtractThreads, FIXED ? 4 : (WANT_DV ? 5 : 6))
 extract_bwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
                    const float2* __restrict__ grad, float2* __restrict__ dvol,
                    unsigned long long* __restrict__ fixed, const uint32_t* __restrict__ absmax,
