@@ -241,10 +241,10 @@ struct InsertCell {
 };
 
 // Insertion geometry of slice frequency (qy, qx): rotation, the strict x' < 0
-// redirect (cj), array coordinates and the whole-point bounds test.
-__device__ __forceinline__ bool insert_cell(const SliceGeom& g, const float* m, float qy, float qx, bool& cj,
-                                            InsertCell& k) {
-    float p[3], c[3];
+// redirect (cj), array coordinates c and the whole-point bounds test.
+__device__ __forceinline__ bool insert_coords(const SliceGeom& g, const float* m, float qy, float qx, bool& cj,
+                                              float c[3]) {
+    float p[3];
     rotate_slice_point(m, qy, qx, p);
     cj = p[2] < 0.0f;
     if (cj) {
@@ -253,7 +253,11 @@ __device__ __forceinline__ bool insert_cell(const SliceGeom& g, const float* m, 
         p[2] = -p[2];
     }
     to_dft_coords(g, p, c);
-    if (!inside_volume(g, c)) return false;
+    return inside_volume(g, c);
+}
+
+// Floor / ceil cell of inside array coordinates c.
+__device__ __forceinline__ void cell_at(const float c[3], InsertCell& k) {
     const float z0 = floorf(c[0]), y0 = floorf(c[1]), x0 = floorf(c[2]);
     k.tz = c[0] - z0;
     k.ty = c[1] - y0;
@@ -264,6 +268,15 @@ __device__ __forceinline__ bool insert_cell(const SliceGeom& g, const float* m, 
     k.iz1 = (int)ceilf(c[0]);
     k.iy1 = (int)ceilf(c[1]);
     k.ix1 = (int)ceilf(c[2]);
+}
+
+// Insertion geometry and cell of slice frequency (qy, qx); false when the
+// point is outside the volume.
+__device__ __forceinline__ bool insert_cell(const SliceGeom& g, const float* m, float qy, float qx, bool& cj,
+                                            InsertCell& k) {
+    float c[3];
+    if (!insert_coords(g, m, qy, qx, cj, c)) return false;
+    cell_at(c, k);
     return true;
 }
 
@@ -321,27 +334,27 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
 // Float splat of one source pixel with x-paired lanes: lanes 2j and 2j+1
 // reduce the x-low and the x-high corner of the same pixel in the same
 // instruction (adjacent voxels, usually one 32-byte L2 sector), serving pixels
-// j and j + 16 in two rounds; the pixel data move by warp shuffles.  Same
-// pixels, corners, weights ((fz * fy) * fx), CTF weighting and values as
-// insert_point.  Must be called by all 32 lanes of the warp (has_pixel false
-// where the tile overhangs the slice).
+// j and j + 16 in two rounds.  Only the pixel's value (and CTF weight) and
+// its three array coordinates move by warp shuffles; each lane rebuilds the
+// floor / ceil cell from them.  Same pixels, corners, weights
+// ((fz * fy) * fx), CTF weighting and values as insert_point.  Must be called
+// by all 32 lanes of the warp (has_pixel false where the tile overhangs the
+// slice).
 __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ img, const float* m,
                                                     float4* __restrict__ acc, const SliceGeom& g, int64_t s,
                                                     bool has_pixel, int iy, int ix, const CtfConst* ctf = nullptr) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31, bx = lane & 1;
-    float dre = 0.f, dim = 0.f, tx = 0.f, wscale = 1.f;
-    int x0 = 0, x1 = 0;
-    int64_t rowbase[4] = {0, 0, 0, 0};
-    float wzy[4] = {0.f, 0.f, 0.f, 0.f};
+    float dre = 0.f, dim = 0.f, wscale = 1.f;
+    float c[3] = {-1.f, 0.f, 0.f};  // c[0] < 0: no point
     if (has_pixel) {
         const float qy = shifted_freq(iy, g.img_h, g.inv_h);
         const float qx = __fmul_rn((float)ix, g.inv_w);
         if (insert_pixel_kept(g, qy, qx)) {
             const float2 d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
             bool cj;
-            InsertCell k;
-            if (insert_cell(g, m, qy, qx, cj, k)) {
+            float ci[3];
+            if (insert_coords(g, m, qy, qx, cj, ci)) {
                 dre = d.x;
                 dim = cj ? -d.y : d.y;
                 if (ctf) {
@@ -350,33 +363,32 @@ __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ i
                     dim *= cv;
                     wscale = cv * cv;
                 }
-                tx = k.tx;
-                x0 = k.ix0;
-                x1 = k.ix1;
-#pragma unroll
-                for (int zy = 0; zy < 4; zy++) {
-                    const int bz = zy >> 1, by = zy & 1;
-                    wzy[zy] = (bz ? k.tz : 1.0f - k.tz) * (by ? k.ty : 1.0f - k.ty);
-                    rowbase[zy] = vox_index(g, bz ? k.iz1 : k.iz0, by ? k.iy1 : k.iy0, 0);
-                }
+                c[0] = ci[0];
+                c[1] = ci[1];
+                c[2] = ci[2];
             }
         }
     }
 #pragma unroll
     for (int half = 0; half < 2; half++) {
         const int src = (lane >> 1) + 16 * half;
+        // every lane runs every shuffle (full mask; ctf is the same for the warp)
         const float sre = __shfl_sync(full, dre, src), sim = __shfl_sync(full, dim, src);
-        const float stx = __shfl_sync(full, tx, src), sws = __shfl_sync(full, wscale, src);
-        // every lane runs every shuffle (full mask), then picks its corner
-        const int sx0 = __shfl_sync(full, x0, src), sx1 = __shfl_sync(full, x1, src);
-        const int sx = bx ? sx1 : sx0;
-        const float fx = bx ? stx : 1.0f - stx;
+        const float sws = ctf ? __shfl_sync(full, wscale, src) : 1.0f;
+        float sc[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) sc[a] = __shfl_sync(full, c[a], src);
+        if (sc[0] < 0.0f) continue;
+        InsertCell k;
+        cell_at(sc, k);
+        const int x = bx ? k.ix1 : k.ix0;
+        const float fx = bx ? k.tx : 1.0f - k.tx;
 #pragma unroll
         for (int zy = 0; zy < 4; zy++) {
-            const float swzy = __shfl_sync(full, wzy[zy], src);
-            const long long sbase = __shfl_sync(full, (long long)rowbase[zy], src);
-            const float w = swzy * fx;
-            if (w != 0.0f) acc_add(acc + sbase + sx, sre * w, sim * w, w * sws);
+            const int bz = zy >> 1, by = zy & 1;
+            const float w = ((bz ? k.tz : 1.0f - k.tz) * (by ? k.ty : 1.0f - k.ty)) * fx;
+            if (w != 0.0f)
+                acc_add(acc + vox_index(g, bz ? k.iz1 : k.iz0, by ? k.iy1 : k.iy0, x), sre * w, sim * w, w * sws);
         }
     }
 }
