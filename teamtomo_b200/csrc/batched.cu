@@ -66,7 +66,7 @@ __host__ inline int tiles_t(int img_h, int wr) {
 template <int TX, bool INSERT>
 __global__ void __launch_bounds__(256)
 batched_slices_kernel(const __grid_constant__ BatchParams bp, unsigned long long* __restrict__ queue,
-                      int64_t total) {
+                      int64_t total, int phase, int nphase) {
     __shared__ float m[9];
     __shared__ CtfConst cc;
     __shared__ int64_t cur;
@@ -97,6 +97,15 @@ batched_slices_kernel(const __grid_constant__ BatchParams bp, unsigned long long
             int iy, ix;
             const bool has_pixel = tile_pixel_t<TX>(bv.g, tile, iy, ix);
             if (INSERT) {
+                // z-phased filling of large accumulators (the same answer in every thread)
+                if (nphase > 1) {
+                    constexpr int TY = 256 / TX;
+                    const int txt = (bv.g.wr + TX - 1) / TX;
+                    const int ty = tile / txt, tx = tile - ty * txt;
+                    if (insert_tile_phase(bv.g, m, min(ty * TY + TY / 2, bv.g.img_h - 1),
+                                          min(tx * TX + TX / 2, bv.g.wr - 1), nphase) != phase)
+                        continue;
+                }
                 // every lane takes part: lane pairs share a pixel's x-corners
                 insert_point_paired(bv.slices, m, bv.acc, bv.g, s, has_pixel, iy, ix, ccp);
             } else {
@@ -124,6 +133,8 @@ static int tiles_for_shape(const SliceGeom& g) {
     return tiles_t<TX>(g.img_h, g.wr);
 }
 
+int insert_phases(size_t acc_bytes);  // insert.cu
+
 template <int TX, bool INSERT>
 static int launch_batched(BatchParams& bp, unsigned long long* queue, int64_t total, cudaStream_t st) {
     for (int v = 0; v < bp.nvol; v++) bp.v[v].tiles = tiles_for_shape<TX>(bp.v[v].g);
@@ -135,8 +146,22 @@ static int launch_batched(BatchParams& bp, unsigned long long* queue, int64_t to
         occ = 1;
     int64_t blocks = (int64_t)sms * occ;
     if (blocks > total) blocks = total;
-    batched_slices_kernel<TX, INSERT><<<(unsigned)blocks, 256, 0, st>>>(bp, queue, total);
-    return check_launch("batched_slices_kernel");
+    // insertion into large accumulators runs in z-phases (insert_phases), one queue pass each
+    int nphase = 1;
+    if (INSERT)
+        for (int v = 0; v < bp.nvol; v++) {
+            const int k = insert_phases((size_t)((int64_t)bp.v[v].g.D * bp.v[v].g.H * bp.v[v].g.W) * sizeof(float4));
+            nphase = k > nphase ? k : nphase;
+        }
+    for (int ph = 0; ph < nphase; ph++) {
+        if (ph > 0) {
+            cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess) return fail(TT_ERR_CUDA, "batched: memset: %s", cudaGetErrorString(e));
+        }
+        batched_slices_kernel<TX, INSERT><<<(unsigned)blocks, 256, 0, st>>>(bp, queue, total, ph, nphase);
+        if (int e = check_launch("batched_slices_kernel")) return e;
+    }
+    return TT_OK;
 }
 
 static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_t tile_shape, void* workspace,

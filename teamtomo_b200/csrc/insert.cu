@@ -36,12 +36,19 @@ namespace tt {
 template <typename R>
 __global__ void __launch_bounds__(kTileThreads)
 insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void* __restrict__ rot,
-                         typename Acc<R>::T* __restrict__ acc, SliceGeom g, int tiles) {
+                         typename Acc<R>::T* __restrict__ acc, SliceGeom g, int tiles, int phase, int nphase) {
     __shared__ float m[9];
     const int64_t s = blockIdx.x / tiles;
     const int tile = blockIdx.x - (int)(s * tiles);
     if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
     __syncthreads();
+    if (nphase > 1) {  // the same answer in every thread: the whole block leaves
+        const int tx_tiles = tiles_x_of(g.wr);
+        const int ty = tile / tx_tiles, tx = tile - ty * tx_tiles;
+        if (insert_tile_phase(g, m, min(ty * kTileY + kTileY / 2, g.img_h - 1),
+                              min(tx * kTileX + kTileX / 2, g.wr - 1), nphase) != phase)
+            return;
+    }
     int iy, ix;
     const bool has_pixel = tile_pixel(g, tile, iy, ix);
     if constexpr (std::is_same<R, float>::value)
@@ -187,19 +194,39 @@ static int check_insert_params(const tt_slice_params* p) {
     return TT_OK;
 }
 
+// Number of z-phases for an accumulator of acc_bytes: one per 1.1 x the L2
+// (at most 16).  Measured on a B200 (126 MB L2, 4096 slices): 320^3 (264 MB)
+// 7.57 -> 6.32 ms with 2 phases; 256^3 (135 MB) and 192^3 are 4-6 % slower
+// with 2 phases than with 1.
+int insert_phases(size_t acc_bytes) {
+    int dev = 0, l2 = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess ||
+        l2 <= 0) {
+        cudaGetLastError();  // a failed query only costs the phasing
+        return 1;
+    }
+    const int k = (int)ceil((double)acc_bytes / (1.1 * (double)l2));
+    return k < 1 ? 1 : (k > 16 ? 16 : k);
+}
+
 int launch_insert_accumulate(const void* image_rfft, int32_t complex128, const void* rot, void* acc,
                              const tt_slice_params* p, cudaStream_t st) {
     SliceGeom g = make_geom(*p);
     const int tiles = tiles_per_slice(g.img_h, g.wr);
     const int64_t items = (int64_t)g.n * tiles;
     if (items > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert: too many blocks");
-    if (complex128)
-        insert_accumulate_kernel<double><<<(unsigned)items, kTileThreads, 0, st>>>((const double2*)image_rfft, rot,
-                                                                                  (double4*)acc, g, tiles);
-    else
-        insert_accumulate_kernel<float><<<(unsigned)items, kTileThreads, 0, st>>>((const float2*)image_rfft, rot,
-                                                                                 (float4*)acc, g, tiles);
-    return check_launch("insert_accumulate_kernel");
+    const size_t acc_bytes = (size_t)((int64_t)g.D * g.H * g.W) * (complex128 ? sizeof(double4) : sizeof(float4));
+    const int nphase = insert_phases(acc_bytes);
+    for (int ph = 0; ph < nphase; ph++) {
+        if (complex128)
+            insert_accumulate_kernel<double><<<(unsigned)items, kTileThreads, 0, st>>>(
+                (const double2*)image_rfft, rot, (double4*)acc, g, tiles, ph, nphase);
+        else
+            insert_accumulate_kernel<float><<<(unsigned)items, kTileThreads, 0, st>>>(
+                (const float2*)image_rfft, rot, (float4*)acc, g, tiles, ph, nphase);
+        if (int e = check_launch("insert_accumulate_kernel")) return e;
+    }
+    return TT_OK;
 }
 
 int launch_insert_finalize(const void* acc, int32_t complex128, int64_t channels, int64_t d, int64_t h, int64_t w,

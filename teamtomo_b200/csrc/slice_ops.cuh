@@ -270,6 +270,22 @@ __device__ __forceinline__ void cell_at(const float c[3], InsertCell& k) {
     k.ix1 = (int)ceilf(c[2]);
 }
 
+// z-phase of an insertion tile: the accumulator of a large volume is filled
+// in nphase passes, pass k taking the tiles whose centre point (after the
+// x' < 0 redirect) lies in the k-th z-slab, so each pass reduces into about
+// 1/nphase of the accumulator and more of its lines stay in L2.  Only the
+// order of the work changes: every tile belongs to exactly one pass.
+// (cy, cx): the tile's centre pixel.
+__device__ __forceinline__ int insert_tile_phase(const SliceGeom& g, const float* m, int cy, int cx, int nphase) {
+    const float qy = shifted_freq(cy, g.img_h, g.inv_h);
+    const float qx = __fmul_rn((float)cx, g.inv_w);
+    float p[3];
+    rotate_slice_point(m, qy, qx, p);
+    const float z = p[2] < 0.0f ? -p[0] : p[0];
+    const int ph = (int)floorf((z + 0.5f) * (float)nphase);
+    return ph < 0 ? 0 : (ph >= nphase ? nphase - 1 : ph);
+}
+
 // Insertion geometry and cell of slice frequency (qy, qx); false when the
 // point is outside the volume.
 __device__ __forceinline__ bool insert_cell(const SliceGeom& g, const float* m, float qy, float qx, bool& cj,
