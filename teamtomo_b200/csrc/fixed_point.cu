@@ -54,28 +54,29 @@ int launch_fixed_absmax(const void* data, int is_f64, int64_t count, uint32_t* a
     return check_launch("absmax_kernel");
 }
 
-// One block per (slice, tile), as insert_accumulate_kernel, in z-phases for
-// accumulators larger than the L2 (integer sums: bit-identical in any order).
+// One block per (slice, row of tiles), as insert_accumulate_kernel, in
+// z-phases for accumulators larger than the L2 (integer sums: bit-identical
+// in any order).
 template <typename R>
 __global__ void __launch_bounds__(kTileThreads)
 insert_fixed_kernel(const typename Acc<R>::C* __restrict__ img, const void* __restrict__ rot,
                     unsigned long long* __restrict__ acc, const uint32_t* __restrict__ absmax, int slices_log2,
-                    SliceGeom g, int tiles, int phase, int nphase) {
+                    SliceGeom g, int phase, int nphase) {
     __shared__ float m[9];
-    const int64_t s = blockIdx.x / tiles;
-    const int tile = blockIdx.x - (int)(s * tiles);
+    const int tx_tiles = tiles_x_of(g.wr);
+    const int rows = (g.img_h + kTileY - 1) / kTileY;
+    const int64_t s = blockIdx.x / rows;
+    const int ty = blockIdx.x - (int)(s * rows);
     if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
     __syncthreads();
-    if (nphase > 1) {  // the same answer in every thread: the whole block leaves
-        const int tx_tiles = tiles_x_of(g.wr);
-        const int ty = tile / tx_tiles, tx = tile - ty * tx_tiles;
-        if (insert_tile_phase(g, m, min(ty * kTileY + kTileY / 2, g.img_h - 1),
-                              min(tx * kTileX + kTileX / 2, g.wr - 1), nphase) != phase)
-            return;
-    }
     const FixedSplat sink{acc, fixed_data_scale(*absmax, slices_log2), fixed_weight_scale(slices_log2)};
-    int iy, ix;
-    if (tile_pixel(g, tile, iy, ix)) insert_point_to<R>(img, m, sink, g, s, iy, ix);
+    for (int tx = 0; tx < tx_tiles; tx++) {
+        if (nphase > 1 && insert_tile_phase(g, m, min(ty * kTileY + kTileY / 2, g.img_h - 1),
+                                            min(tx * kTileX + kTileX / 2, g.wr - 1), nphase) != phase)
+            continue;
+        int iy, ix;
+        if (tile_pixel(g, ty * tx_tiles + tx, iy, ix)) insert_point_to<R>(img, m, sink, g, s, iy, ix);
+    }
 }
 
 // Fixed-point accumulator -> (volume, weights), with the Friedel completion of
@@ -125,18 +126,17 @@ int insert_phases(size_t acc_bytes);  // insert.cu
 int launch_insert_fixed(const void* image_rfft, int32_t complex128, const void* rot, void* acc,
                         const uint32_t* absmax, int64_t max_slices, const tt_slice_params* p, cudaStream_t st) {
     SliceGeom g = make_geom(*p);
-    const int tiles = tiles_per_slice(g.img_h, g.wr);
-    const int64_t items = (int64_t)g.n * tiles;
+    const int64_t items = (int64_t)g.n * ((g.img_h + kTileY - 1) / kTileY);
     if (items > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert: too many blocks");
     const int l = ceil_log2(max_slices);
     const int nphase = insert_phases((size_t)((int64_t)g.D * g.H * g.W) * 4 * sizeof(long long));
     for (int ph = 0; ph < nphase; ph++) {
         if (complex128)
             insert_fixed_kernel<double><<<(unsigned)items, kTileThreads, 0, st>>>(
-                (const double2*)image_rfft, rot, (unsigned long long*)acc, absmax, l, g, tiles, ph, nphase);
+                (const double2*)image_rfft, rot, (unsigned long long*)acc, absmax, l, g, ph, nphase);
         else
             insert_fixed_kernel<float><<<(unsigned)items, kTileThreads, 0, st>>>(
-                (const float2*)image_rfft, rot, (unsigned long long*)acc, absmax, l, g, tiles, ph, nphase);
+                (const float2*)image_rfft, rot, (unsigned long long*)acc, absmax, l, g, ph, nphase);
         if (int e = check_launch("insert_fixed_kernel")) return e;
     }
     return TT_OK;

@@ -32,29 +32,32 @@
 
 namespace tt {
 
-// One block per (slice, tile).
+// One block per (slice, row of tiles): the block loads the rotation once and
+// walks the row, skipping the tiles of other z-phases (a few instructions
+// each, so extra phases cost almost nothing).
 template <typename R>
 __global__ void __launch_bounds__(kTileThreads)
 insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void* __restrict__ rot,
-                         typename Acc<R>::T* __restrict__ acc, SliceGeom g, int tiles, int phase, int nphase) {
+                         typename Acc<R>::T* __restrict__ acc, SliceGeom g, int phase, int nphase) {
     __shared__ float m[9];
-    const int64_t s = blockIdx.x / tiles;
-    const int tile = blockIdx.x - (int)(s * tiles);
+    const int tx_tiles = tiles_x_of(g.wr);
+    const int rows = (g.img_h + kTileY - 1) / kTileY;
+    const int64_t s = blockIdx.x / rows;
+    const int ty = blockIdx.x - (int)(s * rows);
     if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
     __syncthreads();
-    if (nphase > 1) {  // the same answer in every thread: the whole block leaves
-        const int tx_tiles = tiles_x_of(g.wr);
-        const int ty = tile / tx_tiles, tx = tile - ty * tx_tiles;
-        if (insert_tile_phase(g, m, min(ty * kTileY + kTileY / 2, g.img_h - 1),
-                              min(tx * kTileX + kTileX / 2, g.wr - 1), nphase) != phase)
-            return;
+    for (int tx = 0; tx < tx_tiles; tx++) {
+        // the same answer in every thread: the whole block skips the tile
+        if (nphase > 1 && insert_tile_phase(g, m, min(ty * kTileY + kTileY / 2, g.img_h - 1),
+                                            min(tx * kTileX + kTileX / 2, g.wr - 1), nphase) != phase)
+            continue;
+        int iy, ix;
+        const bool has_pixel = tile_pixel(g, ty * tx_tiles + tx, iy, ix);
+        if constexpr (std::is_same<R, float>::value)
+            insert_point_paired(img, m, acc, g, s, has_pixel, iy, ix);  // every lane takes part
+        else if (has_pixel)
+            insert_point<R>(img, m, acc, g, s, iy, ix);
     }
-    int iy, ix;
-    const bool has_pixel = tile_pixel(g, tile, iy, ix);
-    if constexpr (std::is_same<R, float>::value)
-        insert_point_paired(img, m, acc, g, s, has_pixel, iy, ix);  // every lane takes part
-    else if (has_pixel)
-        insert_point<R>(img, m, acc, g, s, iy, ix);
 }
 
 // Accumulator -> (volume, weights) with the Friedel completion of the x=0
@@ -196,8 +199,8 @@ static int check_insert_params(const tt_slice_params* p) {
 
 // Number of z-phases for an accumulator of acc_bytes: one per 1.1 x the L2
 // (at most 16).  Measured on a B200 (126 MB L2, 4096 slices): 320^3 (264 MB)
-// 7.57 -> 6.32 ms with 2 phases; 256^3 (135 MB) and 192^3 are 4-6 % slower
-// with 2 phases than with 1.
+// 7.70 -> 6.12 ms with 2 phases (6.05 with 3); 256^3 (135 MB) 3.79 ms with 1
+// phase, 3.81 with 2.
 int insert_phases(size_t acc_bytes) {
     int dev = 0, l2 = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess ||
@@ -212,18 +215,17 @@ int insert_phases(size_t acc_bytes) {
 int launch_insert_accumulate(const void* image_rfft, int32_t complex128, const void* rot, void* acc,
                              const tt_slice_params* p, cudaStream_t st) {
     SliceGeom g = make_geom(*p);
-    const int tiles = tiles_per_slice(g.img_h, g.wr);
-    const int64_t items = (int64_t)g.n * tiles;
+    const int64_t items = (int64_t)g.n * ((g.img_h + kTileY - 1) / kTileY);
     if (items > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert: too many blocks");
     const size_t acc_bytes = (size_t)((int64_t)g.D * g.H * g.W) * (complex128 ? sizeof(double4) : sizeof(float4));
     const int nphase = insert_phases(acc_bytes);
     for (int ph = 0; ph < nphase; ph++) {
         if (complex128)
             insert_accumulate_kernel<double><<<(unsigned)items, kTileThreads, 0, st>>>(
-                (const double2*)image_rfft, rot, (double4*)acc, g, tiles, ph, nphase);
+                (const double2*)image_rfft, rot, (double4*)acc, g, ph, nphase);
         else
             insert_accumulate_kernel<float><<<(unsigned)items, kTileThreads, 0, st>>>(
-                (const float2*)image_rfft, rot, (float4*)acc, g, tiles, ph, nphase);
+                (const float2*)image_rfft, rot, (float4*)acc, g, ph, nphase);
         if (int e = check_launch("insert_accumulate_kernel")) return e;
     }
     return TT_OK;
