@@ -36,32 +36,37 @@ __device__ __forceinline__ void load_rotation(float* sm, const void* rot, int64_
 }
 
 // VT: float2 (plain volume) or float4 (x-paired copy, tt_pack_volume_xpairs).
-// Eight resident blocks (32 registers, no spills): the gathers are latency-
-// bound at six (64 % warps active); full occupancy takes 8.5 % off the launch.
+// One block per (slice, row of tiles), eight resident blocks (32 registers):
+// the gathers are latency-bound at six (64 % warps active); full occupancy
+// takes 8.5 % off the launch, the row loop another 1 %.
 template <typename VT>
 __global__ void __launch_bounds__(kExtractThreads, 8)
 extract_fwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
                    float2* __restrict__ out, SliceGeom g, int tiles) {
     __shared__ float m[9];
-    const int64_t s = blockIdx.x / tiles;
-    const int tile = blockIdx.x - (int)(s * tiles);
+    const int tx_tiles = tiles_x_of(g.wr);
+    const int rows = tiles / tx_tiles;
+    const int64_t s = blockIdx.x / rows;
+    const int ty = blockIdx.x - (int)(s * rows);
     load_rotation(m, rot, s, g, true);
     __syncthreads();
-    int iy, ix;
-    if (!tile_pixel(g, tile, iy, ix)) return;
-    float qy, qx, c[3];
-    bool cj = false;
-    float2 r = make_float2(0.0f, 0.0f);
-    if (extract_geometry(g, m, iy, ix, qy, qx, cj, c)) {
-        r = sample_trilinear(vol, g, make_corners(g, c));
-        if (cj) r.y = -r.y;
+    for (int tx = 0; tx < tx_tiles; tx++) {
+        int iy, ix;
+        if (!tile_pixel(g, ty * tx_tiles + tx, iy, ix)) continue;
+        float qy, qx, c[3];
+        bool cj = false;
+        float2 r = make_float2(0.0f, 0.0f);
+        if (extract_geometry(g, m, iy, ix, qy, qx, cj, c)) {
+            r = sample_trilinear(vol, g, make_corners(g, c));
+            if (cj) r.y = -r.y;
+        }
+        // streaming store: the slices are written once and should not evict the volume from L2
+        __stcs(out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, r);
     }
-    // streaming store: the slices are written once and should not evict the volume from L2
-    __stcs(out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, r);
 }
 
-// Backward of one slice pixel; acc receives the pixel's 6 contributions to
-// d/dR_zyx.  Called by every lane of the warp (has_pixel false where the tile
+// Backward of one slice pixel; the pixel's 6 contributions to d/dR_zyx are
+// added to acc.  Called by every lane of the warp (has_pixel false where the tile
 // overhangs the slice): the float d/dvolume scatter pairs lanes across the warp.
 template <bool WANT_DV, bool WANT_DR, bool FIXED, typename VT>
 __device__ __forceinline__ void bwd_point(const VT* __restrict__ vol, const float* m,
@@ -162,9 +167,12 @@ __device__ __forceinline__ void mse_point(const VT* __restrict__ vol, const floa
     if (WANT_DV) scatter_dv_paired(dv.dvol, g, si, gv, valid);
 }
 
-// One block per (slice, tile).  WANT_DR: the block's partial sums of the 6
-// non-zero entries of d/dR_zyx go to part[(s * tiles + tile) * 6 + k]: warp
-// totals in float, then the eight warps in double, in a fixed order.  FIXED:
+// One block per (slice, row of tiles): the rotation is loaded and the
+// rotation-gradient partials reduced once per row.  WANT_DR: the row's sums of
+// the 6 non-zero entries of d/dR_zyx (per thread over its pixels, warp totals
+// in float, then the eight warps in double, in a fixed order) go to
+// part[(s * tiles + tile) * 6 + k] of the row's first tile, zeros to the
+// row's other tiles.  FIXED:
 // the volume gradient goes to the
 // fixed-point words `fixed` at the scale set by *absmax and n.  Resident
 // blocks: 6 for the rotation gradient alone (39 registers), 5 with the volume
@@ -177,16 +185,20 @@ extract_bwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
                    float* __restrict__ part, SliceGeom g, int tiles) {
     __shared__ float m[9];
     __shared__ double red[kExtractThreads / 32][6];
-    const int64_t s = blockIdx.x / tiles;
-    const int tile = blockIdx.x - (int)(s * tiles);
+    const int tx_tiles = tiles_x_of(g.wr);
+    const int rows = tiles / tx_tiles;
+    const int64_t s = blockIdx.x / rows;
+    const int ty = blockIdx.x - (int)(s * rows);
     load_rotation(m, rot, s, g, true);
     __syncthreads();
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     DvTarget<FIXED> dv{dvol, fixed, 0.0};
     if (FIXED) dv.scale = fixed_data_scale(*absmax, ceil_log2(g.n));
-    int iy, ix;
-    const bool has_pixel = tile_pixel(g, tile, iy, ix);
-    bwd_point<WANT_DV, WANT_DR, FIXED, VT>(vol, m, grad, dv, g, s, has_pixel, iy, ix, acc);
+    for (int tx = 0; tx < tx_tiles; tx++) {  // every lane runs every tile (the paired scatter shuffles)
+        int iy, ix;
+        const bool has_pixel = tile_pixel(g, ty * tx_tiles + tx, iy, ix);
+        bwd_point<WANT_DV, WANT_DR, FIXED, VT>(vol, m, grad, dv, g, s, has_pixel, iy, ix, acc);
+    }
     if (WANT_DR) {
         // warp totals in float (fixed order), then the warps in double
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -198,31 +210,39 @@ extract_bwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
             double v = 0.0;
 #pragma unroll
             for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][threadIdx.x];
-            part[((int64_t)s * tiles + tile) * 6 + threadIdx.x] = (float)v;
+            // the row's total in the slot of its first tile, zero in the others
+            const int64_t b0 = (int64_t)s * tiles + (int64_t)ty * tx_tiles;
+            part[b0 * 6 + threadIdx.x] = (float)v;
+            for (int tx = 1; tx < tx_tiles; tx++) part[(b0 + tx) * 6 + threadIdx.x] = 0.0f;
         }
     }
 }
 
-// Fused extraction + mean squared error + backward: one block per (slice,
-// tile).  Block partials of the loss (double) go to loss_part[s * tiles + tile]
-// and, with WANT_DR, those of d/dR_zyx to part[(s * tiles + tile) * 6 + k].
+// Fused extraction + mean squared error + backward: one block per (slice, row
+// of tiles).  The row's partials of the loss (double) go to
+// loss_part[s * tiles + tile] and, with WANT_DR, those of d/dR_zyx to
+// part[(s * tiles + tile) * 6 + k], for the row's first tile (zeros for the others).
 template <bool WANT_DV, bool WANT_DR, typename VT>
-__global__ void __launch_bounds__(kExtractThreads)
+__global__ void __launch_bounds__(kExtractThreads, 5)
 slice_mse_kernel(const VT* __restrict__ vol, const void* __restrict__ rot, const float2* __restrict__ target,
                  float2* __restrict__ dvol, float* __restrict__ part, double* __restrict__ loss_part, float scale,
                  SliceGeom g, int tiles) {
     __shared__ float m[9];
     __shared__ double red[kExtractThreads / 32][7];
-    const int64_t s = blockIdx.x / tiles;
-    const int tile = blockIdx.x - (int)(s * tiles);
+    const int tx_tiles = tiles_x_of(g.wr);
+    const int rows = tiles / tx_tiles;
+    const int64_t s = blockIdx.x / rows;
+    const int ty = blockIdx.x - (int)(s * rows);
     load_rotation(m, rot, s, g, true);
     __syncthreads();
     float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     double loss = 0.0;
     const DvTarget<false> dv{dvol, nullptr, 0.0};
-    int iy, ix;
-    const bool has_pixel = tile_pixel(g, tile, iy, ix);
-    mse_point<WANT_DV, WANT_DR, VT>(vol, m, target, dv, g, s, has_pixel, iy, ix, scale, acc, loss);
+    for (int tx = 0; tx < tx_tiles; tx++) {  // every lane runs every tile (the paired scatter shuffles)
+        int iy, ix;
+        const bool has_pixel = tile_pixel(g, ty * tx_tiles + tx, iy, ix);
+        mse_point<WANT_DV, WANT_DR, VT>(vol, m, target, dv, g, s, has_pixel, iy, ix, scale, acc, loss);
+    }
     // rotation-gradient warp totals in float (fixed order), the loss in double
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const float v8[8] = {acc[0], acc[1], acc[2], acc[3], acc[4], acc[5], 0.f, 0.f};
@@ -235,11 +255,15 @@ slice_mse_kernel(const VT* __restrict__ vol, const void* __restrict__ rot, const
         double v = 0.0;
 #pragma unroll
         for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][threadIdx.x];
-        const int64_t b = (int64_t)s * tiles + tile;
-        if (threadIdx.x == 6)
-            loss_part[b] = v;
-        else if (WANT_DR)
-            part[b * 6 + threadIdx.x] = (float)v;
+        // the row's totals in the slots of its first tile, zero in the others
+        const int64_t b0 = (int64_t)s * tiles + (int64_t)ty * tx_tiles;
+        if (threadIdx.x == 6) {
+            loss_part[b0] = v;
+            for (int tx = 1; tx < tx_tiles; tx++) loss_part[b0 + tx] = 0.0;
+        } else if (WANT_DR) {
+            part[b0 * 6 + threadIdx.x] = (float)v;
+            for (int tx = 1; tx < tx_tiles; tx++) part[(b0 + tx) * 6 + threadIdx.x] = 0.0f;
+        }
     }
 }
 
@@ -358,7 +382,7 @@ template <typename VT>
 static int launch_backward_t(const VT* v, const void* rot, const float2* gr, float2* dv, void* grad_rotation,
                              float* part, const SliceGeom& g, cudaStream_t st, void* fixed) {
     const int tiles = extract_tiles(g);
-    const unsigned blocks = (unsigned)((int64_t)g.n * tiles);
+    const unsigned blocks = (unsigned)((int64_t)g.n * (tiles / tiles_x_of(g.wr)));  // one block per row of tiles
     uint32_t* absmax = (uint32_t*)fixed;
     unsigned long long* facc = fixed ? (unsigned long long*)((char*)fixed + kFixedHeaderBytes) : nullptr;
     if (dv && fixed) {
@@ -469,7 +493,7 @@ extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotatio
     const float2* t = (const float2*)targets;
     float2* dv = (float2*)grad_volume;
     cudaStream_t st = as_stream(stream);
-    const unsigned nb = (unsigned)blocks;
+    const unsigned nb = (unsigned)((int64_t)g.n * (tiles / tiles_x_of(g.wr)));  // one block per row of tiles
     if (int e = g.vol_xpairs ? launch_mse((const float4*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part,
                                           loss_part, scale, g, tiles, nb, st)
                              : launch_mse((const float2*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part,
@@ -496,11 +520,12 @@ extern "C" int tt_extract_central_slices_rfft_3d(const void* volume_rfft, const 
     const int tiles = extract_tiles(g);
     const int64_t blocks = (int64_t)g.n * tiles;
     if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract: too many blocks");
+    const unsigned nb = (unsigned)((int64_t)g.n * (tiles / tiles_x_of(g.wr)));  // one block per row of tiles
     if (g.vol_xpairs)
-        extract_fwd_kernel<<<(unsigned)blocks, kExtractThreads, 0, as_stream(stream)>>>(
+        extract_fwd_kernel<<<nb, kExtractThreads, 0, as_stream(stream)>>>(
             (const float4*)volume_rfft, rotation_matrices, (float2*)slices_out, g, tiles);
     else
-        extract_fwd_kernel<<<(unsigned)blocks, kExtractThreads, 0, as_stream(stream)>>>(
+        extract_fwd_kernel<<<nb, kExtractThreads, 0, as_stream(stream)>>>(
             (const float2*)volume_rfft, rotation_matrices, (float2*)slices_out, g, tiles);
     return check_launch("extract_fwd_kernel");
 }

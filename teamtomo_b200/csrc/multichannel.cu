@@ -73,10 +73,7 @@ extract_multi_bwd_kernel(const float2* __restrict__ vol, int64_t vstride, int ch
                 if (WANT_DR) {
                     float2 v[2][2][2];
                     load_corners(vol + ch * vstride, g, k, v);
-                    float t[6];
-                    drot_terms(v, k, gv, cj, g, qy, qx, t);
-#pragma unroll
-                    for (int i = 0; i < 6; i++) acc[i] += t[i];
+                    drot_terms(v, k, gv, cj, g, qy, qx, acc);
                 }
             }
         }

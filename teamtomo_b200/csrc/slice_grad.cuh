@@ -100,9 +100,9 @@ __device__ __forceinline__ void load_corners(const VT* __restrict__ vol, const S
         }
 }
 
-// The pixel's 6 contributions to d/dR_zyx (rows z, y, x x columns y, x —
-// column 0 multiplies the zero z frequency of a central slice) from its
-// corner values: the trilinear gradient from differences of neighbouring
+// Adds the pixel's 6 contributions to d/dR_zyx (rows z, y, x x columns y, x —
+// column 0 multiplies the zero z frequency of a central slice) to acc, from
+// its corner values: the trilinear gradient from differences of neighbouring
 // voxels (subtracting first keeps it accurate where the volume varies
 // slowly), then Re(conj(G') dV/dc) chained through dc/dp and the redirect sign.
 __device__ __forceinline__ void drot_terms(const float2 v[2][2][2], const Corners& k, float2 gv, bool cj,
@@ -126,12 +126,12 @@ __device__ __forceinline__ void drot_terms(const float2 v[2][2][2], const Corner
     const float p0 = k.gz ? fmaf(gv.x, gz.x, gv.y * gz.y) * g.dcdp0 * sg : 0.0f;
     const float p1 = k.gy ? fmaf(gv.x, gy.x, gv.y * gy.y) * g.dcdp1 * sg : 0.0f;
     const float p2 = k.gx ? fmaf(gv.x, gx.x, gv.y * gx.y) * g.dcdp2 * sg : 0.0f;
-    acc[0] = p0 * qy;
-    acc[1] = p0 * qx;
-    acc[2] = p1 * qy;
-    acc[3] = p1 * qx;
-    acc[4] = p2 * qy;
-    acc[5] = p2 * qx;
+    acc[0] += p0 * qy;
+    acc[1] += p0 * qx;
+    acc[2] += p1 * qy;
+    acc[3] += p1 * qx;
+    acc[4] += p2 * qy;
+    acc[5] += p2 * qx;
 }
 
 // Launch of the fixed-order d/drotation reduction (extract.cu).
