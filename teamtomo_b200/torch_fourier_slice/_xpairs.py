@@ -8,20 +8,22 @@ limit of the extraction and of the rotation gradient.  Values and operation
 order are unchanged, so results are bit-identical to the plain layout.
 
 The copy costs one streaming pass over the volume (8 bytes read and 16
-written per voxel) and twice the volume's footprint in L2 while it is read.
-Measured on a B200 (4096 slices; plain -> x-paired):
+written per voxel, 0.05 ms at 256^3) and twice the volume's footprint in L2
+while it is read.  Measured on a B200 (4096 slices, 2048 at 320; plain ->
+x-paired, the pack not included):
 
-    box    copy     extraction   rotation gradient   fused MSE
-    128    17 MB    -4 %         -7.5 %              -5 %
-    192    57 MB    -1.7 %       -7.3 %              -4.5 %
-    256    135 MB   +8.7 %       -4 %                -1 %
+    box    copy     extraction   backward (dV + dR)   fused MSE
+    128    17 MB    -11 %        -6 %                 -12 %
+    192    57 MB    -12 %        -6.5 %               -13 %
+    256    135 MB   -8 %         -1.5 %               -5 %
+    320    264 MB   -8 %         +9.5 %               +6 %
 
-The forward gathers are L1-bound while the volume stays in L2; a copy larger
-than half the L2 turns them into L2 misses.  The gradient kernels (gathers
-plus a scatter, L1-bound at any size) gain everywhere.  Policy
-(``TT_VOLUME_XPAIRS`` = ``auto``, the default): pack when the call's slices
-hold at least two pixels per voxel, and for the forward extraction only when
-the copy fits in half the L2; ``1`` always packs, ``0`` never.
+The forward gathers (8 resident blocks per SM, L1-bound) gain at every size.
+The gradient kernels also scatter into d/dvolume: once the copy is larger
+than the L2, copy and gradient together miss L2 and the plain volume wins.
+Policy (``TT_VOLUME_XPAIRS`` = ``auto``, the default): pack when the call's
+slices hold at least two pixels per voxel, and for the gradient kernels only
+when the copy fits in 1.1 x the L2; ``1`` always packs, ``0`` never.
 """
 
 from __future__ import annotations
@@ -62,8 +64,8 @@ def use_xpairs(n_pixels: int, volume: torch.Tensor, purpose: str = "grad") -> bo
     if n_pixels < MIN_PIXELS_PER_VOXEL * volume.numel():
         return False
     if purpose == "forward":
-        return volume.is_cuda and 16 * volume.numel() <= l2_bytes(volume.device) // 2
-    return True
+        return True
+    return volume.is_cuda and 16 * volume.numel() <= 1.1 * l2_bytes(volume.device)
 
 
 def with_xpairs(params: _lib.SliceParams, flag: bool) -> _lib.SliceParams:

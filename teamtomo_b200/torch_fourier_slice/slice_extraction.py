@@ -47,8 +47,10 @@ class _ExtractCentralSlices(torch.autograd.Function):
             "extract_central_slices_rfft_3d",
         )
         ctx.params = params
-        # the backward reads the volume only for d/drotation: keep the copy for it
-        keep_xp = xp is not None and ctx.needs_input_grad[1]
+        # the backward reads the volume only for d/drotation: keep the copy for
+        # it when the gradient kernels gather faster from it
+        keep_xp = (xp is not None and ctx.needs_input_grad[1]
+                   and _xpairs.use_xpairs(out.numel(), volume_rfft, "grad"))
         ctx.has_xp = keep_xp
         ctx.save_for_backward(volume_rfft, rotation_matrices, *((xp,) if keep_xp else ()))
         return out

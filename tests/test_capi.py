@@ -91,15 +91,17 @@ def test_xpairs_policy(monkeypatch):
 
     vol = torch.zeros((16, 16, 9), dtype=torch.complex64)
     monkeypatch.delenv("TT_VOLUME_XPAIRS", raising=False)
-    assert _xpairs.use_xpairs(2 * vol.numel(), vol) and not _xpairs.use_xpairs(2 * vol.numel() - 1, vol)
+    assert _xpairs.use_xpairs(2 * vol.numel(), vol, "forward")
+    assert not _xpairs.use_xpairs(2 * vol.numel() - 1, vol, "forward")
     assert not _xpairs.use_xpairs(10**9, vol.to(torch.complex128))
-    assert not _xpairs.use_xpairs(10**9, vol, "forward")  # a CPU tensor: no L2 to fit
+    assert _xpairs.use_xpairs(10**9, vol, "forward")
+    assert not _xpairs.use_xpairs(10**9, vol, "grad")  # a CPU tensor: no L2 to fit in
     with pytest.raises(ValueError):
         _xpairs.use_xpairs(1, vol, "backward")
     monkeypatch.setenv("TT_VOLUME_XPAIRS", "0")
     assert not _xpairs.use_xpairs(10**9, vol)
     monkeypatch.setenv("TT_VOLUME_XPAIRS", "1")
-    assert _xpairs.use_xpairs(1, vol)
+    assert _xpairs.use_xpairs(1, vol) and _xpairs.use_xpairs(1, vol, "forward")
     from teamtomo_b200 import _lib
 
     p = _lib.SliceParams()

@@ -200,21 +200,16 @@ def test_full_size_headline_bitwise():
     assert torch.equal(dr0, dr1)
 
 
-def test_auto_policy_packs_for_the_gradient_only(monkeypatch):
-    """256^3 x 512 slices: the auto policy keeps the forward on the plain
-    volume (the copy would not fit in half the L2) and gives the rotation
-    gradient an x-paired copy; both results equal the plain path bitwise."""
+def _auto_run(monkeypatch, n, k, seed):
+    """Forward + backward (d/drotation) through the drop-in API under the auto
+    policy and with the plain volume; returns (results, number of packs)."""
     import teamtomo_b200 as tt
     from teamtomo_b200.torch_fourier_slice import _xpairs
 
-    n, k = 256, 512
-    vol = torch.as_tensor(rfft_volume_np(blob_volume(n, seed=470))).cuda()
-    npix = k * n * (n // 2 + 1)
-    monkeypatch.setenv("TT_VOLUME_XPAIRS", "auto")
-    assert not _xpairs.use_xpairs(npix, vol, "forward") and _xpairs.use_xpairs(npix, vol, "grad")
-    Rn = rotations(k, seed=471)
+    vol = torch.as_tensor(rfft_volume_np(blob_volume(n, seed=seed))).cuda()
+    Rn = rotations(k, seed=seed + 1)
     G = torch.randn((k, n, n // 2 + 1), dtype=torch.complex64, device="cuda",
-                    generator=torch.Generator(device="cuda").manual_seed(17))
+                    generator=torch.Generator(device="cuda").manual_seed(seed + 2))
     packs = []
     real_pack = _xpairs.pack
     monkeypatch.setattr(_xpairs, "pack", lambda v, p: packs.append(1) or real_pack(v, p))
@@ -225,5 +220,33 @@ def test_auto_policy_packs_for_the_gradient_only(monkeypatch):
         S = tt.extract_central_slices_rfft_3d(vol, (n, n, n), R)
         (S * G.conj()).real.sum().backward()
         res[mode] = (S.detach(), R.grad.detach())
-    assert len(packs) == 1  # the auto run's backward
+    return vol, res, len(packs)
+
+
+def test_auto_policy_shares_the_copy_with_the_backward(monkeypatch):
+    """256^3 x 512 slices: the forward gathers from an x-paired copy and the
+    backward reuses it (one pack); results equal the plain path bitwise."""
+    from teamtomo_b200.torch_fourier_slice import _xpairs
+
+    n, k = 256, 512
+    vol, res, packs = _auto_run(monkeypatch, n, k, 470)
+    npix = k * n * (n // 2 + 1)
+    monkeypatch.setenv("TT_VOLUME_XPAIRS", "auto")
+    assert _xpairs.use_xpairs(npix, vol, "forward") and _xpairs.use_xpairs(npix, vol, "grad")
+    assert packs == 1
+    assert torch.equal(res["auto"][0], res["0"][0]) and torch.equal(res["auto"][1], res["0"][1])
+
+
+def test_auto_policy_plain_backward_for_large_volumes(monkeypatch):
+    """320^3 x 700 slices (at least two pixels per voxel): the copy (264 MB) is
+    larger than the L2, so only the forward uses it and the backward reads the
+    plain volume; bitwise equal."""
+    from teamtomo_b200.torch_fourier_slice import _xpairs
+
+    n, k = 320, 700
+    vol, res, packs = _auto_run(monkeypatch, n, k, 480)
+    npix = k * n * (n // 2 + 1)
+    monkeypatch.setenv("TT_VOLUME_XPAIRS", "auto")
+    assert _xpairs.use_xpairs(npix, vol, "forward") and not _xpairs.use_xpairs(npix, vol, "grad")
+    assert packs == 1  # the forward's, not kept for the backward
     assert torch.equal(res["auto"][0], res["0"][0]) and torch.equal(res["auto"][1], res["0"][1])
