@@ -1,7 +1,8 @@
 // Central-slice extraction from an fftshifted rfft volume, and its backward.
 //
 // Forward (extract_central_slices_rfft_3d, _extract_central_slices_rfft_3d.py:84-222):
-// one thread per slice pixel, 8 x 32 pixel tiles per block.  The pixel's
+// one thread per slice pixel of an 8 x 32 tile, one block per row of tiles of
+// a slice.  The pixel's
 // frequency is generated in registers, rotated with the reference's float32
 // operation order, redirected into the stored half (conjugate rule with the
 // x-tolerance tie-break), scaled to array coordinates and sampled trilinearly
