@@ -19,11 +19,14 @@ x-paired, the pack not included):
     320    264 MB   -8 %         +9.5 %               +6 %
 
 The forward gathers (8 resident blocks per SM, L1-bound) gain at every size.
-The gradient kernels also scatter into d/dvolume: once the copy is larger
-than the L2, copy and gradient together miss L2 and the plain volume wins.
-Policy (``TT_VOLUME_XPAIRS`` = ``auto``, the default): pack when the call's
-slices hold at least two pixels per voxel, and for the gradient kernels only
-when the copy fits in 1.1 x the L2; ``1`` always packs, ``0`` never.
+The gradient kernels also scatter into d/dvolume: once copy and gradient no
+longer fit in L2 they gain little in isolation (256^3) or lose (320^3), and
+the extra DRAM traffic costs clock speed under the power cap in a full step
+(256^3 training step: 368K slices/s with the gradients on the plain volume at
+1965 MHz, 363K on the copy at 1890-1950 MHz).  Policy (``TT_VOLUME_XPAIRS``
+= ``auto``, the default): pack when the call's slices hold at least two
+pixels per voxel, and for the gradient kernels only when the copy fits in
+half the L2; ``1`` always packs, ``0`` never.
 """
 
 from __future__ import annotations
@@ -65,7 +68,7 @@ def use_xpairs(n_pixels: int, volume: torch.Tensor, purpose: str = "grad") -> bo
         return False
     if purpose == "forward":
         return True
-    return volume.is_cuda and 16 * volume.numel() <= 1.1 * l2_bytes(volume.device)
+    return volume.is_cuda and 16 * volume.numel() <= l2_bytes(volume.device) // 2
 
 
 def with_xpairs(params: _lib.SliceParams, flag: bool) -> _lib.SliceParams:

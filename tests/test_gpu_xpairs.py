@@ -224,11 +224,12 @@ def _auto_run(monkeypatch, n, k, seed):
 
 
 def test_auto_policy_shares_the_copy_with_the_backward(monkeypatch):
-    """256^3 x 512 slices: the forward gathers from an x-paired copy and the
-    backward reuses it (one pack); results equal the plain path bitwise."""
+    """192^3 x 400 slices: the forward gathers from an x-paired copy (57 MB)
+    and the backward reuses it (one pack); results equal the plain path
+    bitwise."""
     from teamtomo_b200.torch_fourier_slice import _xpairs
 
-    n, k = 256, 512
+    n, k = 192, 400
     vol, res, packs = _auto_run(monkeypatch, n, k, 470)
     npix = k * n * (n // 2 + 1)
     monkeypatch.setenv("TT_VOLUME_XPAIRS", "auto")
@@ -237,14 +238,14 @@ def test_auto_policy_shares_the_copy_with_the_backward(monkeypatch):
     assert torch.equal(res["auto"][0], res["0"][0]) and torch.equal(res["auto"][1], res["0"][1])
 
 
-def test_auto_policy_plain_backward_for_large_volumes(monkeypatch):
-    """320^3 x 700 slices (at least two pixels per voxel): the copy (264 MB) is
-    larger than the L2, so only the forward uses it and the backward reads the
-    plain volume; bitwise equal."""
+@pytest.mark.parametrize("n,k", [(256, 520), (320, 700)])
+def test_auto_policy_plain_backward_for_large_volumes(monkeypatch, n, k):
+    """At least two pixels per voxel, copy larger than half the L2 (135 MB at
+    256^3, 264 MB at 320^3): only the forward uses the copy and the backward
+    reads the plain volume; bitwise equal."""
     from teamtomo_b200.torch_fourier_slice import _xpairs
 
-    n, k = 320, 700
-    vol, res, packs = _auto_run(monkeypatch, n, k, 480)
+    vol, res, packs = _auto_run(monkeypatch, n, k, 480 + n)
     npix = k * n * (n // 2 + 1)
     monkeypatch.setenv("TT_VOLUME_XPAIRS", "auto")
     assert _xpairs.use_xpairs(npix, vol, "forward") and not _xpairs.use_xpairs(npix, vol, "grad")
