@@ -296,13 +296,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def xp_launches(n_pixels, volume, purposes=("forward", "grad")):
-    """1 when an extraction of n_pixels slice pixels (forward, or rotation
-    gradient / fused MSE) gathers from an x-paired copy of the volume (one
-    pack launch), else 0."""
+def xp_launches(n_pixels, volume):
+    """1 when an extraction of n_pixels slice pixels (its forward and backward,
+    or the fused MSE) gathers from an x-paired copy of the volume (one pack
+    launch), else 0."""
     from teamtomo_b200.torch_fourier_slice._xpairs import use_xpairs
 
-    return int(any(use_xpairs(n_pixels, volume, p) for p in purposes))
+    return int(use_xpairs(n_pixels, volume))
 
 
 def load_traffic():
@@ -544,7 +544,7 @@ def config_workload(args):
                     # insertion: splat, finalize, sum; fused MSE: loss kernel, loss and rotation finish
                     # (+ the x-paired copy of the volume)
                     "gpu_launches": n_img // chunk * 3
-                    + n_ext // chunk * (3 + xp_launches(chunk * n * (n // 2 + 1), Vfit, ("grad",)))})
+                    + n_ext // chunk * (3 + xp_launches(chunk * n * (n // 2 + 1), Vfit))})
     print(json.dumps(out))
     return 0
 

@@ -35,7 +35,7 @@ class _CentralSliceMSE(torch.autograd.Function):
         nbytes = int(L.tt_central_slice_mse_workspace_bytes(params))
         ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
         # large calls gather from an x-paired copy of the volume (bit-identical results)
-        xp = _xpairs.pack(volume_rfft, params) if _xpairs.use_xpairs(targets.numel(), volume_rfft, "grad") else None
+        xp = _xpairs.pack(volume_rfft, params) if _xpairs.use_xpairs(targets.numel(), volume_rfft) else None
         _lib.check(L.tt_central_slice_mse(_lib.ptr(xp if xp is not None else volume_rfft), _lib.ptr(R),
                                           _lib.ptr(targets), _lib.ptr(loss), _lib.ptr(dvol), _lib.ptr(drot),
                                           _lib.ptr(ws), nbytes, _xpairs.with_xpairs(params, xp is not None),

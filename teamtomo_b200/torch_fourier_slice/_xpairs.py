@@ -10,7 +10,7 @@ order are unchanged, so results are bit-identical to the plain layout.
 The copy costs one streaming pass over the volume (8 bytes read and 16
 written per voxel, 0.05 ms at 256^3) and twice the volume's footprint in L2
 while it is read.  Measured on a B200 (4096 slices, 2048 at 320; plain ->
-x-paired, the pack not included):
+x-paired, each kernel alone, the pack not included):
 
     box    copy     extraction   backward (dV + dR)   fused MSE
     128    17 MB    -11 %        -6 %                 -12 %
@@ -18,15 +18,14 @@ x-paired, the pack not included):
     256    135 MB   -8 %         -1.5 %               -5 %
     320    264 MB   -8 %         +9.5 %               +6 %
 
-The forward gathers (8 resident blocks per SM, L1-bound) gain at every size.
-The gradient kernels also scatter into d/dvolume: once copy and gradient no
-longer fit in L2 they gain little in isolation (256^3) or lose (320^3), and
-the extra DRAM traffic costs clock speed under the power cap in a full step
-(256^3 training step: 368K slices/s with the gradients on the plain volume at
-1965 MHz, 363K on the copy at 1890-1950 MHz).  Policy (``TT_VOLUME_XPAIRS``
-= ``auto``, the default): pack when the call's slices hold at least two
-pixels per voxel, and for the gradient kernels only when the copy fits in
-half the L2; ``1`` always packs, ``0`` never.
+Once the copy no longer fits in L2 its misses double the DRAM traffic of the
+gathers; in a full training step (extraction, backward, insertion at 256^3)
+that traffic slows the other kernels and pushes the GPU onto its power cap,
+and the step is as fast or faster without the copy (372.9K vs 371.7K
+slices/s).  Policy (``TT_VOLUME_XPAIRS`` = ``auto``, the default): gather
+from a copy when the call's slices hold at least two pixels per voxel and the
+copy fits in half the L2 (boxes up to about 192^3 on a B200); ``1`` always,
+``0`` never.
 """
 
 from __future__ import annotations
@@ -50,13 +49,15 @@ def l2_bytes(device: torch.device) -> int:
     return _l2_bytes[idx]
 
 
-def use_xpairs(n_pixels: int, volume: torch.Tensor, purpose: str = "grad") -> bool:
+def copy_budget(volume: torch.Tensor) -> int:
+    """Largest x-paired copy (bytes) worth making for ``volume``: half the L2
+    of its GPU (0 for a CPU tensor)."""
+    return l2_bytes(volume.device) // 2 if volume.is_cuda else 0
+
+
+def use_xpairs(n_pixels: int, volume: torch.Tensor) -> bool:
     """Whether a call sampling ``n_pixels`` slice pixels from ``volume``
-    (complex64, (d, h, w//2+1)) should gather from an x-paired copy.
-    ``purpose``: ``"forward"`` (the extraction's gathers alone) or ``"grad"``
-    (the rotation gradient and the fused MSE)."""
-    if purpose not in ("forward", "grad"):
-        raise ValueError(f"purpose must be 'forward' or 'grad', got {purpose!r}")
+    (complex64, (d, h, w//2+1)) should gather from an x-paired copy."""
     mode = os.environ.get("TT_VOLUME_XPAIRS", "auto").strip().lower()
     if mode in ("0", "off", "false", "no"):
         return False
@@ -64,11 +65,7 @@ def use_xpairs(n_pixels: int, volume: torch.Tensor, purpose: str = "grad") -> bo
         return False
     if mode in ("1", "on", "true", "yes"):
         return True
-    if n_pixels < MIN_PIXELS_PER_VOXEL * volume.numel():
-        return False
-    if purpose == "forward":
-        return True
-    return volume.is_cuda and 16 * volume.numel() <= l2_bytes(volume.device) // 2
+    return n_pixels >= MIN_PIXELS_PER_VOXEL * volume.numel() and 16 * volume.numel() <= copy_budget(volume)
 
 
 def with_xpairs(params: _lib.SliceParams, flag: bool) -> _lib.SliceParams:

@@ -37,8 +37,7 @@ class _ExtractCentralSlices(torch.autograd.Function):
         out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
         L = _lib.load()
         # large calls gather from an x-paired copy (bit-identical results)
-        xp = (_xpairs.pack(volume_rfft, params) if _xpairs.use_xpairs(out.numel(), volume_rfft, "forward")
-              else None)
+        xp = _xpairs.pack(volume_rfft, params) if _xpairs.use_xpairs(out.numel(), volume_rfft) else None
         _lib.check(
             L.tt_extract_central_slices_rfft_3d(_lib.ptr(xp if xp is not None else volume_rfft),
                                                 _lib.ptr(rotation_matrices), _lib.ptr(out),
@@ -47,10 +46,8 @@ class _ExtractCentralSlices(torch.autograd.Function):
             "extract_central_slices_rfft_3d",
         )
         ctx.params = params
-        # the backward reads the volume only for d/drotation: keep the copy for
-        # it when the gradient kernels gather faster from it
-        keep_xp = (xp is not None and ctx.needs_input_grad[1]
-                   and _xpairs.use_xpairs(out.numel(), volume_rfft, "grad"))
+        # the backward reads the volume only for d/drotation: keep the copy for it
+        keep_xp = xp is not None and ctx.needs_input_grad[1]
         ctx.has_xp = keep_xp
         ctx.save_for_backward(volume_rfft, rotation_matrices, *((xp,) if keep_xp else ()))
         return out
@@ -63,8 +60,8 @@ class _ExtractCentralSlices(torch.autograd.Function):
         dvol = drot = None
         if want_v or want_r:
             xp = saved[2] if ctx.has_xp else None
-            # the rotation gradient's gathers read the x-paired copy at any volume size
-            if xp is None and want_r and _xpairs.use_xpairs(grad.numel(), volume_rfft, "grad"):
+            # direct calls of the backward alone (no forward copy) make their own
+            if xp is None and want_r and _xpairs.use_xpairs(grad.numel(), volume_rfft):
                 xp = _xpairs.pack(volume_rfft, ctx.params)
             dvol, drot = extract_backward(volume_rfft, rotation_matrices, grad, ctx.params,
                                           want_v, want_r, xpairs=xp)

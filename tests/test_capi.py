@@ -91,17 +91,18 @@ def test_xpairs_policy(monkeypatch):
 
     vol = torch.zeros((16, 16, 9), dtype=torch.complex64)
     monkeypatch.delenv("TT_VOLUME_XPAIRS", raising=False)
-    assert _xpairs.use_xpairs(2 * vol.numel(), vol, "forward")
-    assert not _xpairs.use_xpairs(2 * vol.numel() - 1, vol, "forward")
+    assert _xpairs.copy_budget(vol) == 0  # a CPU tensor: no L2 to fit in
+    assert not _xpairs.use_xpairs(10**9, vol)
+    monkeypatch.setattr(_xpairs, "copy_budget", lambda v: 16 * v.numel())
+    assert _xpairs.use_xpairs(2 * vol.numel(), vol) and not _xpairs.use_xpairs(2 * vol.numel() - 1, vol)
     assert not _xpairs.use_xpairs(10**9, vol.to(torch.complex128))
-    assert _xpairs.use_xpairs(10**9, vol, "forward")
-    assert not _xpairs.use_xpairs(10**9, vol, "grad")  # a CPU tensor: no L2 to fit in
-    with pytest.raises(ValueError):
-        _xpairs.use_xpairs(1, vol, "backward")
+    monkeypatch.setattr(_xpairs, "copy_budget", lambda v: 16 * v.numel() - 1)
+    assert not _xpairs.use_xpairs(10**9, vol)
     monkeypatch.setenv("TT_VOLUME_XPAIRS", "0")
+    monkeypatch.setattr(_xpairs, "copy_budget", lambda v: 1 << 40)
     assert not _xpairs.use_xpairs(10**9, vol)
     monkeypatch.setenv("TT_VOLUME_XPAIRS", "1")
-    assert _xpairs.use_xpairs(1, vol) and _xpairs.use_xpairs(1, vol, "forward")
+    assert _xpairs.use_xpairs(1, vol)
     from teamtomo_b200 import _lib
 
     p = _lib.SliceParams()

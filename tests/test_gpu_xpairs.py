@@ -233,21 +233,21 @@ def test_auto_policy_shares_the_copy_with_the_backward(monkeypatch):
     vol, res, packs = _auto_run(monkeypatch, n, k, 470)
     npix = k * n * (n // 2 + 1)
     monkeypatch.setenv("TT_VOLUME_XPAIRS", "auto")
-    assert _xpairs.use_xpairs(npix, vol, "forward") and _xpairs.use_xpairs(npix, vol, "grad")
+    assert _xpairs.use_xpairs(npix, vol)
     assert packs == 1
     assert torch.equal(res["auto"][0], res["0"][0]) and torch.equal(res["auto"][1], res["0"][1])
 
 
 @pytest.mark.parametrize("n,k", [(256, 520), (320, 700)])
-def test_auto_policy_plain_backward_for_large_volumes(monkeypatch, n, k):
-    """At least two pixels per voxel, copy larger than half the L2 (135 MB at
-    256^3, 264 MB at 320^3): only the forward uses the copy and the backward
-    reads the plain volume; bitwise equal."""
+def test_auto_policy_plain_volume_for_large_boxes(monkeypatch, n, k):
+    """At least two pixels per voxel, but a copy larger than half the L2 (135 MB
+    at 256^3, 264 MB at 320^3): forward and backward read the plain volume; the
+    results equal the forced plain path bitwise."""
     from teamtomo_b200.torch_fourier_slice import _xpairs
 
     vol, res, packs = _auto_run(monkeypatch, n, k, 480 + n)
     npix = k * n * (n // 2 + 1)
     monkeypatch.setenv("TT_VOLUME_XPAIRS", "auto")
-    assert _xpairs.use_xpairs(npix, vol, "forward") and not _xpairs.use_xpairs(npix, vol, "grad")
-    assert packs == 1  # the forward's, not kept for the backward
+    assert not _xpairs.use_xpairs(npix, vol)
+    assert packs == 0
     assert torch.equal(res["auto"][0], res["0"][0]) and torch.equal(res["auto"][1], res["0"][1])
