@@ -91,7 +91,7 @@ __device__ __forceinline__ void bwd_point(const VT* __restrict__ vol, const floa
     }
     if (WANT_DV) {
         if (FIXED) {
-            if (valid) scatter_dv(dv, g, k, gv);
+            scatter_dv_fixed_paired(dv.fixed, dv.scale, g, si, gv, valid);
         } else {
             scatter_dv_paired(dv.dvol, g, si, gv, valid);
         }

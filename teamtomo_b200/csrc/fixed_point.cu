@@ -54,6 +54,64 @@ int launch_fixed_absmax(const void* data, int is_f64, int64_t count, uint32_t* a
     return check_launch("absmax_kernel");
 }
 
+// Fixed-point splat of one complex64 source pixel with lane pairs: lanes 2j
+// and 2j+1 take the same pixel (pixels j and j + 16 in two rounds); per row of
+// the cell they add (re | im) of the x-low corner, (w | w) of the two corners
+// and (re | im) of the x-high corner, so an instruction's two words share a
+// 32-byte voxel slot or lie in adjacent ones: 4 sector operations per row
+// where one word per lane takes 6.  Same corners, weights ((fz * fy) * fx) and
+// rounded integers as the FixedSplat path.  Must be called by all 32 lanes of
+// the warp (has_pixel false where the tile overhangs the slice).
+__device__ __forceinline__ void insert_point_fixed_paired(const float2* __restrict__ img, const float* m,
+                                                          unsigned long long* __restrict__ acc, double sd, double sw,
+                                                          const SliceGeom& g, int64_t s, bool has_pixel, int iy,
+                                                          int ix) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, odd = lane & 1;
+    float dre = 0.f, dim = 0.f;
+    float c[3] = {-1.f, 0.f, 0.f};  // c[0] < 0: no point
+    if (has_pixel) {
+        const float qy = shifted_freq(iy, g.img_h, g.inv_h);
+        const float qx = __fmul_rn((float)ix, g.inv_w);
+        if (insert_pixel_kept(g, qy, qx)) {
+            const float2 d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+            bool cj;
+            float ci[3];
+            if (insert_coords(g, m, qy, qx, cj, ci)) {
+                dre = d.x;
+                dim = cj ? -d.y : d.y;
+                c[0] = ci[0];
+                c[1] = ci[1];
+                c[2] = ci[2];
+            }
+        }
+    }
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        const int src = (lane >> 1) + 16 * half;
+        const float sre = __shfl_sync(full, dre, src), sim = __shfl_sync(full, dim, src);
+        float sc[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) sc[a] = __shfl_sync(full, c[a], src);
+        if (sc[0] < 0.0f) continue;
+        InsertCell k;
+        cell_at(sc, k);
+        const double sv = (double)(odd ? sim : sre);
+#pragma unroll
+        for (int zy = 0; zy < 4; zy++) {
+            const int bz = zy >> 1, by = zy & 1;
+            const float wzy = (bz ? k.tz : 1.0f - k.tz) * (by ? k.ty : 1.0f - k.ty);
+            const float w0 = wzy * (1.0f - k.tx), w1 = wzy * k.tx;
+            const int z = bz ? k.iz1 : k.iz0, y = by ? k.iy1 : k.iy0;
+            const int64_t v0 = vox_index(g, z, y, k.ix0), v1 = vox_index(g, z, y, k.ix1);
+            if (w0 != 0.0f) fixed_add(acc + v0 * 4 + odd, sv * (double)w0 * sd);
+            const float wc = odd ? w1 : w0;
+            if (wc != 0.0f) fixed_add(acc + (odd ? v1 : v0) * 4 + 2, (double)wc * 1.0 * sw);
+            if (w1 != 0.0f) fixed_add(acc + v1 * 4 + odd, sv * (double)w1 * sd);
+        }
+    }
+}
+
 // One block per (slice, row of tiles), as insert_accumulate_kernel, in
 // z-phases for accumulators larger than the L2 (integer sums: bit-identical
 // in any order).
@@ -75,7 +133,11 @@ insert_fixed_kernel(const typename Acc<R>::C* __restrict__ img, const void* __re
                                             min(tx * kTileX + kTileX / 2, g.wr - 1), nphase) != phase)
             continue;
         int iy, ix;
-        if (tile_pixel(g, ty * tx_tiles + tx, iy, ix)) insert_point_to<R>(img, m, sink, g, s, iy, ix);
+        const bool has_pixel = tile_pixel(g, ty * tx_tiles + tx, iy, ix);
+        if constexpr (sizeof(R) == 4)
+            insert_point_fixed_paired(img, m, acc, sink.sd, sink.sw, g, s, has_pixel, iy, ix);  // every lane
+        else if (has_pixel)
+            insert_point_to<R>(img, m, sink, g, s, iy, ix);
     }
 }
 

@@ -85,6 +85,42 @@ __device__ __forceinline__ void scatter_dv_paired(float2* __restrict__ dvol, con
     }
 }
 
+// Fixed-point d/dvolume scatter with lane pairs: lanes 2j and 2j+1 take the
+// same pixel (pixels j and j + 16 in two rounds) and add the re and the im
+// word of each corner in the same instruction — one 16-byte voxel slot, one
+// L2 sector, where scatter_dv spends two.  Same corners, weights and rounded
+// integers as scatter_dv (integer sums do not depend on who adds them).  Must
+// be called by all 32 lanes of the warp (valid = false for lanes without a pixel).
+__device__ __forceinline__ void scatter_dv_fixed_paired(unsigned long long* __restrict__ fixed, double scale,
+                                                        const SliceGeom& g, const SourceIdx& si, float2 gv,
+                                                        bool valid) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, odd = lane & 1;
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        const int src = (lane >> 1) + 16 * half;
+        const float sgx = __shfl_sync(full, gv.x, src), sgy = __shfl_sync(full, gv.y, src);
+        const float siz = __shfl_sync(full, valid ? si.z : -1.0f, src);  // < 0: no pixel
+        const float siy = __shfl_sync(full, si.y, src), six = __shfl_sync(full, si.x, src);
+        if (siz < 0.0f) continue;
+        const Corners k = corners_at(g, siz, siy, six);
+        const double sv = (double)(odd ? sgy : sgx);
+#pragma unroll
+        for (int zy = 0; zy < 4; zy++) {
+            const int bz = zy >> 1, by = zy & 1;
+            if ((bz && !k.zin) || (by && !k.yin)) continue;
+            const float wzy = (by ? k.ay1 : k.ay0) * (bz ? k.az1 : k.az0);
+            const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
+#pragma unroll
+            for (int bx = 0; bx < 2; bx++) {
+                if (bx && !k.xin) continue;
+                const float w = (bx ? k.ax1 : k.ax0) * wzy;
+                if (w != 0.0f) fixed_add(fixed + 2 * (base + bx) + odd, sv * (double)w * scale);
+            }
+        }
+    }
+}
+
 // The eight corner values of a pixel; corners past the last index read as
 // zero, as in grid_sample.  VT: float2 (plain layout) or float4 (x-paired).
 template <typename VT>
