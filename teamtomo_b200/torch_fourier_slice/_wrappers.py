@@ -49,13 +49,11 @@ def irfftn_last(x: torch.Tensor, ndim: int) -> torch.Tensor:
     volumes) are not exactly Hermitian, and for such inputs cuFFT's
     multi-dimensional complex-to-real transform differs from the CPU result
     by ~1e-4; this form matches it."""
-    if ndim > 1:
-        x = torch.fft.ifftn(x, dim=tuple(range(-ndim, -1)))
-    m = x.shape[-1]
-    keep = torch.ones(m, dtype=x.real.dtype, device=x.device)
-    keep[0] = 0
-    keep[m - 1] = 0  # the Nyquist bin of the default (even) output length
-    x = torch.complex(x.real, x.imag * keep)
+    # a fresh tensor either way: the caller's input is never modified
+    x = torch.fft.ifftn(x, dim=tuple(range(-ndim, -1))) if ndim > 1 else x.clone()
+    xr = torch.view_as_real(x)
+    xr[..., 0, 1].zero_()
+    xr[..., -1, 1].zero_()  # the Nyquist bin of the default (even) output length
     return torch.fft.irfft(x, dim=-1)
 
 
