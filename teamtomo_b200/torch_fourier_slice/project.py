@@ -54,7 +54,8 @@ class _ProjectionGraph:
                 _project_eager(self.volume, self.R, **kwargs)
         torch.cuda.current_stream(volume.device).wait_stream(side)
         self.graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.graph):
+        # thread-local: CUDA calls other threads make meanwhile are not part of the capture
+        with torch.cuda.graph(self.graph, capture_error_mode="thread_local"):
             self.out = _project_eager(self.volume, self.R, **kwargs)
         self.done = None  # event after the last replay's output copy
 
