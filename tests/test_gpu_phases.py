@@ -58,3 +58,17 @@ def test_phased_batched_ctf_insertion_equals_single_volume():
     vs, ws = tt().insert_central_slices_rfft_3d(imgs, (n, n, n), R)
     assert rel_l2(vp.cpu().numpy(), vs.cpu().numpy()) < 1e-6
     assert rel_l2(wp.cpu().numpy(), ws.cpu().numpy()) < 1e-6
+
+
+def test_phased_complex128_insertion_matches_oracle(oracle):
+    """complex128 images fill a 32-byte-slot accumulator (527 MB at 320^3: four
+    z-phases); values and float64 weights equal the oracle's."""
+    n, k = 320, 24
+    g = torch.Generator(device="cuda").manual_seed(17)
+    imgs = torch.randn((k, n, n // 2 + 1), dtype=torch.complex128, device="cuda", generator=g)
+    R = torch.as_tensor(rotations(k, seed=18)).float().cuda()
+    vol, w = tt().insert_central_slices_rfft_3d(imgs, (n, n, n), R)
+    assert vol.dtype == torch.complex128 and w.dtype == torch.float64
+    rv, rw = oracle.insert(imgs.cpu().numpy(), (n, n, n), R.cpu().numpy(), nthreads=8)
+    assert rel_l2(vol.cpu().numpy(), rv) < 1e-10
+    assert rel_l2(w.cpu().numpy(), rw) < 1e-10
