@@ -327,8 +327,9 @@ int tt_extract_central_slices_rfft_3d_multichannel_backward(
     const void *grad_slices, void *grad_volume, void *grad_rotation, void *workspace,
     size_t workspace_bytes, const tt_slice_params *p, void *stream);
 /* Splat of (n, channels, h, w/2+1) complex64 slices into `channels` caller-zeroed
- * float accumulators (tt_insert_accumulator_bytes(0, channels, ...)); the
- * interpolation weights go to channel 0, which tt_insert_finalize reads. */
+ * float accumulators (tt_insert_accumulator_bytes(0, channels, ...)), one
+ * channel after the other; every channel's slots also receive the
+ * interpolation weights, and tt_insert_finalize reads them from channel 0. */
 int tt_insert_accumulate_multichannel(const void *image_rfft, int64_t channels,
                                       const void *rotation_matrices, void *accumulator,
                                       const tt_slice_params *p, void *stream);

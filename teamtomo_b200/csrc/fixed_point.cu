@@ -74,7 +74,7 @@ __device__ __forceinline__ void insert_point_fixed_paired(const float2* __restri
         const float qy = shifted_freq(iy, g.img_h, g.inv_h);
         const float qx = __fmul_rn((float)ix, g.inv_w);
         if (insert_pixel_kept(g, qy, qx)) {
-            const float2 d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+            const float2 d = load_slice(img + (s * g.slice_rows + slice_row(g, iy)) * (int64_t)g.wr + ix);
             bool cj;
             float ci[3];
             if (insert_coords(g, m, qy, qx, cj, ci)) {

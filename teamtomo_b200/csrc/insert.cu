@@ -231,6 +231,30 @@ int launch_insert_accumulate(const void* image_rfft, int32_t complex128, const v
     return TT_OK;
 }
 
+// Channel-interleaved images (n, c, h, w/2+1) into c float accumulators: the
+// single-channel splat once per channel (storage rows per slice: c * h), so
+// each pass reduces into one accumulator with the paired lanes and z-phases
+// of the single-channel path.  Splatting all channels from one geometry pass
+// reduced into c accumulators at once and was slower: 2.85 vs 1.97 ms for 2
+// channels, 6.52 vs 3.93 ms for 4 (256^3, 1024 slices).  Every channel gets
+// the weights; readers take them from channel 0.
+int launch_insert_accumulate_channels(const float2* img, int64_t channels, const void* rot, float4* acc,
+                                      const tt_slice_params* p, cudaStream_t st) {
+    SliceGeom g = make_geom(*p);
+    g.slice_rows = (int)(channels * g.img_h);
+    const int64_t items = (int64_t)g.n * ((g.img_h + kTileY - 1) / kTileY);
+    if (items > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert multichannel: too many blocks");
+    const int64_t vox = (int64_t)g.D * g.H * g.W;
+    const int nphase = insert_phases((size_t)vox * sizeof(float4));
+    for (int64_t ch = 0; ch < channels; ch++)
+        for (int ph = 0; ph < nphase; ph++) {
+            insert_accumulate_kernel<float><<<(unsigned)items, kTileThreads, 0, st>>>(
+                img + ch * (int64_t)g.img_h * g.wr, rot, acc + ch * vox, g, ph, nphase);
+            if (int e = check_launch("insert_accumulate_kernel")) return e;
+        }
+    return TT_OK;
+}
+
 int launch_insert_finalize(const void* acc, int32_t complex128, int64_t channels, int64_t d, int64_t h, int64_t w,
                            void* volume, void* weights, cudaStream_t st) {
     const int64_t total = channels * d * h * w;

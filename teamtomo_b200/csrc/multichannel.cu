@@ -94,38 +94,6 @@ extract_multi_bwd_kernel(const float2* __restrict__ vol, int64_t vstride, int ch
     }
 }
 
-// Insertion splat of all channels: the data of channel ch go to accumulator
-// ch; the interpolation weight is added to channel 0 only.
-__global__ void __launch_bounds__(kTileThreads)
-insert_multi_kernel(const float2* __restrict__ img, int channels, const void* __restrict__ rot,
-                    float4* __restrict__ acc, int64_t vstride, SliceGeom g, int tiles) {
-    __shared__ float m[9];
-    const int64_t s = blockIdx.x / tiles;
-    const int tile = blockIdx.x - (int)(s * tiles);
-    if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
-    __syncthreads();
-    int iy, ix;
-    if (!tile_pixel(g, tile, iy, ix)) return;
-    const float qy = shifted_freq(iy, g.img_h, g.inv_h);
-    const float qx = __fmul_rn((float)ix, g.inv_w);
-    bool cj;
-    InsertCell k;
-    if (!insert_pixel_kept(g, qy, qx) || !insert_cell(g, m, qy, qx, cj, k)) return;
-    for (int ch = 0; ch < channels; ch++) {
-        const float2 d = __ldcs(img + chan_pixel(g, s, ch, channels, iy, ix));
-        const float dim = cj ? -d.y : d.y;
-        float4* a = acc + ch * vstride;
-#pragma unroll
-        for (int corner = 0; corner < 8; corner++) {
-            const float w = insert_corner_weight(k, corner);
-            if (w == 0.0f) continue;
-            int z, y, x;
-            insert_corner_zyx(k, corner, z, y, x);
-            acc_add(a + vox_index(g, z, y, x), d.x * w, dim * w, ch == 0 ? w : 0.0f);
-        }
-    }
-}
-
 // Insertion backward of all channels: gather adjoint per channel with the
 // shared geometry.
 __global__ void __launch_bounds__(kTileThreads)
@@ -239,6 +207,11 @@ extern "C" int tt_extract_central_slices_rfft_3d_multichannel_backward(
     return TT_OK;
 }
 
+namespace tt {
+int launch_insert_accumulate_channels(const float2* img, int64_t channels, const void* rot, float4* acc,
+                                      const tt_slice_params* p, cudaStream_t st);  // insert.cu
+}  // namespace tt
+
 extern "C" int tt_insert_accumulate_multichannel(const void* image_rfft, int64_t channels,
                                                  const void* rotation_matrices, void* accumulator,
                                                  const tt_slice_params* p, void* stream) {
@@ -252,14 +225,9 @@ extern "C" int tt_insert_accumulate_multichannel(const void* image_rfft, int64_t
     if (p->n == 0) return TT_OK;
     if (!image_rfft || !rotation_matrices || !accumulator)
         return fail(TT_ERR_INVALID, "insert multichannel: NULL pointer argument");
-    SliceGeom g = make_geom(*p);
-    int tiles;
-    int64_t blocks;
-    if (int e = multi_blocks(g, tiles, blocks, "insert multichannel")) return e;
-    const int64_t vstride = p->vol_d * p->vol_h * p->vol_w;
-    insert_multi_kernel<<<(unsigned)blocks, kTileThreads, 0, as_stream(stream)>>>(
-        (const float2*)image_rfft, (int)channels, rotation_matrices, (float4*)accumulator, vstride, g, tiles);
-    return check_launch("insert_multi_kernel");
+    if (channels * p->img_h > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert multichannel: too many rows");
+    return launch_insert_accumulate_channels((const float2*)image_rfft, channels, rotation_matrices,
+                                             (float4*)accumulator, p, as_stream(stream));
 }
 
 extern "C" int tt_insert_central_slices_rfft_3d_multichannel_backward(const void* grad_volume, int64_t channels,

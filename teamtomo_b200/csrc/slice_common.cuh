@@ -35,6 +35,8 @@ struct SliceGeom {
     int vol_unshifted;             // volume is the plain rfftn output (no fftshift of z, y)
     int slice_unshifted;           // slices are stored ifftshifted along rows (irfft-ready)
     int vol_xpairs;                // volume is the x-paired copy (float4 per voxel)
+    int slice_rows;                // storage rows per slice of the insertion's images
+                                   // (img_h; channels * img_h for channel-interleaved stacks)
     float dcdp0, dcdp1, dcdp2;     // d(array coord)/d(frequency) per axis
 };
 
@@ -70,6 +72,7 @@ __host__ inline SliceGeom make_geom(const tt_slice_params& p) {
     g.vol_unshifted = p.volume_unshifted;
     g.slice_unshifted = p.slices_unshifted;
     g.vol_xpairs = p.volume_xpairs;
+    g.slice_rows = (int)p.img_h;
     g.dcdp0 = g.s0 / g.iw0;
     g.dcdp1 = g.s1 / g.iw1;
     g.dcdp2 = 2.0f * g.sx;

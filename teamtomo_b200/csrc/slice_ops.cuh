@@ -330,7 +330,7 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
     const float qx = __fmul_rn((float)ix, g.inv_w);
     if (!insert_pixel_kept(g, qy, qx)) return;
     // issued before the geometry so the load overlaps it
-    const typename Acc<R>::C d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+    const typename Acc<R>::C d = load_slice(img + (s * g.slice_rows + slice_row(g, iy)) * (int64_t)g.wr + ix);
     bool cj;
     InsertCell k;
     if (!insert_cell(g, m, qy, qx, cj, k)) return;
@@ -372,7 +372,7 @@ __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ i
         const float qy = shifted_freq(iy, g.img_h, g.inv_h);
         const float qx = __fmul_rn((float)ix, g.inv_w);
         if (insert_pixel_kept(g, qy, qx)) {
-            const float2 d = load_slice(img + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
+            const float2 d = load_slice(img + (s * g.slice_rows + slice_row(g, iy)) * (int64_t)g.wr + ix);
             bool cj;
             float ci[3];
             if (insert_coords(g, m, qy, qx, cj, ci)) {

@@ -191,7 +191,8 @@ def insert_backward(grad_volume, R, volume_shape, fftfreq_max=None, zyx_matrices
 def insert_accumulate_multichannel(images, R, volume_shape, acc, fftfreq_max=None, zyx_matrices=False,
                                    images_unshifted=False):
     """Add the splat of (n, c, h, w//2+1) complex64 slices into c float
-    accumulators (c, d, h, w//2+1, 4) — weights in channel 0."""
+    accumulators (c, d, h, w//2+1, 4), one channel after the other (readers
+    take the weights from channel 0)."""
     if not (images.is_contiguous() and R.is_contiguous() and acc.is_contiguous()):
         raise ValueError("insertion needs C-contiguous slices, rotations and accumulator")
     params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=None, rotation=R,
