@@ -25,6 +25,20 @@ def _pad_amount(n: int, pad_factor: float) -> int:
     return int((n * (pad_factor - 1.0)) // 2)
 
 
+# float64 volumes: the padding, sinc^2 weighting and 3D rfft run in float64,
+# the central slices are sampled from the complex64 rounding of that rfft (the
+# extraction kernels sample complex64) and the projections are returned as
+# float64, the dtype the reference returns for them.
+def _slice_source(dft: torch.Tensor) -> torch.Tensor:
+    if dft.dtype == torch.complex128:
+        dft = dft.to(torch.complex64)
+    return dft.contiguous()
+
+
+def _out_dtype(volume: torch.Tensor) -> torch.dtype:
+    return torch.float64 if volume.dtype == torch.float64 else torch.float32
+
+
 # CUDA-graph replay of small projections.  A projection of a small volume is
 # a chain of about ten short kernels (the padding / sinc^2 pass, the 3D rfft,
 # the extraction, the 2D inverse FFTs, the crop) whose host-side launch cost
@@ -93,8 +107,9 @@ def project_3d_to_2d(
 ) -> torch.Tensor:
     """Project a cubic volume by sampling central slices through its DFT.
 
-    ``volume`` (d, d, d) float32; ``rotation_matrices`` (..., 3, 3); returns
-    (..., d, d) projections.  Differentiable w.r.t. volume and rotations."""
+    ``volume`` (d, d, d) float32 or float64; ``rotation_matrices`` (..., 3, 3);
+    returns (..., d, d) projections in the volume's dtype (float64 volumes are
+    sampled in single precision).  Differentiable w.r.t. volume and rotations."""
     d, h, w = volume.shape[-3:]
     if len({d, h, w}) != 1:
         raise ValueError("all dimensions of volume must be equal.")
@@ -126,7 +141,7 @@ def _project_eager(volume, rotation_matrices, pad_factor, fftfreq_max, zyx_matri
     shape = (n_pad, n_pad, n_pad)
     fft_in = _wrappers.project_prepare(volume, p)  # padded * sinc^2, fftshifted
     # unshifted rfft; cuFFT may hand back a non-contiguous layout
-    dft = torch.fft.rfftn(fft_in, dim=(-3, -2, -1)).contiguous()
+    dft = _slice_source(torch.fft.rfftn(fft_in, dim=(-3, -2, -1)))
     R, stack = rotation_arg(rotation_matrices, volume.device)
     params = slice_params(n=R.shape[0], image_shape=shape, volume=dft, rotation=R,
                           fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
@@ -135,7 +150,7 @@ def _project_eager(volume, rotation_matrices, pad_factor, fftfreq_max, zyx_matri
     # irfftn without an output size, as the reference: an odd padded box
     # gives images one column narrower (2 * (n_pad // 2) wide)
     images = _wrappers.irfftn_last(slices, 2)
-    out = _wrappers.recentre_crop_2d(images, p)
+    out = _wrappers.recentre_crop_2d(images, p).to(_out_dtype(volume))
     return out.reshape(*stack, *out.shape[-2:])
 
 
@@ -157,12 +172,12 @@ def project_3d_to_2d_multichannel(
     n_pad = d + 2 * p
     shape = (n_pad, n_pad, n_pad)
     fft_in = torch.stack([_wrappers.project_prepare(volume[ch], p) for ch in range(c)])
-    dft = torch.fft.rfftn(fft_in, dim=(-3, -2, -1)).contiguous()
+    dft = _slice_source(torch.fft.rfftn(fft_in, dim=(-3, -2, -1)))
     R, stack = rotation_arg(rotation_matrices, volume.device)
     params = slice_params(n=R.shape[0], image_shape=shape, volume=dft[0], rotation=R,
                           fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
                           rot_tolerance=1e-8, volume_unshifted=True, slices_unshifted=True)
     slices = _ExtractMultichannel.apply(dft, R, params, (R.shape[0], c, n_pad, n_pad // 2 + 1))
     images = _wrappers.irfftn_last(slices, 2)
-    out = _wrappers.recentre_crop_2d(images.reshape(-1, *images.shape[-2:]), p)
+    out = _wrappers.recentre_crop_2d(images.reshape(-1, *images.shape[-2:]), p).to(_out_dtype(volume))
     return out.reshape(*stack, c, *out.shape[-2:])

@@ -30,9 +30,11 @@ from ._params import resolve_deterministic, rotation_arg, slice_params
 class _ExtractCentralSlices(torch.autograd.Function):
     @staticmethod
     def forward(ctx, volume_rfft, rotation_matrices, params, out_shape):
-        # the kernels index raw memory in C order
+        # the kernels index raw memory in C order and sample complex64
         if not (volume_rfft.is_contiguous() and rotation_matrices.is_contiguous()):
             raise ValueError("extraction needs C-contiguous volume and rotation tensors")
+        if volume_rfft.dtype != torch.complex64:
+            raise RuntimeError(f"the extraction kernels sample complex64 volumes (got {volume_rfft.dtype})")
         dev = volume_rfft.device
         out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
         L = _lib.load()
@@ -77,6 +79,8 @@ class _ExtractMultichannel(torch.autograd.Function):
     def forward(ctx, volumes, rotation_matrices, params, out_shape):
         if not (volumes.is_contiguous() and rotation_matrices.is_contiguous()):
             raise ValueError("extraction needs C-contiguous volume and rotation tensors")
+        if volumes.dtype != torch.complex64:
+            raise RuntimeError(f"the extraction kernels sample complex64 volumes (got {volumes.dtype})")
         dev = volumes.device
         out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
         L = _lib.load()

@@ -129,6 +129,32 @@ def test_wrapper_errors():
         tt().backproject_2d_to_3d(torch.zeros((2, 8, 9), device="cuda"), torch.eye(3, device="cuda")[None])
 
 
+def test_project_float64_volumes(oracle, monkeypatch):
+    """float64 volumes project to float64 images (the reference's dtype),
+    sampled in single precision: the float32 projection of the same volume
+    within rounding, the oracle within the float32 tolerance, and a float64
+    volume gradient."""
+    vol = cuda(blob_volume(24, seed=7)).double()
+    R = cuda(rotations(6, seed=8)).float()
+    for graphs in ("1", "0"):  # the graph-replayed and the eager path
+        monkeypatch.setenv("TT_PROJECT_GRAPHS", graphs)
+        p64 = tt().project_3d_to_2d(vol, R)
+        assert p64.dtype == torch.float64
+        p32 = tt().project_3d_to_2d(vol.float(), R)
+        assert rel_l2(p64.float().cpu().numpy(), p32.cpu().numpy()) < 1e-6
+        ref = oracle.project_3d_to_2d(vol.cpu().numpy(), R.cpu().numpy())
+        assert rel_l2(p64.cpu().numpy(), ref) < RTOL
+    mc = tt().project_3d_to_2d_multichannel(torch.stack([vol, 2 * vol]), R)
+    assert mc.dtype == torch.float64
+    assert rel_l2(mc[:, 1].cpu().numpy(), 2 * mc[:, 0].cpu().numpy()) < 1e-6
+    v = vol.clone().requires_grad_(True)
+    tt().project_3d_to_2d(v, R).square().sum().backward()
+    assert v.grad.dtype == torch.float64 and torch.isfinite(v.grad).all()
+    with pytest.raises(RuntimeError):
+        tt().extract_central_slices_rfft_3d(torch.zeros((8, 8, 5), dtype=torch.complex128, device="cuda"),
+                                            (8, 8, 8), R)
+
+
 def test_project_is_differentiable(oracle):
     n = 16
     vol = cuda(blob_volume(n, seed=2)).requires_grad_(True)
@@ -137,8 +163,12 @@ def test_project_is_differentiable(oracle):
     proj.square().sum().backward()
     assert vol.grad is not None and R.grad is not None
     assert torch.isfinite(vol.grad).all() and torch.isfinite(R.grad).all()
-    # directional derivative against a central difference of the GPU forward
-    d = torch.randn_like(vol)
+    # directional derivative against a central difference of the GPU forward.
+    # The loss is quadratic in the volume, so the central difference is exact
+    # up to float32 rounding of lp - lm; a seeded direction keeps the
+    # derivative large against that rounding (a direction nearly orthogonal to
+    # the gradient would not).
+    d = torch.randn(vol.shape, device="cuda", generator=torch.Generator(device="cuda").manual_seed(3))
     eps = 1e-2
     with torch.no_grad():
         lp = tt().project_3d_to_2d(vol + eps * d, R).double().square().sum()
