@@ -296,13 +296,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def xp_launches(n_pixels, volume):
+def copy_launches(n_pixels, volume):
     """1 when an extraction of n_pixels slice pixels (its forward and backward,
-    or the fused MSE) gathers from an x-paired copy of the volume (one pack
-    launch), else 0."""
-    from teamtomo_b200.torch_fourier_slice._xpairs import use_xpairs
+    or the fused MSE) gathers from a copy of the volume (one pack launch),
+    else 0."""
+    from teamtomo_b200.torch_fourier_slice import _layout
 
-    return int(use_xpairs(n_pixels, volume))
+    return int(_layout.choose(n_pixels, volume) != _layout.PLAIN)
 
 
 def load_traffic():
@@ -544,7 +544,7 @@ def config_workload(args):
                     # insertion: splat, finalize, sum; fused MSE: loss kernel, loss and rotation finish
                     # (+ the x-paired copy of the volume)
                     "gpu_launches": n_img // chunk * 3
-                    + n_ext // chunk * (3 + xp_launches(chunk * n * (n // 2 + 1), Vfit))})
+                    + n_ext // chunk * (3 + copy_launches(chunk * n * (n // 2 + 1), Vfit))})
     print(json.dumps(out))
     return 0
 
@@ -823,7 +823,7 @@ def main():
             # extract (+ the x-paired copy of the volume it gathers from), backward,
             # rotation-gradient finish, insert splat, insert finalize (+ absmax
             # pre-passes and the fixed-point add-back when deterministic)
-            "gpu_launches": ((8 if det else 5) + xp_launches(ns * n * (n // 2 + 1), V)) * args.steps,
+            "gpu_launches": ((8 if det else 5) + copy_launches(ns * n * (n // 2 + 1), V)) * args.steps,
             "loss": float(loss.item()),
         }
         print(json.dumps(line))

@@ -40,6 +40,13 @@ enum {
     TT_ERR_WORKSPACE = 3  /* workspace missing or too small */
 };
 
+/* Layouts of the volume the extraction gathers read (tt_slice_params.volume_layout). */
+enum tt_volume_layout {
+    TT_VOLUME_PLAIN = 0,   /* the complex64 rfft volume itself */
+    TT_VOLUME_XPAIRS = 1,  /* x-paired copy, tt_pack_volume_xpairs */
+    TT_VOLUME_BRICKS = 2   /* 2 x 2 x 2 bricked copy, tt_pack_volume_bricks */
+};
+
 /* Geometry of one batch of central slices through one rfft volume. */
 typedef struct tt_slice_params {
     int64_t n;                     /* number of slices (rotation matrices) */
@@ -60,9 +67,11 @@ typedef struct tt_slice_params {
     int32_t deterministic;         /* 1: insertion and the volume gradient accumulate in 64-bit
                                       fixed point, bit-identical for any launch order (the
                                       workspace queries grow accordingly) */
-    int32_t volume_xpairs;         /* 1: volume_rfft is the x-paired copy written by
-                                      tt_pack_volume_xpairs (extraction forward, backward and
-                                      tt_central_slice_mse only; other entry points refuse it).
+    int32_t volume_layout;         /* layout of volume_rfft (tt_volume_layout): TT_VOLUME_PLAIN,
+                                      TT_VOLUME_XPAIRS (the copy of tt_pack_volume_xpairs) or
+                                      TT_VOLUME_BRICKS (tt_pack_volume_bricks); the copies are
+                                      taken by the extraction forward, backward and
+                                      tt_central_slice_mse only, other entry points refuse them.
                                       Occupies the struct's former tail padding: 0 keeps the
                                       plain layout, so zero-initialised structs are unchanged. */
 } tt_slice_params;
@@ -111,12 +120,29 @@ int tt_slice_geometry(const void *rotation_matrices, int32_t mode, uint8_t *flag
  * or plain when p->volume_unshifted).  A pixel's eight trilinear corners are
  * then four 16-byte loads instead of eight 8-byte ones, which lowers the L1
  * wavefronts of the scattered gathers.  Pass the copy as volume_rfft with
- * p->volume_xpairs = 1; results are bit-identical to the plain layout.
+ * p->volume_layout = TT_VOLUME_XPAIRS; results are bit-identical to the plain layout.
  * tt_volume_xpairs_bytes: p->vol_d * vol_h * vol_w * 16.  The source is
  * complex64 (vol_d, vol_h, vol_w); xpairs must be 16-byte aligned.  The
  * reference has no such layout (it samples with grid_sample on the volume). */
 size_t tt_volume_xpairs_bytes(const tt_slice_params *p);
 int tt_pack_volume_xpairs(const void *volume_rfft, void *xpairs, const tt_slice_params *p, void *stream);
+
+/* Bricked copy of an rfft volume for the extraction gathers: 2 x 2 x 2 voxel
+ * bricks of 64 bytes in (z, y, x) brick order, voxels (z, y, x) inside a
+ * brick, always in fftshifted (z, y) order (a p->volume_unshifted source is
+ * shifted while packing).  Voxel (z, y, x) sits at complex64 index
+ *   ((z/2 * ceil(vol_h/2) + y/2) * ceil(vol_w/2) + x/2) * 8 + (z%2)*4 + (y%2)*2 + x%2,
+ * slots past an odd dimension are zero.  A 128-byte line then holds a
+ * 4 x 2 x 2 block of voxels instead of 16 voxels of one row, so the
+ * trilinear corners of a warp's 8 x 4 pixels touch fewer lines.  Pass the
+ * copy as volume_rfft with p->volume_layout = TT_VOLUME_BRICKS; results are
+ * bit-identical to the plain layout.  tt_volume_bricks_bytes:
+ * ceil(vol_d/2) * ceil(vol_h/2) * ceil(vol_w/2) * 64.  The source is complex64
+ * (vol_d, vol_h, vol_w), 8-byte aligned; bricks must be 16-byte aligned and
+ * hold fewer than 2^31 slots (boxes up to about 2000^3).  The
+ * reference has no such layout (it samples with grid_sample on the volume). */
+size_t tt_volume_bricks_bytes(const tt_slice_params *p);
+int tt_pack_volume_bricks(const void *volume_rfft, void *bricks, const tt_slice_params *p, void *stream);
 
 /* Bytes of workspace tt_extract_central_slices_rfft_3d_backward needs when a
  * rotation gradient or (p->deterministic) a volume gradient is requested

@@ -34,7 +34,7 @@ class SliceParams(ctypes.Structure):
         ("x_tolerance", _f32), ("x_tolerance10", _f32),
         ("has_rot_tolerance", _i32), ("rot_tolerance", _f32),
         ("rotation_f64", _i32), ("volume_unshifted", _i32), ("slices_unshifted", _i32),
-        ("deterministic", _i32), ("volume_xpairs", _i32),
+        ("deterministic", _i32), ("volume_layout", _i32),
     ]
 
 
@@ -66,6 +66,8 @@ SIGNATURES = {
     "tt_slice_geometry": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_volume_xpairs_bytes": ([ctypes.POINTER(SliceParams)], _sz),
     "tt_pack_volume_xpairs": ([_vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
+    "tt_volume_bricks_bytes": ([ctypes.POINTER(SliceParams)], _sz),
+    "tt_pack_volume_bricks": ([_vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_extract_backward_workspace_bytes": ([ctypes.POINTER(SliceParams)], _sz),
     "tt_extract_central_slices_rfft_3d_backward": (
         [_vp, _vp, _vp, _vp, _vp, _vp, _sz, ctypes.POINTER(SliceParams), _vp], _i32),

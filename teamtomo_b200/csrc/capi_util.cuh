@@ -32,10 +32,16 @@ inline int check_launch(const char* what) {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Whether the bricked copy of the volume (8 slots per 2 x 2 x 2 brick) has
+// fewer than 2^31 slots, the range of its 32-bit slot offsets.
+inline bool bricks_fit(const tt_slice_params* p) {
+    return ((p->vol_d + 1) / 2) * ((p->vol_h + 1) / 2) * ((p->vol_w + 1) / 2) * 8 < (1LL << 31);
+}
+
 // Validates the common slice parameters; vol_w must be the rfft width of a
 // real dimension and all sizes must fit the int32 index arithmetic used on
 // the per-slice grid.
-inline int validate_params(const tt_slice_params* p, bool allow_xpairs = false) {
+inline int validate_params(const tt_slice_params* p, bool allow_layouts = false) {
     if (!p) return fail(TT_ERR_INVALID, "params is NULL");
     if (p->n < 0) return fail(TT_ERR_INVALID, "n must be >= 0 (got %lld)", (long long)p->n);
     if (p->img_d < 1 || p->img_h < 1 || p->img_w < 1)
@@ -47,9 +53,12 @@ inline int validate_params(const tt_slice_params* p, bool allow_xpairs = false) 
         return fail(TT_ERR_INVALID, "slice or volume too large");
     if (p->n > (1LL << 31) - 1) return fail(TT_ERR_INVALID, "too many slices");
     if (p->deterministic != 0 && p->deterministic != 1) return fail(TT_ERR_INVALID, "deterministic must be 0 or 1");
-    if (p->volume_xpairs != 0 && p->volume_xpairs != 1) return fail(TT_ERR_INVALID, "volume_xpairs must be 0 or 1");
-    if (p->volume_xpairs && !allow_xpairs)
-        return fail(TT_ERR_INVALID, "volume_xpairs: this entry point takes the plain volume layout");
+    if (p->volume_layout < TT_VOLUME_PLAIN || p->volume_layout > TT_VOLUME_BRICKS)
+        return fail(TT_ERR_INVALID, "volume_layout must be 0 (plain), 1 (x-paired) or 2 (bricked)");
+    if (p->volume_layout != TT_VOLUME_PLAIN && !allow_layouts)
+        return fail(TT_ERR_INVALID, "volume_layout: this entry point takes the plain volume layout");
+    if (p->volume_layout == TT_VOLUME_BRICKS && !bricks_fit(p))
+        return fail(TT_ERR_INVALID, "volume_layout: a bricked copy must hold fewer than 2^31 voxel slots");
     return TT_OK;
 }
 

@@ -36,7 +36,8 @@ __device__ __forceinline__ void load_rotation(float* sm, const void* rot, int64_
     if (threadIdx.x < 9) sm[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, apply_tol);
 }
 
-// VT: float2 (plain volume) or float4 (x-paired copy, tt_pack_volume_xpairs).
+// VT: float2 (plain volume), float4 (x-paired copy, tt_pack_volume_xpairs) or
+// VoxBrick2 (bricked copy, tt_pack_volume_bricks).
 // One block per (slice, row of tiles), eight resident blocks (32 registers):
 // the gathers are latency-bound at six (64 % warps active); full occupancy
 // takes 8.5 % off the launch, the row loop another 1 %.
@@ -417,12 +418,39 @@ static int launch_backward_t(const VT* v, const void* rot, const float2* gr, flo
     return TT_OK;
 }
 
-// `v` is the plain complex64 volume or, with g.vol_xpairs, its x-paired copy.
+// `v` is the plain complex64 volume or the copy g.vol_layout names.
 static int launch_backward(const void* v, const void* rot, const float2* gr, float2* dv, void* grad_rotation,
                            float* part, const SliceGeom& g, cudaStream_t st, void* fixed = nullptr) {
-    if (g.vol_xpairs)
-        return launch_backward_t((const float4*)v, rot, gr, dv, grad_rotation, part, g, st, fixed);
-    return launch_backward_t((const float2*)v, rot, gr, dv, grad_rotation, part, g, st, fixed);
+    switch (g.vol_layout) {
+        case TT_VOLUME_XPAIRS:
+            return launch_backward_t((const float4*)v, rot, gr, dv, grad_rotation, part, g, st, fixed);
+        case TT_VOLUME_BRICKS:
+            return launch_backward_t((const VoxBrick2*)v, rot, gr, dv, grad_rotation, part, g, st, fixed);
+        default:
+            return launch_backward_t((const float2*)v, rot, gr, dv, grad_rotation, part, g, st, fixed);
+    }
+}
+
+// Bricked copy: voxel (z, y, x), in fftshifted (z, y) order whatever the
+// source's, sits in 2 x 2 x 2 brick ((z/2 * ceil(H/2) + y/2) * ceil(W/2) + x/2)
+// at slot (z&1)*4 + (y&1)*2 + (x&1): eight complex64 voxels, 64 bytes, two
+// x-adjacent bricks per 128-byte line.  One thread per destination slot (a
+// warp writes four whole bricks, 256 contiguous bytes), reading the source
+// voxel (an unshifted source remapped by vox_index) or zero for the slots
+// past an odd dimension.  Grid-stride over the slots.
+__global__ void pack_bricks_kernel(const float2* __restrict__ vol, float2* __restrict__ bricks, SliceGeom g,
+                                   int64_t slots) {
+    const int bh = (g.H + 1) >> 1, bw = (g.W + 1) >> 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < slots;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = i >> 3;
+        const int s = (int)(i & 7);
+        const int bx = (int)(b % bw);
+        const int64_t bzy = b / bw;
+        const int by = (int)(bzy % bh), bz = (int)(bzy / bh);
+        const int z = 2 * bz + (s >> 2), y = 2 * by + ((s >> 1) & 1), x = 2 * bx + (s & 1);
+        bricks[i] = (z < g.D && y < g.H && x < g.W) ? vol[vox_index(g, z, y, x)] : make_float2(0.0f, 0.0f);
+    }
 }
 
 // x-paired copy: xp[r * W + x] = (vol[r * W + x], vol[r * W + x + 1]), zero
@@ -495,11 +523,21 @@ extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotatio
     float2* dv = (float2*)grad_volume;
     cudaStream_t st = as_stream(stream);
     const unsigned nb = (unsigned)((int64_t)g.n * (tiles / tiles_x_of(g.wr)));  // one block per row of tiles
-    if (int e = g.vol_xpairs ? launch_mse((const float4*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part,
-                                          loss_part, scale, g, tiles, nb, st)
-                             : launch_mse((const float2*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part,
-                                          loss_part, scale, g, tiles, nb, st))
-        return e;
+    int e;
+    switch (g.vol_layout) {
+        case TT_VOLUME_XPAIRS:
+            e = launch_mse((const float4*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part, loss_part,
+                           scale, g, tiles, nb, st);
+            break;
+        case TT_VOLUME_BRICKS:
+            e = launch_mse((const VoxBrick2*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part, loss_part,
+                           scale, g, tiles, nb, st);
+            break;
+        default:
+            e = launch_mse((const float2*)volume_rfft, rotation_matrices, t, dv, grad_rotation, part, loss_part,
+                           scale, g, tiles, nb, st);
+    }
+    if (e) return e;
     mse_loss_finish_kernel<<<1, 1024, 0, st>>>(loss_part, blocks, 1.0 / m, loss);
     if (int e = check_launch("mse_loss_finish_kernel")) return e;
     if (grad_rotation) {
@@ -522,12 +560,20 @@ extern "C" int tt_extract_central_slices_rfft_3d(const void* volume_rfft, const 
     const int64_t blocks = (int64_t)g.n * tiles;
     if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract: too many blocks");
     const unsigned nb = (unsigned)((int64_t)g.n * (tiles / tiles_x_of(g.wr)));  // one block per row of tiles
-    if (g.vol_xpairs)
-        extract_fwd_kernel<<<nb, kExtractThreads, 0, as_stream(stream)>>>(
-            (const float4*)volume_rfft, rotation_matrices, (float2*)slices_out, g, tiles);
-    else
-        extract_fwd_kernel<<<nb, kExtractThreads, 0, as_stream(stream)>>>(
-            (const float2*)volume_rfft, rotation_matrices, (float2*)slices_out, g, tiles);
+    cudaStream_t st = as_stream(stream);
+    switch (g.vol_layout) {
+        case TT_VOLUME_XPAIRS:
+            extract_fwd_kernel<<<nb, kExtractThreads, 0, st>>>((const float4*)volume_rfft, rotation_matrices,
+                                                               (float2*)slices_out, g, tiles);
+            break;
+        case TT_VOLUME_BRICKS:
+            extract_fwd_kernel<<<nb, kExtractThreads, 0, st>>>((const VoxBrick2*)volume_rfft, rotation_matrices,
+                                                               (float2*)slices_out, g, tiles);
+            break;
+        default:
+            extract_fwd_kernel<<<nb, kExtractThreads, 0, st>>>((const float2*)volume_rfft, rotation_matrices,
+                                                               (float2*)slices_out, g, tiles);
+    }
     return check_launch("extract_fwd_kernel");
 }
 
@@ -551,6 +597,28 @@ extern "C" int tt_pack_volume_xpairs(const void* volume_rfft, void* xpairs, cons
     const dim3 grid((unsigned)((W + 31) / 32), (unsigned)(gy < 65535 ? gy : 65535));
     pack_xpairs_kernel<<<grid, block, 0, as_stream(stream)>>>((const float2*)volume_rfft, (float4*)xpairs, rows, W);
     return check_launch("pack_xpairs_kernel");
+}
+
+extern "C" size_t tt_volume_bricks_bytes(const tt_slice_params* p) {
+    if (!p || p->vol_d < 1 || p->vol_h < 1 || p->vol_w < 1) return 0;
+    return (size_t)(((p->vol_d + 1) / 2) * ((p->vol_h + 1) / 2) * ((p->vol_w + 1) / 2)) * 64;
+}
+
+extern "C" int tt_pack_volume_bricks(const void* volume_rfft, void* bricks, const tt_slice_params* p,
+                                     void* stream) {
+    if (int e = validate_params(p, true)) return e;
+    if (!volume_rfft || !bricks) return fail(TT_ERR_INVALID, "pack_volume_bricks: NULL pointer argument");
+    if ((reinterpret_cast<uintptr_t>(bricks) & 15) != 0)
+        return fail(TT_ERR_INVALID, "pack_volume_bricks: the bricked copy must be 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(volume_rfft) & 7) != 0)
+        return fail(TT_ERR_INVALID, "pack_volume_bricks: the volume must be 8-byte aligned");
+    if (!bricks_fit(p)) return fail(TT_ERR_INVALID, "pack_volume_bricks: the copy must hold fewer than 2^31 slots");
+    const SliceGeom g = make_geom(*p);
+    const int64_t slots = (int64_t)(tt_volume_bricks_bytes(p) / sizeof(float2));
+    const int64_t want = (slots + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148 * 64 ? want : 148 * 64);
+    pack_bricks_kernel<<<grid, 256, 0, as_stream(stream)>>>((const float2*)volume_rfft, (float2*)bricks, g, slots);
+    return check_launch("pack_bricks_kernel");
 }
 
 extern "C" int tt_slice_geometry(const void* rotation_matrices, int32_t mode, uint8_t* flags, float* coords,

@@ -34,7 +34,7 @@ struct SliceGeom {
     int rot_f64;                   // rotation matrices are float64
     int vol_unshifted;             // volume is the plain rfftn output (no fftshift of z, y)
     int slice_unshifted;           // slices are stored ifftshifted along rows (irfft-ready)
-    int vol_xpairs;                // volume is the x-paired copy (float4 per voxel)
+    int vol_layout;                // TT_VOLUME_PLAIN / _XPAIRS / _BRICKS (tt_slice_params.volume_layout)
     int slice_rows;                // storage rows per slice of the insertion's images
                                    // (img_h; channels * img_h for channel-interleaved stacks)
     float dcdp0, dcdp1, dcdp2;     // d(array coord)/d(frequency) per axis
@@ -71,7 +71,7 @@ __host__ inline SliceGeom make_geom(const tt_slice_params& p) {
     g.rot_f64 = p.rotation_f64;
     g.vol_unshifted = p.volume_unshifted;
     g.slice_unshifted = p.slices_unshifted;
-    g.vol_xpairs = p.volume_xpairs;
+    g.vol_layout = p.volume_layout;
     g.slice_rows = (int)p.img_h;
     g.dcdp0 = g.s0 / g.iw0;
     g.dcdp1 = g.s1 / g.iw1;

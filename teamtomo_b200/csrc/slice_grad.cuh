@@ -122,17 +122,18 @@ __device__ __forceinline__ void scatter_dv_fixed_paired(unsigned long long* __re
 }
 
 // The eight corner values of a pixel; corners past the last index read as
-// zero, as in grid_sample.  VT: float2 (plain layout) or float4 (x-paired).
+// zero, as in grid_sample.  VT: float2 (plain layout), float4 (x-paired) or
+// VoxBrick2 (bricked).
 template <typename VT>
 __device__ __forceinline__ void load_corners(const VT* __restrict__ vol, const SliceGeom& g, const Corners& k,
                                              float2 v[2][2][2]) {
+    const XRows<VT> rows(vol, g, k);
 #pragma unroll
     for (int bz = 0; bz < 2; bz++)
 #pragma unroll
         for (int by = 0; by < 2; by++) {
             const bool row_ok = (!bz || k.zin) && (!by || k.yin);
-            const int64_t base = vox_index(g, k.z0 + (row_ok ? bz : 0), k.y0 + (row_ok ? by : 0), k.x0);
-            load_xrow(vol, base, row_ok, row_ok && k.xin, v[bz][by][0], v[bz][by][1]);
+            rows.load(g, row_ok ? bz : 0, row_ok ? by : 0, row_ok, row_ok && k.xin, v[bz][by][0], v[bz][by][1]);
         }
 }
 

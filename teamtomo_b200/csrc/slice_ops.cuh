@@ -95,29 +95,78 @@ __device__ __forceinline__ bool extract_geometry(const SliceGeom& g, const float
     return inside_volume(g, c);
 }
 
-// The two x-corners (x0, x0 + 1) of the volume row starting at voxel `base`:
-// v0 when lo, v1 when hi (hi implies lo), zero otherwise.  Plain layout: two
-// 8-byte gathers.
-__device__ __forceinline__ void load_xrow(const float2* __restrict__ vol, int64_t base, bool lo, bool hi,
-                                          float2& v0, float2& v1) {
+// Element type of the bricked copy (brick_index addressing): one complex64 voxel.
+struct VoxBrick2 {
+    float x, y;
+};
+
+// The two x-corners (x0, x0 + 1) of volume row (z, y) (fftshifted
+// coordinates): v0 when lo, v1 when hi (hi implies lo), zero otherwise.
+// Plain layout: two 8-byte gathers.
+__device__ __forceinline__ void load_xrow(const float2* __restrict__ vol, const SliceGeom& g, int z, int y, int x0,
+                                          bool lo, bool hi, float2& v0, float2& v1) {
+    const int64_t base = vox_index(g, z, y, x0);
     v0 = lo ? __ldg(vol + base) : make_float2(0.0f, 0.0f);
     v1 = hi ? __ldg(vol + base + 1) : make_float2(0.0f, 0.0f);
 }
 
 // x-paired layout (entry = (V[x], V[x + 1])): one 16-byte gather.
-__device__ __forceinline__ void load_xrow(const float4* __restrict__ vol, int64_t base, bool lo, bool hi,
-                                          float2& v0, float2& v1) {
-    const float4 q = lo ? __ldg(vol + base) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+__device__ __forceinline__ void load_xrow(const float4* __restrict__ vol, const SliceGeom& g, int z, int y, int x0,
+                                          bool lo, bool hi, float2& v0, float2& v1) {
+    const float4 q = lo ? __ldg(vol + vox_index(g, z, y, x0)) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     v0 = make_float2(q.x, q.y);
     v1 = hi ? make_float2(q.z, q.w) : make_float2(0.0f, 0.0f);
 }
 
+// The four x-rows (z0 + bz, y0 + by) of a trilinear corner set k, addressed
+// for layout VT: row (bz, by) gives v0 = V[.., x0] when lo and v1 =
+// V[.., x0 + 1] when hi (hi implies lo), zero otherwise.
+template <typename VT>
+struct XRows {
+    const VT* vol;
+    int z0, y0, x0;
+    __device__ __forceinline__ XRows(const VT* v, const SliceGeom&, const Corners& k)
+        : vol(v), z0(k.z0), y0(k.y0), x0(k.x0) {}
+    __device__ __forceinline__ void load(const SliceGeom& g, int bz, int by, bool lo, bool hi, float2& v0,
+                                         float2& v1) const {
+        load_xrow(vol, g, z0 + bz, y0 + by, x0, lo, hi, v0, v1);
+    }
+};
+
+// Bricked layout (always fftshifted): the corner (z0, y0, x0) is addressed
+// once; its +1 neighbours are the next slot of the brick along an even
+// coordinate and the first slot of the next brick along an odd one (x: 1 or
+// 7 slots, y: 2 or one brick row - 2, z: 4 or one brick plane - 4).  32-bit
+// slot offsets: bricked copies hold fewer than 2^31 slots.
+template <>
+struct XRows<VoxBrick2> {
+    const float2* p;
+    uint32_t base, dz, dy, dx;
+    __device__ __forceinline__ XRows(const VoxBrick2* v, const SliceGeom& g, const Corners& k)
+        : p(reinterpret_cast<const float2*>(v)) {
+        const uint32_t bh = (uint32_t)(g.H + 1) >> 1, bw = (uint32_t)(g.W + 1) >> 1;
+        base = ((((uint32_t)k.z0 >> 1) * bh + ((uint32_t)k.y0 >> 1)) * bw + ((uint32_t)k.x0 >> 1)) * 8u +
+               (((uint32_t)k.z0 & 1u) << 2) + (((uint32_t)k.y0 & 1u) << 1) + ((uint32_t)k.x0 & 1u);
+        dx = (k.x0 & 1) ? 7u : 1u;
+        dy = (k.y0 & 1) ? bw * 8u - 2u : 2u;
+        dz = (k.z0 & 1) ? bh * bw * 8u - 4u : 4u;
+    }
+    __device__ __forceinline__ void load(const SliceGeom&, int bz, int by, bool lo, bool hi, float2& v0,
+                                         float2& v1) const {
+        const uint32_t i = base + (bz ? dz : 0u) + (by ? dy : 0u);
+        v0 = lo ? __ldg(p + i) : make_float2(0.0f, 0.0f);
+        v1 = hi ? __ldg(p + (i + dx)) : make_float2(0.0f, 0.0f);
+    }
+};
+
 // Trilinear sample of the complex volume at corner set k; VT is float2 (plain
-// layout) or float4 (x-paired layout), with the same values and FMA order.
+// layout), float4 (x-paired) or VoxBrick2 (bricked), with the same values and
+// FMA order.
 template <typename VT>
 __device__ __forceinline__ float2 sample_trilinear(const VT* __restrict__ vol, const SliceGeom& g,
                                                    const Corners& k) {
     float2 r = make_float2(0.0f, 0.0f);
+    const XRows<VT> rows(vol, g, k);
 #pragma unroll
     for (int bz = 0; bz < 2; bz++) {
         if (bz && !k.zin) continue;
@@ -126,9 +175,8 @@ __device__ __forceinline__ float2 sample_trilinear(const VT* __restrict__ vol, c
         for (int by = 0; by < 2; by++) {
             if (by && !k.yin) continue;
             const float wzy = (by ? k.ay1 : k.ay0) * wz;
-            const int64_t base = vox_index(g, k.z0 + bz, k.y0 + by, k.x0);
             float2 v0, v1;
-            load_xrow(vol, base, true, k.xin, v0, v1);
+            rows.load(g, bz, by, true, k.xin, v0, v1);
             const float w0 = k.ax0 * wzy;
             r.x = fmaf(v0.x, w0, r.x);
             r.y = fmaf(v0.y, w0, r.y);

@@ -19,7 +19,7 @@ import math
 import torch
 
 from . import _lib
-from .torch_fourier_slice import _xpairs
+from .torch_fourier_slice import _layout
 from .torch_fourier_slice._params import rotation_arg, slice_params
 
 
@@ -34,11 +34,12 @@ class _CentralSliceMSE(torch.autograd.Function):
         L = _lib.load()
         nbytes = int(L.tt_central_slice_mse_workspace_bytes(params))
         ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
-        # large calls gather from an x-paired copy of the volume (bit-identical results)
-        xp = _xpairs.pack(volume_rfft, params) if _xpairs.use_xpairs(targets.numel(), volume_rfft) else None
-        _lib.check(L.tt_central_slice_mse(_lib.ptr(xp if xp is not None else volume_rfft), _lib.ptr(R),
+        # large calls gather from a bricked copy of the volume (bit-identical results)
+        layout = _layout.choose(targets.numel(), volume_rfft)
+        copy = _layout.pack(volume_rfft, params, layout)
+        _lib.check(L.tt_central_slice_mse(_lib.ptr(copy if copy is not None else volume_rfft), _lib.ptr(R),
                                           _lib.ptr(targets), _lib.ptr(loss), _lib.ptr(dvol), _lib.ptr(drot),
-                                          _lib.ptr(ws), nbytes, _xpairs.with_xpairs(params, xp is not None),
+                                          _lib.ptr(ws), nbytes, _layout.with_layout(params, layout),
                                           _lib.stream_of(dev)), "central_slice_mse")
         ctx.save_for_backward(dvol, drot)
         return loss

@@ -120,7 +120,7 @@ def project_3d_to_2d(
     R_in = torch.as_tensor(rotation_matrices)
     if _graph_eligible(volume, R_in, d + 2 * p):
         key = (volume.device, tuple(volume.shape), volume.dtype, tuple(R_in.shape), R_in.dtype,
-               float(pad_factor), fftfreq_max, bool(zyx_matrices), os.environ.get("TT_VOLUME_XPAIRS", "auto"))
+               float(pad_factor), fftfreq_max, bool(zyx_matrices), os.environ.get("TT_VOLUME_LAYOUT", "auto"))
         with _graphs_lock:
             entry = _graphs.get(key)
             if entry is None:

@@ -23,7 +23,7 @@ from __future__ import annotations
 import torch
 
 from .. import _lib
-from . import _xpairs
+from . import _layout
 from ._params import resolve_deterministic, rotation_arg, slice_params
 
 
@@ -38,20 +38,20 @@ class _ExtractCentralSlices(torch.autograd.Function):
         dev = volume_rfft.device
         out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
         L = _lib.load()
-        # large calls gather from an x-paired copy (bit-identical results)
-        xp = _xpairs.pack(volume_rfft, params) if _xpairs.use_xpairs(out.numel(), volume_rfft) else None
+        # large calls gather from a bricked copy (bit-identical results)
+        layout = _layout.choose(out.numel(), volume_rfft)
+        copy = _layout.pack(volume_rfft, params, layout)
         _lib.check(
-            L.tt_extract_central_slices_rfft_3d(_lib.ptr(xp if xp is not None else volume_rfft),
+            L.tt_extract_central_slices_rfft_3d(_lib.ptr(copy if copy is not None else volume_rfft),
                                                 _lib.ptr(rotation_matrices), _lib.ptr(out),
-                                                _xpairs.with_xpairs(params, xp is not None),
-                                                _lib.stream_of(dev)),
+                                                _layout.with_layout(params, layout), _lib.stream_of(dev)),
             "extract_central_slices_rfft_3d",
         )
         ctx.params = params
         # the backward reads the volume only for d/drotation: keep the copy for it
-        keep_xp = xp is not None and ctx.needs_input_grad[1]
-        ctx.has_xp = keep_xp
-        ctx.save_for_backward(volume_rfft, rotation_matrices, *((xp,) if keep_xp else ()))
+        keep = copy is not None and ctx.needs_input_grad[1]
+        ctx.layout = layout if keep else _layout.PLAIN
+        ctx.save_for_backward(volume_rfft, rotation_matrices, *((copy,) if keep else ()))
         return out
 
     @staticmethod
@@ -61,12 +61,14 @@ class _ExtractCentralSlices(torch.autograd.Function):
         want_v, want_r = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         dvol = drot = None
         if want_v or want_r:
-            xp = saved[2] if ctx.has_xp else None
+            layout = ctx.layout
+            copy = saved[2] if layout != _layout.PLAIN else None
             # direct calls of the backward alone (no forward copy) make their own
-            if xp is None and want_r and _xpairs.use_xpairs(grad.numel(), volume_rfft):
-                xp = _xpairs.pack(volume_rfft, ctx.params)
+            if copy is None and want_r:
+                layout = _layout.choose(grad.numel(), volume_rfft)
+                copy = _layout.pack(volume_rfft, ctx.params, layout)
             dvol, drot = extract_backward(volume_rfft, rotation_matrices, grad, ctx.params,
-                                          want_v, want_r, xpairs=xp)
+                                          want_v, want_r, copy=copy, layout=layout)
         return dvol, drot, None, None
 
 
@@ -112,14 +114,16 @@ class _ExtractMultichannel(torch.autograd.Function):
 
 
 def extract_backward(volume_rfft, rotation_matrices, grad, params, want_volume=True,
-                     want_rotation=True, xpairs=None):
+                     want_rotation=True, copy=None, layout=_layout.PLAIN):
     """Fused backward: (d/dvolume, d/drotation) for upstream slice gradient
-    ``grad``.  ``xpairs``: the volume's x-paired copy (``_xpairs.pack``), read
+    ``grad``.  ``copy``: the volume's ``layout`` copy (``_layout.pack``), read
     by the rotation gradient's gathers in place of ``volume_rfft``."""
     dev = volume_rfft.device
     grad = _lib.dense(grad.to(torch.complex64))
     L = _lib.load()
-    params = _xpairs.with_xpairs(params, xpairs is not None)
+    if copy is None:
+        layout = _layout.PLAIN
+    params = _layout.with_layout(params, layout)
     dvol = torch.zeros_like(volume_rfft) if want_volume else None
     drot = torch.empty_like(rotation_matrices) if want_rotation else None
     ws = None
@@ -129,7 +133,7 @@ def extract_backward(volume_rfft, rotation_matrices, grad, params, want_volume=T
         ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev)
     _lib.check(
         L.tt_extract_central_slices_rfft_3d_backward(
-            _lib.ptr(xpairs if xpairs is not None else volume_rfft), _lib.ptr(rotation_matrices),
+            _lib.ptr(copy if copy is not None else volume_rfft), _lib.ptr(rotation_matrices),
             _lib.ptr(grad), _lib.ptr(dvol),
             _lib.ptr(drot), _lib.ptr(ws), nbytes, params, _lib.stream_of(dev)),
         "extract_central_slices_rfft_3d backward",

@@ -57,58 +57,65 @@ def test_param_struct_layout():
     # 7 int64 + 12 four-byte fields (the last one in what was the tail padding)
     assert ctypes.sizeof(_lib.SliceParams) == 104
     assert _lib.SliceParams.fftfreq_max.offset == 60 and _lib.SliceParams.deterministic.offset == 96
-    assert _lib.SliceParams.volume_xpairs.offset == 100
+    assert _lib.SliceParams.volume_layout.offset == 100
 
 
-def test_xpairs_flag_validation():
-    """volume_xpairs: accepted by the extraction entry points, refused by the
-    others and outside {0, 1}; the pack checks its pointers and alignment."""
+@pytest.mark.parametrize("layout", [1, 2])
+def test_volume_layout_validation(layout):
+    """volume_layout: the copies are accepted by the extraction entry points,
+    refused by the others, and codes outside {0, 1, 2} are refused; the packs
+    check their pointers and alignment."""
     from teamtomo_b200 import _lib
 
     L = _lib.load()
     fake = ctypes.c_void_p(16)
-    p = _params(volume_xpairs=1)
+    p = _params(volume_layout=layout)
     assert L.tt_volume_xpairs_bytes(ctypes.byref(p)) == 16 * 16 * 9 * 16
+    assert L.tt_volume_bricks_bytes(ctypes.byref(p)) == 8 * 8 * 5 * 64
     assert L.tt_insert_accumulate(fake, 0, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
-    assert b"volume_xpairs" in L.tt_last_error()
+    assert b"volume_layout" in L.tt_last_error()
     assert L.tt_insert_central_slices_rfft_3d(fake, 0, fake, fake, fake, fake, 1 << 30, ctypes.byref(p),
                                               None) == _lib.TT_ERR_INVALID
     assert L.tt_extract_central_slices_rfft_3d_multichannel(fake, 2, fake, fake, ctypes.byref(p),
                                                             None) == _lib.TT_ERR_INVALID
-    # accepted (fails later, on the missing workspace, not on the flag)
+    # accepted (fails later, on the missing workspace, not on the layout)
     assert L.tt_extract_central_slices_rfft_3d_backward(fake, fake, fake, None, fake, None, 0,
                                                         ctypes.byref(p), None) == _lib.TT_ERR_WORKSPACE
-    p = _params(volume_xpairs=2)
-    assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    for bad in (3, -1):
+        p = _params(volume_layout=bad)
+        assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
     p = _params()
-    assert L.tt_pack_volume_xpairs(None, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
-    assert L.tt_pack_volume_xpairs(fake, ctypes.c_void_p(24), ctypes.byref(p), None) == _lib.TT_ERR_INVALID
-    assert b"16-byte" in L.tt_last_error()
+    for pack in (L.tt_pack_volume_xpairs, L.tt_pack_volume_bricks):
+        assert pack(None, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+        assert pack(fake, ctypes.c_void_p(24), ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+        assert b"16-byte" in L.tt_last_error()
+        assert pack(ctypes.c_void_p(20), fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+        assert b"8-byte" in L.tt_last_error()
 
 
-def test_xpairs_policy(monkeypatch):
-    from teamtomo_b200.torch_fourier_slice import _xpairs
+def test_volume_layout_policy(monkeypatch):
+    from teamtomo_b200.torch_fourier_slice import _layout
 
     vol = torch.zeros((16, 16, 9), dtype=torch.complex64)
-    monkeypatch.delenv("TT_VOLUME_XPAIRS", raising=False)
-    assert _xpairs.copy_budget(vol) == 0  # a CPU tensor: no L2 to fit in
-    assert not _xpairs.use_xpairs(10**9, vol)
-    monkeypatch.setattr(_xpairs, "copy_budget", lambda v: 16 * v.numel())
-    assert _xpairs.use_xpairs(2 * vol.numel(), vol) and not _xpairs.use_xpairs(2 * vol.numel() - 1, vol)
-    assert not _xpairs.use_xpairs(10**9, vol.to(torch.complex128))
-    monkeypatch.setattr(_xpairs, "copy_budget", lambda v: 16 * v.numel() - 1)
-    assert not _xpairs.use_xpairs(10**9, vol)
-    monkeypatch.setenv("TT_VOLUME_XPAIRS", "0")
-    monkeypatch.setattr(_xpairs, "copy_budget", lambda v: 1 << 40)
-    assert not _xpairs.use_xpairs(10**9, vol)
-    monkeypatch.setenv("TT_VOLUME_XPAIRS", "1")
-    assert _xpairs.use_xpairs(1, vol)
+    monkeypatch.delenv("TT_VOLUME_LAYOUT", raising=False)
+    # auto: the bricked copy from half a slice pixel per voxel up
+    assert _layout.choose(vol.numel() // 2, vol) == _layout.BRICKS
+    assert _layout.choose(vol.numel() // 2 - 1, vol) == _layout.PLAIN
+    assert _layout.choose(10**9, vol.to(torch.complex128)) == _layout.PLAIN
+    assert _layout.choose(10**9, vol[None]) == _layout.PLAIN
+    for mode, code in (("plain", _layout.PLAIN), ("xpairs", _layout.XPAIRS), ("bricks", _layout.BRICKS)):
+        monkeypatch.setenv("TT_VOLUME_LAYOUT", mode)
+        assert _layout.choose(1, vol) == code
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "bogus")
+    with pytest.raises(ValueError):
+        _layout.choose(1, vol)
+    assert _layout.pack(vol, None, _layout.PLAIN) is None
     from teamtomo_b200 import _lib
 
     p = _lib.SliceParams()
     p.n, p.deterministic = 7, 1
-    q = _xpairs.with_xpairs(p, True)
-    assert (q.n, q.deterministic, q.volume_xpairs, p.volume_xpairs) == (7, 1, 1, 0)
+    q = _layout.with_layout(p, _layout.BRICKS)
+    assert (q.n, q.deterministic, q.volume_layout, p.volume_layout) == (7, 1, 2, 0)
 
 
 def test_validation_rejects_before_launch():
