@@ -341,7 +341,12 @@ int tt_extract_central_lines_rfft_2d_backward(const void *image_rfft, int64_t im
  * (n, channels, img_h, img_w/2+1) complex64 — the reference's (..., c, h, w)
  * layout.  Replace the per-channel loops of
  * extract_central_slices_rfft_3d_multichannel (_extract_central_slices_rfft_3d.py:225-367)
- * and insert_central_slices_rfft_3d_multichannel (_insert_central_slices_rfft_3d.py:109-210). */
+ * and insert_central_slices_rfft_3d_multichannel (_insert_central_slices_rfft_3d.py:109-210).
+ * The two extraction entry points also take p->volume_layout =
+ * TT_VOLUME_BRICKS: volume_rfft is then the channels' bricked copies
+ * (tt_pack_volume_bricks of each channel) back to back, each
+ * tt_volume_bricks_bytes long; grad_volume stays plain.  They refuse
+ * TT_VOLUME_XPAIRS. */
 int tt_extract_central_slices_rfft_3d_multichannel(const void *volume_rfft, int64_t channels,
                                                    const void *rotation_matrices, void *slices_out,
                                                    const tt_slice_params *p, void *stream);

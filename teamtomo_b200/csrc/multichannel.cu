@@ -20,9 +20,11 @@ __device__ __forceinline__ int64_t chan_pixel(const SliceGeom& g, int64_t s, int
 }
 
 // Extraction: one thread per slice pixel, all channels; eight resident blocks
-// (32 registers, no spills) for the gathers.
+// (32 registers) for the gathers.  VT: float2 (plain volumes) or VoxBrick2
+// (the channels' bricked copies back to back); vstride in VT elements.
+template <typename VT>
 __global__ void __launch_bounds__(kTileThreads, 8)
-extract_multi_fwd_kernel(const float2* __restrict__ vol, int64_t vstride, int channels,
+extract_multi_fwd_kernel(const VT* __restrict__ vol, int64_t vstride, int channels,
                          const void* __restrict__ rot, float2* __restrict__ out, SliceGeom g, int tiles) {
     __shared__ float m[9];
     const int64_t s = blockIdx.x / tiles;
@@ -47,10 +49,12 @@ extract_multi_fwd_kernel(const float2* __restrict__ vol, int64_t vstride, int ch
 }
 
 // Backward: d/dvolume per channel, d/drotation summed over the channels
-// (block partials reduced as in the single-channel kernel).
-template <bool WANT_DV, bool WANT_DR>
+// (block partials reduced as in the single-channel kernel).  The gathers read
+// vol (VT as in the forward, channel stride vstride); d/dvolume is plain
+// complex64 with channel stride dstride.
+template <bool WANT_DV, bool WANT_DR, typename VT>
 __global__ void __launch_bounds__(kTileThreads)
-extract_multi_bwd_kernel(const float2* __restrict__ vol, int64_t vstride, int channels,
+extract_multi_bwd_kernel(const VT* __restrict__ vol, int64_t vstride, int64_t dstride, int channels,
                          const void* __restrict__ rot, const float2* __restrict__ grad,
                          float2* __restrict__ dvol, float* __restrict__ part, SliceGeom g, int tiles) {
     __shared__ float m[9];
@@ -69,7 +73,7 @@ extract_multi_bwd_kernel(const float2* __restrict__ vol, int64_t vstride, int ch
             for (int ch = 0; ch < channels; ch++) {
                 float2 gv = __ldcs(grad + chan_pixel(g, s, ch, channels, iy, ix));
                 if (cj) gv.y = -gv.y;
-                if (WANT_DV) scatter_dv(DvTarget<false>{dvol + ch * vstride, nullptr, 0.0}, g, k, gv);
+                if (WANT_DV) scatter_dv(DvTarget<false>{dvol + ch * dstride, nullptr, 0.0}, g, k, gv);
                 if (WANT_DR) {
                     float2 v[2][2][2];
                     load_corners(vol + ch * vstride, g, k, v);
@@ -142,6 +146,32 @@ static int check_channels(int64_t channels, const char* what) {
     return TT_OK;
 }
 
+// Multichannel extraction volumes: plain, or the channels' bricked copies back
+// to back (vstride = one copy's slots); the x-paired copy is not taken.
+static int multi_volume_stride(const tt_slice_params* p, int64_t& vstride, const char* what) {
+    if (p->volume_layout == TT_VOLUME_XPAIRS)
+        return fail(TT_ERR_INVALID, "%s: volume_layout: plain or bricked volumes only", what);
+    vstride = p->volume_layout == TT_VOLUME_BRICKS
+                  ? ((p->vol_d + 1) / 2) * ((p->vol_h + 1) / 2) * ((p->vol_w + 1) / 2) * 8
+                  : p->vol_d * p->vol_h * p->vol_w;
+    return TT_OK;
+}
+
+template <typename VT>
+static void launch_multi_bwd(const VT* v, int64_t vstride, int64_t dstride, int c, const void* rot,
+                             const float2* gr, float2* dv, bool want_dr, float* part, const SliceGeom& g, int tiles,
+                             unsigned nb, cudaStream_t st) {
+    if (dv && want_dr)
+        extract_multi_bwd_kernel<true, true, VT><<<nb, kTileThreads, 0, st>>>(v, vstride, dstride, c, rot, gr, dv,
+                                                                            part, g, tiles);
+    else if (dv)
+        extract_multi_bwd_kernel<true, false, VT><<<nb, kTileThreads, 0, st>>>(v, vstride, dstride, c, rot, gr, dv,
+                                                                             part, g, tiles);
+    else
+        extract_multi_bwd_kernel<false, true, VT><<<nb, kTileThreads, 0, st>>>(v, vstride, dstride, c, rot, gr,
+                                                                              dv, part, g, tiles);
+}
+
 }  // namespace tt
 
 using namespace tt;
@@ -149,8 +179,10 @@ using namespace tt;
 extern "C" int tt_extract_central_slices_rfft_3d_multichannel(const void* volume_rfft, int64_t channels,
                                                               const void* rotation_matrices, void* slices_out,
                                                               const tt_slice_params* p, void* stream) {
-    if (int e = validate_params(p)) return e;
+    if (int e = validate_params(p, true)) return e;
     if (int e = check_channels(channels, "extract multichannel")) return e;
+    int64_t vstride;
+    if (int e = multi_volume_stride(p, vstride, "extract multichannel")) return e;
     if (p->n == 0) return TT_OK;
     if (!volume_rfft || !rotation_matrices || !slices_out)
         return fail(TT_ERR_INVALID, "extract multichannel: NULL pointer argument");
@@ -158,9 +190,12 @@ extern "C" int tt_extract_central_slices_rfft_3d_multichannel(const void* volume
     int tiles;
     int64_t blocks;
     if (int e = multi_blocks(g, tiles, blocks, "extract multichannel")) return e;
-    const int64_t vstride = p->vol_d * p->vol_h * p->vol_w;
-    extract_multi_fwd_kernel<<<(unsigned)blocks, kTileThreads, 0, as_stream(stream)>>>(
-        (const float2*)volume_rfft, vstride, (int)channels, rotation_matrices, (float2*)slices_out, g, tiles);
+    if (p->volume_layout == TT_VOLUME_BRICKS)
+        extract_multi_fwd_kernel<<<(unsigned)blocks, kTileThreads, 0, as_stream(stream)>>>(
+            (const VoxBrick2*)volume_rfft, vstride, (int)channels, rotation_matrices, (float2*)slices_out, g, tiles);
+    else
+        extract_multi_fwd_kernel<<<(unsigned)blocks, kTileThreads, 0, as_stream(stream)>>>(
+            (const float2*)volume_rfft, vstride, (int)channels, rotation_matrices, (float2*)slices_out, g, tiles);
     return check_launch("extract_multi_fwd_kernel");
 }
 
@@ -168,8 +203,10 @@ extern "C" int tt_extract_central_slices_rfft_3d_multichannel_backward(
     const void* volume_rfft, int64_t channels, const void* rotation_matrices, const void* grad_slices,
     void* grad_volume, void* grad_rotation, void* workspace, size_t workspace_bytes, const tt_slice_params* p,
     void* stream) {
-    if (int e = validate_params(p)) return e;
+    if (int e = validate_params(p, true)) return e;
     if (int e = check_channels(channels, "extract multichannel backward")) return e;
+    int64_t vstride;
+    if (int e = multi_volume_stride(p, vstride, "extract multichannel backward")) return e;
     if (p->deterministic)
         return fail(TT_ERR_INVALID, "extract multichannel backward: no deterministic mode; run the channels "
                                     "through tt_extract_central_slices_rfft_3d_backward");
@@ -185,23 +222,20 @@ extern "C" int tt_extract_central_slices_rfft_3d_multichannel_backward(
     if (grad_rotation && (!workspace || workspace_bytes < need))
         return fail(TT_ERR_WORKSPACE, "extract multichannel backward: workspace of %zu bytes needed, got %zu",
                     need, workspace_bytes);
-    const int64_t vstride = p->vol_d * p->vol_h * p->vol_w;
+    const int64_t dstride = p->vol_d * p->vol_h * p->vol_w;
     cudaStream_t st = as_stream(stream);
-    const float2* v = (const float2*)volume_rfft;
     const float2* gr = (const float2*)grad_slices;
     float2* dv = (float2*)grad_volume;
     float* part = (float*)workspace;
     const unsigned nb = (unsigned)blocks;
     const int c = (int)channels;
-    if (dv && grad_rotation)
-        extract_multi_bwd_kernel<true, true><<<nb, kTileThreads, 0, st>>>(v, vstride, c, rotation_matrices, gr, dv,
-                                                                        part, g, tiles);
-    else if (dv)
-        extract_multi_bwd_kernel<true, false><<<nb, kTileThreads, 0, st>>>(v, vstride, c, rotation_matrices, gr,
-                                                                         dv, part, g, tiles);
+    const bool want_dr = grad_rotation != nullptr;
+    if (p->volume_layout == TT_VOLUME_BRICKS)
+        launch_multi_bwd((const VoxBrick2*)volume_rfft, vstride, dstride, c, rotation_matrices, gr, dv, want_dr,
+                         part, g, tiles, nb, st);
     else
-        extract_multi_bwd_kernel<false, true><<<nb, kTileThreads, 0, st>>>(v, vstride, c, rotation_matrices, gr,
-                                                                         dv, part, g, tiles);
+        launch_multi_bwd((const float2*)volume_rfft, vstride, dstride, c, rotation_matrices, gr, dv, want_dr, part,
+                         g, tiles, nb, st);
     if (int e = check_launch("extract_multi_bwd_kernel")) return e;
     if (grad_rotation) return launch_drot_finish(part, rotation_matrices, grad_rotation, g, tiles, st);
     return TT_OK;

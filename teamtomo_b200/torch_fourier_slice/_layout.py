@@ -91,3 +91,22 @@ def pack(volume: torch.Tensor, params: _lib.SliceParams, layout: int) -> torch.T
         _lib.check(L.tt_pack_volume_bricks(_lib.ptr(volume), _lib.ptr(out), params, st), "pack_volume_bricks")
         return out
     raise ValueError(f"unknown volume layout {layout}")
+
+
+def pack_channels(volumes: torch.Tensor, params: _lib.SliceParams, layout: int) -> torch.Tensor | None:
+    """The channels' bricked copies back to back, as the multichannel
+    extraction takes them (one flat complex64 tensor), for ``layout`` =
+    ``BRICKS``; None for ``PLAIN`` (the multichannel kernels take no
+    x-paired copy)."""
+    if layout == PLAIN:
+        return None
+    if layout != BRICKS:
+        raise ValueError("the multichannel extraction takes plain or bricked volumes")
+    L = _lib.load()
+    st = _lib.stream_of(volumes.device)
+    slots = int(L.tt_volume_bricks_bytes(params)) // 8
+    out = torch.empty((volumes.shape[0], slots), dtype=torch.complex64, device=volumes.device)
+    for ch in range(volumes.shape[0]):
+        _lib.check(L.tt_pack_volume_bricks(_lib.ptr(volumes[ch]), _lib.ptr(out[ch]), params, st),
+                   "pack_volume_bricks")
+    return out

@@ -86,19 +86,32 @@ class _ExtractMultichannel(torch.autograd.Function):
         dev = volumes.device
         out = torch.empty(out_shape, dtype=torch.complex64, device=dev)
         L = _lib.load()
+        # large calls gather from the channels' bricked copies (bit-identical results)
+        layout = _multichannel_layout(out_shape[0] * out_shape[2] * out_shape[3], volumes)
+        copy = _layout.pack_channels(volumes, params, layout)
         _lib.check(L.tt_extract_central_slices_rfft_3d_multichannel(
-            _lib.ptr(volumes), volumes.shape[0], _lib.ptr(rotation_matrices), _lib.ptr(out), params,
-            _lib.stream_of(dev)), "extract_central_slices_rfft_3d_multichannel")
+            _lib.ptr(copy if copy is not None else volumes), volumes.shape[0], _lib.ptr(rotation_matrices),
+            _lib.ptr(out), _layout.with_layout(params, layout), _lib.stream_of(dev)),
+            "extract_central_slices_rfft_3d_multichannel")
         ctx.params = params
-        ctx.save_for_backward(volumes, rotation_matrices)
+        # the backward reads the volumes only for d/drotation: keep the copies for it
+        keep = copy is not None and ctx.needs_input_grad[1]
+        ctx.layout = layout if keep else _layout.PLAIN
+        ctx.save_for_backward(volumes, rotation_matrices, *((copy,) if keep else ()))
         return out
 
     @staticmethod
     def backward(ctx, grad):
-        volumes, R = ctx.saved_tensors
+        saved = ctx.saved_tensors
+        volumes, R = saved[0], saved[1]
         want_v, want_r = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         if not (want_v or want_r):
             return None, None, None, None
+        layout = ctx.layout
+        copy = saved[2] if layout != _layout.PLAIN else None
+        if copy is None and want_r:
+            layout = _multichannel_layout(grad.shape[0] * grad.shape[2] * grad.shape[3], volumes)
+            copy = _layout.pack_channels(volumes, ctx.params, layout)
         dev = volumes.device
         grad = _lib.dense(grad.to(torch.complex64))
         L = _lib.load()
@@ -107,10 +120,18 @@ class _ExtractMultichannel(torch.autograd.Function):
         nbytes = int(L.tt_extract_backward_workspace_bytes(ctx.params)) if want_r else 0
         ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=dev) if want_r else None
         _lib.check(L.tt_extract_central_slices_rfft_3d_multichannel_backward(
-            _lib.ptr(volumes), volumes.shape[0], _lib.ptr(R), _lib.ptr(grad), _lib.ptr(dvol), _lib.ptr(drot),
-            _lib.ptr(ws), nbytes, ctx.params, _lib.stream_of(dev)),
+            _lib.ptr(copy if copy is not None else volumes), volumes.shape[0], _lib.ptr(R), _lib.ptr(grad),
+            _lib.ptr(dvol), _lib.ptr(drot), _lib.ptr(ws), nbytes,
+            _layout.with_layout(ctx.params, layout if copy is not None else _layout.PLAIN), _lib.stream_of(dev)),
             "extract_central_slices_rfft_3d_multichannel backward")
         return dvol, drot, None, None
+
+
+def _multichannel_layout(n_pixels, volumes):
+    """Layout of a multichannel call sampling ``n_pixels`` pixels per channel:
+    the single-volume policy for one channel, the x-paired copy excepted."""
+    layout = _layout.choose(n_pixels, volumes[0])
+    return _layout.PLAIN if layout == _layout.XPAIRS else layout
 
 
 def extract_backward(volume_rfft, rotation_matrices, grad, params, want_volume=True,

@@ -62,9 +62,10 @@ def test_param_struct_layout():
 
 @pytest.mark.parametrize("layout", [1, 2])
 def test_volume_layout_validation(layout):
-    """volume_layout: the copies are accepted by the extraction entry points,
-    refused by the others, and codes outside {0, 1, 2} are refused; the packs
-    check their pointers and alignment."""
+    """volume_layout: the copies are accepted by the extraction entry points
+    (the multichannel ones take the bricked copies only), refused by the
+    others, and codes outside {0, 1, 2} are refused; the packs check their
+    pointers and alignment."""
     from teamtomo_b200 import _lib
 
     L = _lib.load()
@@ -76,8 +77,10 @@ def test_volume_layout_validation(layout):
     assert b"volume_layout" in L.tt_last_error()
     assert L.tt_insert_central_slices_rfft_3d(fake, 0, fake, fake, fake, fake, 1 << 30, ctypes.byref(p),
                                               None) == _lib.TT_ERR_INVALID
-    assert L.tt_extract_central_slices_rfft_3d_multichannel(fake, 2, fake, fake, ctypes.byref(p),
-                                                            None) == _lib.TT_ERR_INVALID
+    if layout == 1:
+        assert L.tt_extract_central_slices_rfft_3d_multichannel(fake, 2, fake, fake, ctypes.byref(p),
+                                                                None) == _lib.TT_ERR_INVALID
+        assert b"plain or bricked" in L.tt_last_error()
     # accepted (fails later, on the missing workspace, not on the layout)
     assert L.tt_extract_central_slices_rfft_3d_backward(fake, fake, fake, None, fake, None, 0,
                                                         ctypes.byref(p), None) == _lib.TT_ERR_WORKSPACE

@@ -279,3 +279,53 @@ def test_auto_policy_plain_volume_for_few_slices(monkeypatch):
     assert _layout.choose(k * n * (n // 2 + 1), vol) == _layout.PLAIN
     assert packs == []
     assert torch.equal(res["auto"][0], res["plain"][0]) and torch.equal(res["auto"][1], res["plain"][1])
+
+
+@pytest.mark.parametrize("n,c", [(64, 3), (63, 2)])
+def test_multichannel_bricks_bitwise(monkeypatch, oracle, n, c):
+    """The multichannel extraction from the channels' bricked copies equals
+    the plain volumes bitwise (slices, d/drotation; d/dvolume within
+    float-atomic reordering), and the oracle per channel; the multichannel
+    projection (an unshifted rfft source) too."""
+    import teamtomo_b200 as tt
+
+    vols = torch.stack([torch.as_tensor(rfft_volume_np(blob_volume(n, seed=500 + n + i))) for i in range(c)]).cuda()
+    Rn = rotations(40, seed=501 + n)
+    G = torch.randn((40, c, n, n // 2 + 1), dtype=torch.complex64, device="cuda",
+                    generator=torch.Generator(device="cuda").manual_seed(17))
+    real = torch.as_tensor(np.stack([blob_volume(n, seed=520 + i) for i in range(c)])).float().cuda()
+    res = {}
+    for mode in ("plain", "bricks"):
+        monkeypatch.setenv("TT_VOLUME_LAYOUT", mode)
+        R = torch.as_tensor(Rn).float().cuda().requires_grad_(True)
+        V = vols.clone().requires_grad_(True)
+        S = tt.extract_central_slices_rfft_3d_multichannel(V, (n, n, n), R)
+        (S * G.conj()).real.sum().backward()
+        P = tt.project_3d_to_2d_multichannel(real, torch.as_tensor(Rn).float().cuda())
+        res[mode] = (S.detach(), R.grad.detach(), V.grad.detach(), P)
+    a, b = res["plain"], res["bricks"]
+    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and torch.equal(a[3], b[3])
+    assert rel_l2(b[2].cpu().numpy(), a[2].cpu().numpy()) < 1e-6
+    for ch in range(c):
+        ref = oracle.extract(vols[ch].cpu().numpy(), (n, n, n), Rn.astype(np.float32))
+        assert rel_l2(b[0][:, ch].cpu().numpy(), ref) < 1e-5
+
+
+def test_multichannel_auto_policy_packs_once(monkeypatch):
+    """At least half a pixel per voxel: one bricked pack of all channels in
+    the forward, reused by the backward."""
+    import teamtomo_b200 as tt
+    from teamtomo_b200.torch_fourier_slice import _layout
+
+    n, k, c = 64, 64, 2
+    vols = torch.randn((c, n, n, n // 2 + 1), dtype=torch.complex64, device="cuda",
+                       generator=torch.Generator(device="cuda").manual_seed(19))
+    packs = []
+    real_pack = _layout.pack_channels
+    monkeypatch.setattr(_layout, "pack_channels",
+                        lambda v, p, lay: (packs.append(lay) if lay else None) or real_pack(v, p, lay))
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "auto")
+    R = torch.as_tensor(rotations(k, seed=530)).float().cuda().requires_grad_(True)
+    S = tt.extract_central_slices_rfft_3d_multichannel(vols, (n, n, n), R)
+    S.real.sum().backward()
+    assert packs == [_layout.BRICKS] and torch.isfinite(R.grad).all()
