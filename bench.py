@@ -542,7 +542,7 @@ def config_workload(args):
                                "images": n_img, "orientations": n_ext},
                     "torch_gpu_reference": None, "clocks": clk,
                     # insertion: splat, finalize, sum; fused MSE: loss kernel, loss and rotation finish
-                    # (+ the x-paired copy of the volume)
+                    # (+ the pack of the volume copy the gathers read)
                     "gpu_launches": n_img // chunk * 3
                     + n_ext // chunk * (3 + copy_launches(chunk * n * (n // 2 + 1), Vfit))})
     print(json.dumps(out))
@@ -820,7 +820,7 @@ def main():
                        "deterministic": det},
             "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "fused_mse": fused, "torch_gpu_reference": torch_gpu,
-            # extract (+ the x-paired copy of the volume it gathers from), backward,
+            # extract (+ the pack of the bricked volume copy it gathers from), backward,
             # rotation-gradient finish, insert splat, insert finalize (+ absmax
             # pre-passes and the fixed-point add-back when deterministic)
             "gpu_launches": ((8 if det else 5) + copy_launches(ns * n * (n // 2 + 1), V)) * args.steps,

@@ -349,3 +349,23 @@ def test_fused_mse_validation():
     p = _params(n=0)
     assert L.tt_central_slice_mse(fake, fake, fake, fake, None, None, fake, need, ctypes.byref(p),
                                   None) == _lib.TT_ERR_INVALID
+
+
+def test_multichannel_layout_policy(monkeypatch):
+    """The multichannel extraction follows the single-volume policy per
+    channel, except that it takes no x-paired copy."""
+    from teamtomo_b200.torch_fourier_slice import _layout
+    from teamtomo_b200.torch_fourier_slice.slice_extraction import _multichannel_layout
+
+    vols = torch.zeros((3, 16, 16, 9), dtype=torch.complex64)
+    per_channel = vols[0].numel()
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "auto")
+    assert _multichannel_layout(per_channel, vols) == _layout.BRICKS
+    assert _multichannel_layout(per_channel // 2 - 1, vols) == _layout.PLAIN
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "xpairs")
+    assert _multichannel_layout(per_channel, vols) == _layout.PLAIN
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "bricks")
+    assert _multichannel_layout(1, vols) == _layout.BRICKS
+    with pytest.raises(ValueError):
+        _layout.pack_channels(vols, None, _layout.XPAIRS)
+    assert _layout.pack_channels(vols, None, _layout.PLAIN) is None
