@@ -28,7 +28,9 @@ def _pad_amount(n: int, pad_factor: float) -> int:
 # float64 volumes: the padding, sinc^2 weighting and 3D rfft run in float64,
 # the central slices are sampled from the complex64 rounding of that rfft (the
 # extraction kernels sample complex64) and the projections are returned as
-# float64, the dtype the reference returns for them.
+# float64.  The reference raises RuntimeError for float64 volumes (its
+# grid_sample gets a float64 volume and float32 coordinates); projecting them
+# is a deliberate extension.
 def _slice_source(dft: torch.Tensor) -> torch.Tensor:
     if dft.dtype == torch.complex128:
         dft = dft.to(torch.complex64)

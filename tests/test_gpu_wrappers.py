@@ -130,10 +130,10 @@ def test_wrapper_errors():
 
 
 def test_project_float64_volumes(oracle, monkeypatch):
-    """float64 volumes project to float64 images (the reference's dtype),
-    sampled in single precision: the float32 projection of the same volume
-    within rounding, the oracle within the float32 tolerance, and a float64
-    volume gradient."""
+    """float64 volumes project to float64 images (the reference raises
+    RuntimeError for them), sampled in single precision: the float32
+    projection of the same volume within rounding, the oracle within the
+    float32 tolerance, and a float64 volume gradient."""
     vol = cuda(blob_volume(24, seed=7)).double()
     R = cuda(rotations(6, seed=8)).float()
     for graphs in ("1", "0"):  # the graph-replayed and the eager path
