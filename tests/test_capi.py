@@ -369,3 +369,17 @@ def test_multichannel_layout_policy(monkeypatch):
     with pytest.raises(ValueError):
         _layout.pack_channels(vols, None, _layout.XPAIRS)
     assert _layout.pack_channels(vols, None, _layout.PLAIN) is None
+
+
+def test_bricks_slot_limit_in_policy(monkeypatch):
+    """The gathers address a bricked copy with 32-bit slot offsets, so the
+    auto policy keeps volumes whose copy would reach 2^31 slots plain (shapes
+    only: meta tensors hold no memory)."""
+    from teamtomo_b200.torch_fourier_slice import _layout
+
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "auto")
+    fits = torch.empty((1024, 1024, 513), dtype=torch.complex64, device="meta")
+    too_big = torch.empty((2048, 2048, 1025), dtype=torch.complex64, device="meta")
+    assert _layout.bricks_fit(fits) and not _layout.bricks_fit(too_big)
+    assert _layout.choose(10**13, fits) == _layout.BRICKS
+    assert _layout.choose(10**13, too_big) == _layout.PLAIN
