@@ -383,3 +383,20 @@ def test_bricks_slot_limit_in_policy(monkeypatch):
     assert _layout.bricks_fit(fits) and not _layout.bricks_fit(too_big)
     assert _layout.choose(10**13, fits) == _layout.BRICKS
     assert _layout.choose(10**13, too_big) == _layout.PLAIN
+
+
+def test_bricks_slot_limit_in_the_c_abi():
+    """A volume whose bricked copy would hold 2^31 slots or more (1500 x 1500
+    x 1001: 2.25 G slots, below the 2^32-voxel volume limit) is refused with
+    the bricked layout and by the pack, before any launch."""
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    fake = ctypes.c_void_p(16)
+    big = dict(vol_d=1500, vol_h=1500, vol_w=1001)
+    p = _params(volume_layout=2, **big)
+    assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert b"2^31" in L.tt_last_error()
+    p = _params(**big)
+    assert L.tt_pack_volume_bricks(fake, fake, ctypes.byref(p), None) == _lib.TT_ERR_INVALID
+    assert b"2^31" in L.tt_last_error()
