@@ -6,9 +6,10 @@ reference on the GPU.
 offline: their build backend (hatchling + hatch-vcs) is not installed.  The
 packages are plain Python, so this recipe does what the install would do for
 them: it copies each package's ``src`` tree into ``baseline/_ref``.  Run it
-where the reference checkout exists:
+where the reference checkout exists, giving its root as the argument or in
+``TT_REFERENCE_ROOT``:
 
-    python baseline/install_reference.py [/path/to/reference]
+    python baseline/install_reference.py /path/to/reference
 """
 
 from __future__ import annotations
@@ -21,7 +22,10 @@ PACKAGES = ("torch-fourier-slice", "torch-image-interpolation", "torch-grid-util
 
 
 def main() -> int:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TT_REFERENCE_ROOT")
+    if not ref:
+        print("usage: install_reference.py REFERENCE_ROOT (or set TT_REFERENCE_ROOT)", file=sys.stderr)
+        return 2
     dest = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref")
     os.makedirs(dest, exist_ok=True)
     for pkg in PACKAGES:

@@ -54,6 +54,10 @@ def choose(n_pixels: int, volume: torch.Tensor) -> int:
     if volume.dtype != torch.complex64 or volume.ndim != 3:
         return PLAIN
     if mode != "auto":
+        if _MODES[mode] == BRICKS and not bricks_fit(volume):
+            raise ValueError(f"TT_VOLUME_LAYOUT=bricks: the bricked copy of a {tuple(volume.shape)} volume "
+                             "would hold 2^31 slots or more (the gathers' 32-bit slot offsets); "
+                             "use auto or plain for this volume")
         return _MODES[mode]
     return BRICKS if n_pixels >= MIN_PIXELS_PER_VOXEL * volume.numel() and bricks_fit(volume) else PLAIN
 

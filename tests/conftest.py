@@ -3,6 +3,7 @@
 from __future__ import annotations
 
 import os
+import subprocess
 import sys
 
 import numpy as np
@@ -15,6 +16,33 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    config.addinivalue_line(
+        "markers",
+        "fake_pointers: passes made-up device addresses to the C ABI to check that validation refuses "
+        "the call; run with no CUDA device visible, so that a missed check fails on the host",
+    )
+
+
+def _device_visible() -> bool:
+    import torch
+
+    return torch.cuda.is_available()
+
+
+def pytest_pyfunc_call(pyfuncitem):
+    """Tests marked ``fake_pointers`` hand addresses such as 16 to the C ABI
+    and expect a validation error before any launch.  On a machine with a GPU
+    a regression in that validation would launch a kernel on them, so there
+    the test runs in a child process that sees no CUDA device
+    (``CUDA_VISIBLE_DEVICES=""``): a missed check then fails with a CUDA
+    error on the host instead of a memory fault on the device."""
+    if pyfuncitem.get_closest_marker("fake_pointers") is None or not _device_visible():
+        return None
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-p", "no:cacheprovider", pyfuncitem.nodeid],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, f"{pyfuncitem.nodeid} with no device visible:\n{r.stdout[-4000:]}\n{r.stderr[-2000:]}"
+    return True
 
 
 def pytest_collection_modifyitems(config, items):

@@ -36,7 +36,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TT_REFERENCE_ROOT")
+if not REF:
+    sys.exit("usage: make_golden.py REFERENCE_ROOT (or set TT_REFERENCE_ROOT): the reference checkout's root")
 for pkg in ("torch-fourier-slice", "torch-image-interpolation", "torch-grid-utils"):
     sys.path.insert(0, os.path.join(REF, "packages", "primitives", pkg, "src"))
 

@@ -60,6 +60,7 @@ def test_param_struct_layout():
     assert _lib.SliceParams.volume_layout.offset == 100
 
 
+@pytest.mark.fake_pointers
 @pytest.mark.parametrize("layout", [1, 2])
 def test_volume_layout_validation(layout):
     """volume_layout: the copies are accepted by the extraction entry points
@@ -121,6 +122,7 @@ def test_volume_layout_policy(monkeypatch):
     assert (q.n, q.deterministic, q.volume_layout, p.volume_layout) == (7, 1, 2, 0)
 
 
+@pytest.mark.fake_pointers
 def test_validation_rejects_before_launch():
     from teamtomo_b200 import _lib
 
@@ -155,6 +157,7 @@ def test_validation_rejects_before_launch():
     assert L.tt_extract_central_slices_rfft_3d(fake, fake, fake, ctypes.byref(p), None) == _lib.TT_OK
 
 
+@pytest.mark.fake_pointers
 def test_batched_validation_and_layout():
     from teamtomo_b200 import _lib
 
@@ -172,6 +175,7 @@ def test_batched_validation_and_layout():
     assert L.tt_extract_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
 
 
+@pytest.mark.fake_pointers
 def test_deterministic_mode_workspace_and_validation():
     from teamtomo_b200 import _lib
 
@@ -330,6 +334,7 @@ def test_streaming_host_checks():
         streaming.InsertionAccumulator((8, 8, 8), "cpu", deterministic=True)
 
 
+@pytest.mark.fake_pointers
 def test_fused_mse_validation():
     from teamtomo_b200 import _lib
 
@@ -383,8 +388,14 @@ def test_bricks_slot_limit_in_policy(monkeypatch):
     assert _layout.bricks_fit(fits) and not _layout.bricks_fit(too_big)
     assert _layout.choose(10**13, fits) == _layout.BRICKS
     assert _layout.choose(10**13, too_big) == _layout.PLAIN
+    # a forced bricked layout names the limit instead of failing in the C ABI
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "bricks")
+    assert _layout.choose(10**13, fits) == _layout.BRICKS
+    with pytest.raises(ValueError, match="2\\^31"):
+        _layout.choose(10**13, too_big)
 
 
+@pytest.mark.fake_pointers
 def test_bricks_slot_limit_in_the_c_abi():
     """A volume whose bricked copy would hold 2^31 slots or more (1500 x 1500
     x 1001: 2.25 G slots, below the 2^32-voxel volume limit) is refused with
