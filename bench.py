@@ -15,9 +15,10 @@ Workload (one "step", the 256^3 differentiation configuration):
   slices/s = 4096 / step time.  Synthetic data stand in for the reference's
   simulated maps (no network, no dataset).
 
---impl reference times the reference algorithm on the host CPU cores (the
-oracle's C restatement of it, all threads) on a bounded sample of the same
-workload, with the same metric and unit.
+--impl reference times the reference's own torch code (baseline/_ref,
+unmodified) on the host CPU cores on a bounded sample of the same workload,
+with the same metric and unit (the oracle's C restatement stands in when
+baseline/_ref is absent).
 
 Prints ONE JSON line (rank 0).
 """
@@ -62,7 +63,9 @@ def parse_args():
     ap.add_argument("--torch-gpu-sample", type=int, default=512, help="slices timed on the reference's torch path")
     ap.add_argument("--e2e-chunk", type=int, default=256, help="slices per streamed chunk in the e2e leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=1024, help="slices per CPU-baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=1024, help="slices of the oracle-port CPU sample")
+    ap.add_argument("--ref-cpu-sample", type=int, default=32,
+                    help="slices of the reference-torch-on-CPU sample (cpu_baseline)")
     ap.add_argument("--deterministic", action="store_true",
                     help="64-bit fixed-point insertion and volume gradient (bit-reproducible)")
     ap.add_argument("--workload", choices=["differentiation", "batched", "project", "backproject", "fullscale"],
@@ -162,11 +165,69 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------
-# CPU leg (oracle port of the reference algorithm)
+# CPU legs: the reference's own torch code on the host cores (the reported
+# baseline) and the oracle's C restatement of it (a second figure)
 # ----------------------------------------------------------------------------
 
-def cpu_sample_step(O, vol_np, rots_np, targets_np, nthreads):
-    """One bounded CPU sample: extract + grad (dV, dR) + insert of len(rots) slices."""
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def reference_modules():
+    """The unmodified reference slice functions from baseline/_ref (placed
+    there by baseline/install_reference.py), or None when absent."""
+    if not os.path.isdir(os.path.join(REF_DIR, "torch_fourier_slice")):
+        return None
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    from torch_fourier_slice import extract_central_slices_rfft_3d as ref_extract
+    from torch_fourier_slice import insert_central_slices_rfft_3d as ref_insert
+
+    return ref_extract, ref_insert
+
+
+def cpu_workload(box, sample, mods, seed=ROT_SEED):
+    """The GPU arm's workload on the host: the same seeded blob volumes, the
+    first ``sample`` of its 4096 rotations, targets = central slices of the
+    second volume (taken with the reference's extraction when ``mods`` holds
+    it, else with the oracle port) plus complex noise at the same relative
+    level.  Input preparation, outside every timed region."""
+    import torch
+
+    cpu = torch.device("cpu")
+    V0 = rfft_volume_torch(blob_volume_torch(box, seed, cpu))
+    Vt = rfft_volume_torch(blob_volume_torch(box, seed + 1000, cpu))
+    R = torch.tensor(rotations(N_SLICES, seed)[:sample])
+    if mods is not None:
+        with torch.no_grad():
+            T = mods[0](Vt, (box, box, box), R.double())
+    else:
+        from oracle import oracle as O
+
+        T = torch.from_numpy(O.extract(Vt.numpy(), (box, box, box), R.numpy(), nthreads=os.cpu_count() or 1))
+    gen = torch.Generator().manual_seed(7)
+    T = T + 0.5 * T.abs().mean() * torch.randn(T.shape, dtype=T.dtype, generator=gen)
+    return V0, R, T
+
+
+def reference_cpu_step(mods, V0, R, T, box):
+    """One sample step of the reference's own code on the CPU: extraction,
+    the MSE against the targets, its autograd backward for d/drotation, and
+    the insertion of the targets.  Its autograd w.r.t. the volume expands the
+    volume per sample point (4.5 TB at 128^3 x 64 slices), so d/dvolume is
+    left out; the rotations go in as float64 (the reference zeroes near-zero
+    elements of its argument in place, which a float32 leaf refuses)."""
+    ref_extract, ref_insert = mods
+    shape = (box, box, box)
+    Rg = R.double().clone().requires_grad_(True)
+    S = ref_extract(V0, shape, Rg)
+    loss = (S - T).abs().square().mean()
+    loss.backward()
+    ref_insert(T, shape, Rg.detach())
+
+
+def port_cpu_step(O, vol_np, rots_np, targets_np, nthreads):
+    """One bounded sample of the oracle's C restatement: extract + grad
+    (dV, dR) + insert."""
     n = vol_np.shape[0]
     s = O.extract(vol_np, (n, n, n), rots_np, nthreads=nthreads)
     g = (2.0 / s.size) * (s - targets_np)
@@ -174,51 +235,89 @@ def cpu_sample_step(O, vol_np, rots_np, targets_np, nthreads):
     O.insert(targets_np, (n, n, n), rots_np, nthreads=nthreads)
 
 
-def cpu_inputs(box, sample, seed=ROT_SEED):
-    rng = np.random.default_rng(seed)
-    real = rng.standard_normal((box, box, box)).astype(np.float32)
-    vol = np.fft.fftshift(np.fft.rfftn(np.fft.fftshift(real)), axes=(0, 1)).astype(np.complex64)
-    rots = rotations(sample, seed)
-    tg = (rng.standard_normal((sample, box, box // 2 + 1)) +
-          1j * rng.standard_normal((sample, box, box // 2 + 1))).astype(np.complex64)
-    return vol, rots, tg
-
-
-def run_cpu_baseline(box, sample, repeats=1):
+def run_port_baseline(V0, R, T, repeats=1):
     from oracle import oracle as O
 
     O.lib()
     threads = os.cpu_count() or 1
-    vol, rots, tg = cpu_inputs(box, sample)
-    cpu_sample_step(O, vol, rots[:4], tg[:4], threads)  # warm
+    vol, rots, tg = V0.numpy(), R.numpy(), T.numpy()
+    port_cpu_step(O, vol, rots[:4], tg[:4], threads)  # warm
     times = []
     for _ in range(repeats):
         t0 = time.perf_counter()
-        cpu_sample_step(O, vol, rots, tg, threads)
+        port_cpu_step(O, vol, rots, tg, threads)
         times.append(time.perf_counter() - t0)
     t = min(times)
-    return {"value": sample / t, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{sample} slices of the {box}^3 step (extract + dV/dR + insert), oracle C "
+    return {"value": len(rots) / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(rots)} slices of the {vol.shape[0]}^3 step (extract + dV/dR + insert), oracle C "
                       f"restatement, OpenMP {threads} threads, best of {repeats}"}
 
 
+def run_cpu_baseline(box, ref_sample, port_sample):
+    """cpu_baseline of the GPU arm's line: the reference's torch code on the
+    host cores (kind "reference"), with the oracle port beside it."""
+    import torch
+
+    mods = reference_modules()
+    V0, R, T = cpu_workload(box, max(ref_sample, port_sample), mods)
+    port = run_port_baseline(V0, R[:port_sample], T[:port_sample])
+    if mods is None:
+        port["reference"] = {"unavailable": "baseline/_ref missing (run baseline/install_reference.py)"}
+        return port
+    reference_cpu_step(mods, V0, R[:2], T[:2], box)  # warm
+    t0 = time.perf_counter()
+    reference_cpu_step(mods, V0, R[:ref_sample], T[:ref_sample], box)
+    t = time.perf_counter() - t0
+    return {"value": ref_sample / t, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "reference",
+            "host_cpus": os.cpu_count(),
+            "sample": f"{ref_sample} of the 4096 slices of the {box}^3 step: the reference's torch code "
+                      f"(baseline/_ref, unmodified) on the CPU, extraction + MSE + autograd d/drotation + "
+                      f"insertion; d/dvolume excluded (the reference's autograd expands the volume per point)",
+            "port": port}
+
+
 def reference_arm(args):
+    """--impl reference: the reference's own torch code on the host cores,
+    every step a bounded sample of the 4096-slice step sized so that the
+    whole run stays within about two minutes (the oracle port stands in when
+    baseline/_ref is absent)."""
+    import torch
+
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle import oracle as O
+    mods = reference_modules()
+    probe = 2
+    V0, R, T = cpu_workload(args.box, 64, mods)
+    if mods is not None:
+        kind, threads = "reference", torch.get_num_threads()
 
-    O.lib()
-    threads = os.cpu_count() or 1
-    sample = args.cpu_sample
-    vol, rots, tg = cpu_inputs(args.box, sample)
+        def step(k):
+            reference_cpu_step(mods, V0, R[:k], T[:k], args.box)
+    else:
+        from oracle import oracle as O
+
+        O.lib()
+        kind, threads = "port", os.cpu_count() or 1
+        vol, rots, tg = V0.numpy(), R.numpy(), T.numpy()
+
+        def step(k):
+            port_cpu_step(O, vol, rots[:k], tg[:k], threads)
+    t0 = time.perf_counter()
+    step(probe)
+    per_slice = (time.perf_counter() - t0) / probe
+    total_steps = max(args.steps, 1) + max(args.warmup, 0)
+    sample = int(max(2, min(64, 120.0 / total_steps / max(per_slice, 1e-6))))
     for _ in range(args.warmup):
-        cpu_sample_step(O, vol, rots[:8], tg[:8], threads)
+        step(sample)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        cpu_sample_step(O, vol, rots, tg, threads)
+        step(sample)
     dt = time.perf_counter() - t0
     value = sample * args.steps / dt
+    what = ("the reference's torch code (baseline/_ref, unmodified) on the CPU: extraction + MSE + autograd "
+            "d/drotation + insertion; d/dvolume excluded (the reference's autograd expands the volume per "
+            "point)") if kind == "reference" else "oracle C restatement (baseline/_ref absent), OpenMP"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
@@ -226,8 +325,9 @@ def reference_arm(args):
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "box": args.box, "slices_per_step": sample,
                    "note": "each step is a bounded sample of the 4096-slice step"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{sample} slices per step of the {args.box}^3 step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "host_cpus": os.cpu_count(),
+                         "sample": f"{sample} slices per step of the {args.box}^3 step: {what}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -247,13 +347,10 @@ def torch_gpu_reference(dev, n, V0, R0, T, sample, chunk=128):
     128^3 x 64 slices), so d/dvolume is left out of this leg."""
     import torch
 
-    ref_dir = os.path.join(ROOT, "baseline", "_ref")
-    if not os.path.isdir(os.path.join(ref_dir, "torch_fourier_slice")):
+    mods = reference_modules()
+    if mods is None:
         return {"unavailable": "baseline/_ref missing (run baseline/install_reference.py where the reference is)"}
-    if ref_dir not in sys.path:
-        sys.path.insert(0, ref_dir)
-    from torch_fourier_slice import extract_central_slices_rfft_3d as ref_extract
-    from torch_fourier_slice import insert_central_slices_rfft_3d as ref_insert
+    ref_extract, ref_insert = mods
 
     shape = (n, n, n)
     sample = min(sample, R0.shape[0])
@@ -751,8 +848,13 @@ def main():
         hT = T.cpu().pin_memory()
         h_loss = torch.empty((), dtype=torch.float32).pin_memory()
         h_dR = torch.empty_like(hR).pin_memory()
+        # every result of the step comes back: loss, d/drotation, d/dvolume and
+        # the inserted (volume, weights)
+        h_dV = torch.empty_like(hV).pin_memory()
+        h_vol = torch.empty_like(hV).pin_memory()
+        h_w = torch.empty(hV.shape, dtype=torch.float32).pin_memory()
         h2d = hV.numel() * 8 + hR.numel() * 4 + hT.numel() * 8
-        d2h = 4 + h_dR.numel() * 4
+        d2h = 4 + h_dR.numel() * 4 + h_dV.numel() * 8 + h_vol.numel() * 8 + h_w.numel() * 4
         bound = float(torch.view_as_real(hT).abs().max()) if det else None  # input property, outside the timing
         m_total = hT.numel()
 
@@ -769,11 +871,15 @@ def main():
                 loss += lc.detach()
                 acc.add(Tc, Rc.detach())
                 h_dR[s0:s1].copy_(Rc.grad, non_blocking=True)
-            vol, w = acc.finalize()
             if world > 1:
                 tt.distributed.all_reduce_volume_gradient(Vd.grad)
+            h_dV.copy_(Vd.grad, non_blocking=True)
+            vol, w = acc.finalize()
+            if world > 1:
                 tt.distributed.all_reduce_sum(vol)
                 tt.distributed.all_reduce_sum(w)
+            h_vol.copy_(vol, non_blocking=True)
+            h_w.copy_(w, non_blocking=True)
             h_loss.copy_(loss, non_blocking=True)
 
         e2e_steps = max(3, min(args.steps, 10))
@@ -794,7 +900,8 @@ def main():
             el2 = float(t.item())
         e2e = {"value": world * ns * e2e_steps / (el2 / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "steps": e2e_steps, "chunk_slices": args.e2e_chunk,
-               "overlap": "H2D of chunk k+1 on a copy stream during compute of chunk k"}
+               "overlap": "H2D of chunk k+1 on a copy stream during compute of chunk k",
+               "d2h": "loss, d/drotation, d/dvolume, inserted volume and weights"}
 
     torch_gpu = None
     if rank == 0 and world == 1 and not args.no_torch_gpu:
@@ -806,7 +913,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = run_cpu_baseline(n, args.cpu_sample)
+        cpu = run_cpu_baseline(n, args.ref_cpu_sample, args.cpu_sample)
 
     if rank == 0:
         line = {

@@ -8,6 +8,8 @@ and bitwise invariance of the deterministic mode to how the work is split.
 
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -86,6 +88,17 @@ def test_differentiation_256cube_4096_slices(oracle):
     (vol_i * H.conj()).real.sum().backward()
     rhs = torch.sum(G.to(torch.complex128) * Xg.grad.to(torch.complex128).conj()).real.item()
     assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+    # the full d/dvolume and the full insertion (volume and weights) of all
+    # 4096 slices against the oracle (OpenMP, a few seconds each)
+    threads = os.cpu_count() or 1
+    G_np, R_np = G.cpu().numpy(), R.cpu().numpy()
+    ref_dv, _ = oracle.extract_grad(vol, (n, n, n), R_np, G_np, want_drot=False, nthreads=threads)
+    assert rel_l2(Vg.grad.cpu().numpy(), ref_dv) < 1e-5
+    w_i = tt().insert_central_slices_rfft_3d(G, (n, n, n), R)[1]
+    rv, rw = oracle.insert(G_np, (n, n, n), R_np, nthreads=threads)
+    assert rel_l2(vol_i.detach().cpu().numpy(), rv) < 1e-5
+    assert rel_l2(w_i.cpu().numpy(), rw) < 1e-5
+    assert np.array_equal(w_i.cpu().numpy() != 0, rw != 0)
 
 
 def test_batched_uneven_ctf_configuration(oracle):
@@ -136,3 +149,78 @@ def test_full_scale_320cube_streamed_insertion():
     # float32 sums of 40,000 terms per low-frequency voxel: summation noise, within 1e-5
     assert rel_l2(vf.cpu().numpy(), out[0][0].cpu().numpy()) < 1e-5
     assert rel_l2(wf.cpu().numpy(), out[0][1].cpu().numpy()) < 1e-5
+
+
+def test_full_scale_320cube_ctf_insertion_vs_oracle(oracle):
+    """The full-scale configuration's CTF-weighted insertion (per-image
+    defocus U(0.8, 2.5) um, 300 kV, Cs 2.7 mm, Ac 0.07, 1 A/px) at 320^3, on
+    3,000 images, against the oracle: volume = insertion of ctf * image,
+    weights = insertion of ctf^2."""
+    from teamtomo_b200 import batched as B
+
+    n, k = 320, 3_000
+    rng = np.random.default_rng(1005)
+    imgs = (rng.standard_normal((k, n, n // 2 + 1)) + 1j * rng.standard_normal((k, n, n // 2 + 1)))
+    imgs = imgs.astype(np.complex64)
+    rots = rotations(k, seed=1005).astype(np.float32)
+    defocus = rng.uniform(0.8, 2.5, k)
+    ctf = B.ctf_params(defocus, voltage_kv=300.0, spherical_aberration_mm=2.7, amplitude_contrast=0.07,
+                       pixel_size_a=1.0, device="cuda")
+    (vol, w), = B.insert_central_slices_rfft_3d_batched([cuda(imgs)], [cuda(rots)], ctf=[ctf])
+    threads = os.cpu_count() or 1
+    cc = ctf.cpu().numpy()
+    rv = np.zeros((n, n, n // 2 + 1), np.complex128)
+    rw = np.zeros((n, n, n // 2 + 1), np.float64)
+    for a in range(0, k, 500):  # the insertion is linear: sum the chunks' volumes
+        c = np.stack([oracle.ctf_2d(*cc[j], image_shape=(n, n)) for j in range(a, min(a + 500, k))])
+        v1, _ = oracle.insert((imgs[a:a + 500] * c).astype(np.complex64), (n, n, n), rots[a:a + 500],
+                              nthreads=threads)
+        v2, _ = oracle.insert((c * c).astype(np.complex64), (n, n, n), rots[a:a + 500], nthreads=threads)
+        rv += v1
+        rw += v2.real
+    assert rel_l2(vol.cpu().numpy(), rv) < 1e-5
+    assert rel_l2(w.cpu().numpy(), rw) < 1e-5
+
+
+def test_full_scale_320cube_100k_orientation_extraction(oracle):
+    """The full-scale configuration's 100,000-orientation extraction with
+    forward and backward at 320^3, in chunks of 10,000: sampled slices and
+    their rotation gradients against the oracle, the volume gradient of the
+    first 1,000 slices against the oracle, and the adjoint identity of the
+    whole pass."""
+    n, k, chunk = 320, 100_000, 10_000
+    vol = rfft_volume_np(blob_volume(n, seed=1005))
+    V = cuda(vol)
+    R_all = cuda(rotations(k, seed=1006)).float()
+    Vg = V.clone().requires_grad_(True)
+    pick = np.sort(np.random.default_rng(7).choice(k, 16, replace=False))
+    lhs = 0.0
+    S_pick, G_pick, dR_pick = [], [], []
+    for a in range(0, k, chunk):
+        Rc = R_all[a:a + chunk].clone().requires_grad_(True)
+        S = tt().extract_central_slices_rfft_3d(Vg, (n, n, n), Rc)
+        G = torch.randn(S.shape, dtype=S.dtype, device="cuda",
+                        generator=torch.Generator(device="cuda").manual_seed(a))
+        (S * G.conj()).real.sum().backward()
+        lhs += torch.sum(S.detach().to(torch.complex128) * G.to(torch.complex128).conj()).real.item()
+        sel = [int(i) - a for i in pick if a <= i < a + chunk]
+        S_pick.append(S.detach()[sel].cpu().numpy())
+        G_pick.append(G[sel].cpu().numpy())
+        dR_pick.append(Rc.grad[sel].cpu().numpy())
+        del S, G
+    rhs = torch.sum(Vg.grad.to(torch.complex128) * V.to(torch.complex128).conj()).real.item()
+    assert abs(lhs - rhs) <= 1e-5 * abs(lhs)
+    Rp = R_all[pick].cpu().numpy()
+    threads = os.cpu_count() or 1
+    assert rel_l2(np.concatenate(S_pick), oracle.extract(vol, (n, n, n), Rp, nthreads=threads)) < 1e-6
+    _, dr = oracle.extract_grad(vol, (n, n, n), Rp, np.concatenate(G_pick), want_dvol=False, nthreads=threads)
+    assert rel_l2(np.concatenate(dR_pick), dr) < 1e-5
+    # volume gradient of the first 1,000 slices
+    m = 1_000
+    Vm = V.clone().requires_grad_(True)
+    Sm = tt().extract_central_slices_rfft_3d(Vm, (n, n, n), R_all[:m])
+    Gm = torch.randn(Sm.shape, dtype=Sm.dtype, device="cuda", generator=torch.Generator(device="cuda").manual_seed(1))
+    (Sm * Gm.conj()).real.sum().backward()
+    ref_dv, _ = oracle.extract_grad(vol, (n, n, n), R_all[:m].cpu().numpy(), Gm.cpu().numpy(), want_drot=False,
+                                    nthreads=threads)
+    assert rel_l2(Vm.grad.cpu().numpy(), ref_dv) < 1e-5
