@@ -68,7 +68,10 @@ def parse_args():
                     help="slices of the reference-torch-on-CPU sample (cpu_baseline)")
     ap.add_argument("--deterministic", action="store_true",
                     help="64-bit fixed-point insertion and volume gradient (bit-reproducible)")
-    ap.add_argument("--workload", choices=["differentiation", "batched", "project", "backproject", "fullscale"],
+    ap.add_argument("--case", choices=KERNEL_CASES, default=None,
+                    help="with --workload kernels: run only this case")
+    ap.add_argument("--workload", choices=["differentiation", "batched", "project", "backproject", "fullscale",
+                                           "kernels"],
                     default="differentiation",
                     help="differentiation: the 256^3 extract+insert+bwd step (headline); batched: 32 "
                          "uneven CTF-weighted volumes in one graph-captured launch per stage")
@@ -646,6 +649,201 @@ def config_workload(args):
     return 0
 
 
+# ----------------------------------------------------------------------------
+# per-kernel cases: one small invocation of each kernel, for ncu captures
+# (``--workload kernels --case NAME``) and live per-kernel timings (all cases)
+# ----------------------------------------------------------------------------
+
+KERNEL_CASES = ("extract", "backward", "mse", "insert", "insert_bwd", "det_insert", "det_backward",
+                "batched_extract", "batched_insert", "sample3d", "insert3d", "affine3d", "mc_extract",
+                "mc_backward", "mc_insert", "lines", "project", "backproject", "pack_bricks")
+
+
+def kernel_case(name, dev):
+    """Inputs and one call of case ``name``: returns (fn, algorithmic bytes
+    per call, the kernels the call launches).  Inputs exceed the L2 (126 MB)
+    where the kernel's own data allow, but stay at a few GB on the device."""
+    import torch
+
+    import teamtomo_b200 as tt
+    from teamtomo_b200 import batched as B
+    from teamtomo_b200.torch_fourier_slice import _layout
+    from teamtomo_b200.torch_fourier_slice._params import slice_params
+
+    n, ns = 256, 512
+    P, vox = n * (n // 2 + 1), n * n * (n // 2 + 1)
+    shape = (n, n, n)
+    gen = torch.Generator(device=dev).manual_seed(11)
+
+    def crandn(*sh):
+        return torch.randn(sh, dtype=torch.complex64, device=dev, generator=gen)
+
+    V = rfft_volume_torch(blob_volume_torch(n, ROT_SEED, dev))
+    R = torch.tensor(rotations(ns, ROT_SEED), device=dev)
+    if name == "extract":
+        return (lambda: tt.extract_central_slices_rfft_3d(V, shape, R)), ns * 8 * P + 8 * vox, \
+            "pack_bricks_kernel, extract_fwd_kernel<VoxBrick2>"
+    if name in ("backward", "det_backward"):
+        Vg = V.clone().requires_grad_(True)
+        Rg = R.clone().requires_grad_(True)
+        G = crandn(ns, n, n // 2 + 1)
+        det = name == "det_backward"
+
+        def fn():
+            Vg.grad = None
+            Rg.grad = None
+            S = tt.extract_central_slices_rfft_3d(Vg, shape, Rg, deterministic=det)
+            S.backward(G)
+        return fn, ns * 8 * P + 16 * vox, "extract_bwd_kernel (+ forward, pack, drot_finish)"
+    if name == "mse":
+        Vg = V.clone().requires_grad_(True)
+        Rg = R.clone().requires_grad_(True)
+        T = crandn(ns, n, n // 2 + 1)
+
+        def fn():
+            Vg.grad = None
+            Rg.grad = None
+            tt.losses.central_slice_mse(Vg, shape, Rg, T).backward()
+        return fn, ns * 8 * P + 16 * vox, "slice_mse_kernel (+ pack, loss and drot finish)"
+    if name in ("insert", "det_insert"):
+        T = crandn(ns, n, n // 2 + 1)
+        det = name == "det_insert"
+        return (lambda: tt.insert_central_slices_rfft_3d(T, shape, R, deterministic=det)), \
+            ns * 8 * P + 12 * vox, "insert_accumulate_kernel / insert_fixed_kernel + finalize"
+    if name == "insert_bwd":
+        T = crandn(ns, n, n // 2 + 1).requires_grad_(True)
+        H = crandn(n, n, n // 2 + 1)
+
+        def fn():
+            T.grad = None
+            v, _ = tt.insert_central_slices_rfft_3d(T, shape, R)
+            v.backward(H)
+        return fn, 8 * vox + ns * 8 * P, "insert_bwd_kernel (+ the insertion)"
+    return kernel_case_more(name, dev, V, R, crandn, gen)
+
+
+def kernel_case_more(name, dev, V, R, crandn, gen):
+    """The cases of kernel_case beyond the single-volume slice kernels."""
+    import torch
+
+    import teamtomo_b200 as tt
+    from teamtomo_b200 import batched as B
+    from teamtomo_b200.torch_fourier_slice import _layout
+    from teamtomo_b200.torch_fourier_slice._params import slice_params
+
+    n = 256
+    P, vox = n * (n // 2 + 1), n * n * (n // 2 + 1)
+    if name in ("batched_extract", "batched_insert"):
+        boxes = (64, 96, 128, 160, 200, 256, 96, 128)
+        counts = (2000,) * len(boxes)
+        vols = [rfft_volume_torch(blob_volume_torch(b, 2000 + i, dev)) for i, b in enumerate(boxes)]
+        rots = [torch.tensor(rotations(c, 3000 + i), device=dev) for i, c in enumerate(counts)]
+        rng = np.random.default_rng(1004)
+        ctfs = [B.ctf_params(rng.uniform(0.5, 3.0, c), device=dev) for c in counts]
+        slice_bytes = sum(c * 8 * b * (b // 2 + 1) for c, b in zip(counts, boxes))
+        vb = sum(b * b * (b // 2 + 1) for b in boxes)
+        if name == "batched_extract":
+            return (lambda: B.extract_central_slices_rfft_3d_batched(vols, rots, ctf=ctfs)), slice_bytes + 8 * vb, \
+                "batched_slices_kernel<extract>"
+        sl = B.extract_central_slices_rfft_3d_batched(vols, rots, ctf=ctfs)
+        return (lambda: B.insert_central_slices_rfft_3d_batched(sl, rots, ctf=ctfs)), slice_bytes + 12 * vb, \
+            "batched_slices_kernel<insert> + insert_finalize_kernel"
+    if name in ("sample3d", "insert3d"):
+        m = 1 << 24
+        img = torch.randn((n, n, n), device=dev, generator=gen)
+        coords = torch.rand((m, 3), device=dev, generator=gen) * (n - 1)
+        if name == "sample3d":
+            return (lambda: tt.sample_image_3d(img, coords)), 4 * n ** 3 + 16 * m, "sample3d_kernel"
+        vals = torch.randn(m, device=dev, generator=gen)
+        return (lambda: tt.insert_into_image_3d(vals, coords, torch.zeros_like(img))), 16 * m + 8 * n ** 3, \
+            "insert3d_kernel"
+    if name == "affine3d":
+        img = torch.randn((n, n, n), device=dev, generator=gen)
+        M = torch.eye(4, device=dev)
+        M[:3, :3] = torch.tensor(rotations(1, 5)[0], device=dev, dtype=torch.float32)
+        return (lambda: tt.torch_transform_image.affine_transform_image_3d(img, M, "trilinear")), 8 * n ** 3, \
+            "affine3d_kernel"
+    if name.startswith("mc_"):
+        c, ns = 4, 256
+        vols = torch.stack([rfft_volume_torch(blob_volume_torch(n, 4000 + i, dev)) for i in range(c)])
+        Rm = R[:ns]
+        if name == "mc_extract":
+            return (lambda: tt.extract_central_slices_rfft_3d_multichannel(vols, (n, n, n), Rm)), \
+                c * (ns * 8 * P + 8 * vox), "multichannel extraction kernel"
+        if name == "mc_backward":
+            Vg = vols.clone().requires_grad_(True)
+            Rg = Rm.clone().requires_grad_(True)
+            G = crandn(ns, c, n, n // 2 + 1)
+
+            def fn():
+                Vg.grad = None
+                Rg.grad = None
+                tt.extract_central_slices_rfft_3d_multichannel(Vg, (n, n, n), Rg).backward(G)
+            return fn, c * (ns * 8 * P + 16 * vox), "multichannel backward kernel"
+        T = crandn(ns, c, n, n // 2 + 1)
+        return (lambda: tt.insert_central_slices_rfft_3d_multichannel(T, (n, n, n), Rm)), \
+            c * (ns * 8 * P + 8 * vox) + 4 * vox, "insert_accumulate_kernel per channel + finalize"
+    if name == "lines":
+        h = 4096
+        img = crandn(h, h // 2 + 1)
+        th = torch.rand(65536, device=dev, generator=gen) * 6.283185307
+        R2 = torch.stack([torch.stack([th.cos(), -th.sin()], -1), torch.stack([th.sin(), th.cos()], -1)], -2)
+        return (lambda: tt.extract_central_slices_rfft_2d(img, (h, h), R2)), 65536 * 8 * (h // 2 + 1) + 8 * h * (
+            h // 2 + 1), "line_extract_kernel"
+    if name == "project":
+        b, k = 128, 2048
+        vol = blob_volume_torch(b, 1001, dev)
+        Rp = torch.tensor(rotations(k, 1001), device=dev)
+        # non-FFT bytes: pad x sinc^2 (read b^3, write (2b)^3), extraction (write k (2b)(b+1)),
+        # recentre / crop (read k (2b)^2, write k b^2), all float32 / complex64
+        return (lambda: tt.project_3d_to_2d(vol, Rp)), 4 * b ** 3 + 4 * (2 * b) ** 3 + k * 8 * 2 * b * (b + 1) + \
+            k * 4 * ((2 * b) ** 2 + b * b), "project_prepare_kernel, extraction, recentre_crop_2d_kernel"
+    if name == "backproject":
+        b, k = 128, 2048
+        imgs = torch.randn((k, b, b), device=dev, generator=gen)
+        Rp = torch.tensor(rotations(k, 1002), device=dev)
+        return (lambda: tt.backproject_2d_to_3d(imgs, Rp)), k * 4 * (b * b + (2 * b) ** 2) + k * 8 * 2 * b * (
+            b + 1) + 20 * (2 * b) ** 2 * (b + 1) + 8 * (2 * b) ** 3, \
+            "pad_fftshift_2d_kernel, insertion, normalize_unshift_kernel, backproject_finish_kernel"
+    if name == "pack_bricks":
+        p = slice_params(n=1, image_shape=(n, n, n), volume=V, rotation=R)
+        return (lambda: _layout.pack(V, p, _layout.BRICKS)), 16 * vox, "pack_bricks_kernel"
+    raise ValueError(f"unknown kernel case {name!r}")
+
+
+def kernels_workload(args):
+    """--workload kernels: each case (or --case NAME) once for warm-up, then
+    the measured calls inside an NVTX range named "measured" (ncu:
+    --nvtx --nvtx-include measured/), with CUDA-event times on the current
+    stream; one JSON line per case."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    names = [args.case] if args.case else list(KERNEL_CASES)
+    for name in names:
+        fn, algo, kernels = kernel_case(name, dev)
+        fn()
+        torch.cuda.synchronize(dev)
+        reps = max(args.steps, 1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("measured")
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize(dev)
+        ms = a.elapsed_time(b) / reps
+        peak, kind = load_peaks()
+        print(json.dumps({"case": name, "kernels": kernels, "ms_per_call": round(ms, 4), "algorithmic_bytes": algo,
+                          "achieved_gbs": round(algo / ms / 1e6, 1), "frac_of_peak": round(algo / ms / 1e6 / peak, 4),
+                          "peak_gbs": peak, "peak_source": kind}), flush=True)
+        del fn
+        torch.cuda.empty_cache()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -654,6 +852,8 @@ def main():
         return batched_workload(args)
     if args.workload in ("project", "backproject", "fullscale"):
         return config_workload(args)
+    if args.workload == "kernels":
+        return kernels_workload(args)
 
     import torch
     import torch.distributed as dist

@@ -52,18 +52,24 @@ extract_fwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
     const int ty = blockIdx.x - (int)(s * rows);
     load_rotation(m, rot, s, g, true);
     __syncthreads();
+    // this thread's pixels share one slice row across the row of tiles
+    const int lane = threadIdx.x & 31;
+    const int iy = ty * kTileY + (threadIdx.x >> 5) * 4 + (lane >> 3);
+    if (iy >= g.img_h) return;
+    const SliceRow row = slice_row_geom(g, m, iy);
+    float2* orow = out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr;
     for (int tx = 0; tx < tx_tiles; tx++) {
-        int iy, ix;
-        if (!tile_pixel(g, ty * tx_tiles + tx, iy, ix)) continue;
-        float qy, qx, c[3];
+        const int ix = tx * kTileX + (lane & 7);
+        if (ix >= g.wr) continue;
+        float qx, c[3];
         bool cj = false;
         float2 r = make_float2(0.0f, 0.0f);
-        if (extract_geometry(g, m, iy, ix, qy, qx, cj, c)) {
+        if (extract_geometry_row(g, m, row, ix, qx, cj, c)) {
             r = sample_trilinear(vol, g, make_corners(g, c));
             if (cj) r.y = -r.y;
         }
         // streaming store: the slices are written once and should not evict the volume from L2
-        __stcs(out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, r);
+        __stcs(orow + ix, r);
     }
 }
 

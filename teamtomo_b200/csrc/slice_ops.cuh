@@ -95,6 +95,43 @@ __device__ __forceinline__ bool extract_geometry(const SliceGeom& g, const float
     return inside_volume(g, c);
 }
 
+// The part of the extraction geometry that depends only on the slice row:
+// its frequency qy, qy^2 for the fftfreq_max test, and the rotation's products
+// m[i][1] * qy, each rounded as rotate_slice_point rounds it.  The slice
+// kernels walk a row of tiles with a fixed row per thread, so these are formed
+// once per thread instead of once per pixel.
+struct SliceRow {
+    float qy, qy2, my[3];
+};
+
+__device__ __forceinline__ SliceRow slice_row_geom(const SliceGeom& g, const float* m, int iy) {
+    SliceRow r;
+    r.qy = shifted_freq(iy, g.img_h, g.inv_h);
+    r.qy2 = __fmul_rn(r.qy, r.qy);
+#pragma unroll
+    for (int i = 0; i < 3; i++) r.my[i] = __fmul_rn(m[i * 3 + 1], r.qy);
+    return r;
+}
+
+// extract_geometry with the row part precomputed: the same operations and
+// roundings, so the same flags and coordinates bit for bit.
+__device__ __forceinline__ bool extract_geometry_row(const SliceGeom& g, const float* m, const SliceRow& row, int ix,
+                                                     float& qx, bool& cj, float c[3]) {
+    qx = __fmul_rn((float)ix, g.inv_w);
+    if (g.has_fmax && !(__fsqrt_rn(__fadd_rn(row.qy2, __fmul_rn(qx, qx))) <= g.fmax)) return false;
+    float p[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) p[i] = __fadd_rn(row.my[i], __fmul_rn(m[i * 3 + 2], qx));
+    cj = extract_conj(g, m, p[2]);
+    if (cj) {
+        p[0] = -p[0];
+        p[1] = -p[1];
+        p[2] = -p[2];
+    }
+    to_dft_coords(g, p, c);
+    return inside_volume(g, c);
+}
+
 // Element type of the bricked copy (brick_index addressing): one complex64 voxel.
 struct VoxBrick2 {
     float x, y;

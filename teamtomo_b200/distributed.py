@@ -9,11 +9,11 @@ box, 132 MB at 320^3) and a shard of the slices / images.
   partial gradients: ``replicate_volume`` marks the volume so that its
   gradient is all-reduced (SUM) in the backward pass.
 * Insertion: each rank splats its shard; one all-reduce sums the partial
-  (volume, weights).  The Friedel completion is linear, so it is applied
-  before the sum.
+  volume and weights, packed side by side.  The Friedel completion is
+  linear, so it is applied before the sum.
 * Deterministic insertion: the ranks first agree on one fixed-point scale
   (MAX all-reduce of the absmax word, SUM of the slice counts), accumulate
-  64-bit integers, and all-reduce the integers.  Integer sums are exact, so
+  64-bit integers, and all-reduce the three live integer words per voxel.  Integer sums are exact, so
   the result is bit-identical for any number of ranks and any sharding.
 
 The collectives are the only data exchanged; nothing crosses NVLink in the
@@ -105,13 +105,23 @@ def insert_central_slices_rfft_3d(
     if not resolve_deterministic(deterministic):
         volume, weights = _ins.insert_central_slices_rfft_3d(img, volume_shape, R, fftfreq_max=fftfreq_max,
                                                              zyx_matrices=zyx_matrices, deterministic=False)
-        return _all_reduce_sum(volume, group), _all_reduce_sum(weights, group)
+        # one collective for both: (re, im) of the volume and the weights side by side
+        re_im = torch.view_as_real(volume).reshape(-1)
+        flat = torch.cat([re_im, weights.reshape(-1).to(re_im.dtype)])
+        dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+        re_im.copy_(flat[:re_im.numel()])
+        weights.reshape(-1).copy_(flat[re_im.numel():])
+        return volume, weights
     # one scale for all ranks: the largest |re|, |im| anywhere and the total slice count
     absmax = _ins.fixed_absmax(img)
     dist.all_reduce(absmax, op=dist.ReduceOp.MAX, group=group)
     total = max(_sum_count(n, dev, group), 1)
     acc = _ins.new_fixed_accumulator(volume_shape, dev)
     _ins.insert_fixed_accumulate(img, R, volume_shape, acc[0], absmax, total, fftfreq_max, zyx_matrices)
-    dist.all_reduce(acc, op=dist.ReduceOp.SUM, group=group)  # exact integer sum
+    # exact integer sum of the three live words per voxel (re, im, w), without
+    # the slot's pad word: a quarter fewer bytes on the wire
+    live = acc[..., :3].contiguous()
+    dist.all_reduce(live, op=dist.ReduceOp.SUM, group=group)
+    acc[..., :3] = live
     volume, weights = _ins.insert_fixed_finalize(acc, c128, absmax, total)
     return volume[0], weights
