@@ -475,9 +475,16 @@ def batched_workload(args):
     vox = [b * b * (b // 2 + 1) for b in boxes]
     # extraction writes 8P per slice + reads the volume once; insertion reads 8P
     # per slice + writes volume and weights once
-    algo = sum(c * 16 * p for c, p in zip(counts, P)) + sum(20 * v for v in vox)
+    algo_e = sum(c * 8 * p for c, p in zip(counts, P)) + sum(8 * v for v in vox)
+    algo_i = sum(c * 8 * p for c, p in zip(counts, P)) + sum(12 * v for v in vox)
+    algo = algo_e + algo_i
     peak, peak_kind = load_peaks()
     gbs = algo / (ms / 1e3) / 1e9
+    # DRAM traffic: the ncu captures' traffic per algorithmic byte of each stage
+    # (8 volumes x 2000 slices, profiles/ncu_batched_*), scaled to this step
+    tr = load_traffic()
+    re_, ri_ = tr.get("batched_extract_per_algorithmic_byte"), tr.get("batched_insert_per_algorithmic_byte")
+    traffic = int(re_ * algo_e + ri_ * algo_i) if re_ and ri_ else None
     line = {
         "metric": "slices/s CTF-weighted extract+insert, 32 uneven volumes, one launch per stage",
         "value": total / (ms / 1e3), "unit": "slices/s", "n_gpus": 1, "steps": args.steps,
@@ -487,9 +494,12 @@ def batched_workload(args):
                    "total_slices": total, "tile_shapes": {"extract": ts_e, "insert": ts_i},
                    "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(gbs / peak, 4), "traffic": None, "kernel": "extract+insert step",
-                     "peak_source": peak_kind},
-        "autotune_ms": {k: {str(s): round(t, 4) for s, t in v.items()} for k, v in tuned.items()},
+                     "frac": round(gbs / peak, 4), "traffic": traffic, "kernel": "extract+insert step",
+                     "peak_source": peak_kind,
+                     "traffic_source": "ncu per-algorithmic-byte traffic of the batched stages at 8 volumes x "
+                                       "2000 slices, scaled to this step's algorithmic bytes"},
+        "autotune_ms": {k: {(f"{s[0]}/{s[1]}" if s[1] else str(s[0])): round(t, 4) for s, t in v.items()}
+                        for k, v in tuned.items()},
         "clocks": clk, "gpu_launches": args.steps * (3 + nvol),
     }
     del outs
@@ -1073,15 +1083,19 @@ def main():
                 h_dR[s0:s1].copy_(Rc.grad, non_blocking=True)
             if world > 1:
                 tt.distributed.all_reduce_volume_gradient(Vd.grad)
-            h_dV.copy_(Vd.grad, non_blocking=True)
             vol, w = acc.finalize()
             if world > 1:
                 tt.distributed.all_reduce_sum(vol)
                 tt.distributed.all_reduce_sum(w)
-            h_vol.copy_(vol, non_blocking=True)
-            h_w.copy_(w, non_blocking=True)
-            h_loss.copy_(loss, non_blocking=True)
+            # the results go out on their own stream: the device-to-host copies
+            # of this step overlap the host-to-device copies of the next one
+            d2h.wait_stream(stream)
+            with torch.cuda.stream(d2h):
+                for src, dst in ((Vd.grad, h_dV), (vol, h_vol), (w, h_w), (loss, h_loss)):
+                    src.record_stream(d2h)
+                    dst.copy_(src, non_blocking=True)
 
+        d2h = torch.cuda.Stream(device=dev)
         e2e_steps = max(3, min(args.steps, 10))
         e2e_step()
         torch.cuda.synchronize(dev)
@@ -1091,6 +1105,7 @@ def main():
         s2.record(stream)
         for _ in range(e2e_steps):
             e2e_step()
+        stream.wait_stream(d2h)  # the last step's results are on the host before the clock stops
         e2.record(stream)
         torch.cuda.synchronize(dev)
         el2 = s2.elapsed_time(e2)
@@ -1100,7 +1115,8 @@ def main():
             el2 = float(t.item())
         e2e = {"value": world * ns * e2e_steps / (el2 / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "steps": e2e_steps, "chunk_slices": args.e2e_chunk,
-               "overlap": "H2D of chunk k+1 on a copy stream during compute of chunk k",
+               "overlap": "H2D of chunk k+1 on a copy stream during compute of chunk k; D2H of a step's "
+                          "results on a third stream during the next step's H2D",
                "d2h": "loss, d/drotation, d/dvolume, inserted volume and weights"}
 
     torch_gpu = None

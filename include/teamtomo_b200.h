@@ -196,15 +196,16 @@ int tt_central_slice_mse(const void *volume_rfft, const void *rotation_matrices,
  * fixed memory budget that must not grow): it takes no workspace and calls no
  * allocator; the rotation-gradient partial sums go to a 4 MiB array built
  * into the library instead.
- *  - Limit: when grad_rotation is requested, n * ceil((img_w/2+1) / 8) *
- *    ceil(img_h / 32) * 24 bytes (the per-tile partial sums) must not exceed
- *    TT_NOALLOC_SCRATCH_BYTES (at a 256^3 box that is 1285 slices per call);
+ *  - Limit: when grad_rotation is requested, n * ceil(img_h / 32) * 24 bytes
+ *    (the partial sums of each row of 8 x 32 pixel tiles) must not exceed
+ *    TT_NOALLOC_SCRATCH_BYTES (at a 256^3 box that is 21845 slices per call);
  *    larger calls fail with TT_ERR_INVALID and a message.
  *  - The first call on each device looks up the array's device address
  *    (cudaGetSymbolAddress) with that device current; make it before any
  *    stream capture.
  *  - All calls share the array: calls that overlap on the GPU race and must be
- *    serialised by the caller.  Nothing needs clearing between calls.
+ *    serialised by the caller.  Each call writes every slot it reads, so
+ *    nothing needs clearing between calls.
  *  - The deterministic (fixed-point) volume gradient needs a workspace: a
  *    call with p->deterministic and a grad_volume fails with TT_ERR_INVALID.
  * This entry point has no counterpart in the reference. */

@@ -1,12 +1,14 @@
-"""Tile-shape autotuner for the batched slice kernels.
+"""Tile-shape and volume-layout autotuner for the batched slice kernels.
 
 The batched kernels are compiled for three tile shapes (8x32, 16x16 and 32x8
-pixels per 256-thread block).  Which one is fastest depends on the box size
-(how a warp's pixels spread over the volume's cache lines).  ``tune`` times
-each shape on synthetic data of a given box size with CUDA events and records
-the winner in a JSON cache keyed by (GPU name, kind, box); the batched API
-looks the cache up (``cached_tile_shape``) and falls back to 8x32 (shape 0)
-for box sizes never tuned.
+pixels per 256-thread block), and the batched extraction gathers either from
+the volumes themselves or from their 2 x 2 x 2 bricked copies.  Which
+combination is fastest depends on the box size (how a warp's pixels spread
+over the volume's cache lines).  ``tune`` times every combination on
+synthetic data of a given box size with CUDA events and records the winner in
+a JSON cache keyed by (GPU name, kind, box); the batched API looks the cache
+up (``cached_tile_shape``, ``cached_layout``) and falls back to 8x32 (shape 0)
+and the pixels-per-voxel layout policy for box sizes never tuned.
 
 Cache file: ``$TT_AUTOTUNE_CACHE`` or ``~/.cache/teamtomo_b200/autotune.json``.
 """
@@ -62,39 +64,55 @@ def cached_tile_shape(kind: str, box: int, device) -> int:
         return _load().get(_key(kind, box, device), DEFAULT_TILE_SHAPE)
 
 
+def cached_layout(kind: str, box: int, device) -> int | None:
+    """Tuned volume layout (0 plain, 2 bricked) of the batched extraction at
+    this box size, or None when never tuned."""
+    with _lock:
+        return _load().get(_key(kind, box, device) + ":layout")
+
+
 def tune(kind: str, box: int, n_slices: int = 512, device=None, repeats: int = 5) -> dict[int, float]:
     """Time every tile shape for `kind` ('extract' or 'insert') at box size
     `box`, store the fastest in the cache and return {shape: ms}."""
     from . import batched
 
     dev = torch.device(device or "cuda")
+    if kind == "extract":
+        # the bricked layout packs each volume once per call: time it where the
+        # pack is amortised as in use (four slice pixels per voxel or more)
+        n_slices = max(n_slices, 4 * box)
     g = torch.Generator(device=dev).manual_seed(box)
     shape3 = (box, box, box // 2 + 1)
     R = torch.linalg.qr(torch.randn((n_slices, 3, 3), device=dev, generator=g))[0].contiguous()
     ctf = batched.ctf_params(1.5, n=n_slices, device=dev)
+    layouts = (None,)
     if kind == "extract":
         vol = torch.randn(shape3, dtype=torch.complex64, device=dev, generator=g)
-        run = lambda ts: batched.extract_central_slices_rfft_3d_batched(  # noqa: E731
-            [vol], [R], ctf=[ctf], tile_shape=ts)
+        layouts = ("plain", "bricks")
+        run = lambda ts, lay: batched.extract_central_slices_rfft_3d_batched(  # noqa: E731
+            [vol], [R], ctf=[ctf], tile_shape=ts, volume_layout=lay)
     elif kind == "insert":
         img = torch.randn((n_slices, box, box // 2 + 1), dtype=torch.complex64, device=dev, generator=g)
-        run = lambda ts: batched.insert_central_slices_rfft_3d_batched(  # noqa: E731
+        run = lambda ts, lay: batched.insert_central_slices_rfft_3d_batched(  # noqa: E731
             [img], [R], ctf=[ctf], tile_shape=ts)
     else:
         raise ValueError("kind must be 'extract' or 'insert'")
     times = {}
-    for ts in TILE_SHAPES:
-        run(ts)
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize(dev)
-        start.record()
-        for _ in range(repeats):
-            run(ts)
-        end.record()
-        torch.cuda.synchronize(dev)
-        times[ts] = start.elapsed_time(end) / repeats
-    best = min(times, key=times.get)
+    for lay in layouts:
+        for ts in TILE_SHAPES:
+            run(ts, lay)
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize(dev)
+            start.record()
+            for _ in range(repeats):
+                run(ts, lay)
+            end.record()
+            torch.cuda.synchronize(dev)
+            times[(ts, lay)] = start.elapsed_time(end) / repeats
+    best_ts, best_lay = min(times, key=times.get)
     with _lock:
-        _load()[_key(kind, box, dev)] = best
+        _load()[_key(kind, box, dev)] = best_ts
+        if best_lay is not None:
+            _load()[_key(kind, box, dev) + ":layout"] = 2 if best_lay == "bricks" else 0
         _save()
     return times

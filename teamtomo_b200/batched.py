@@ -63,6 +63,25 @@ def _tile_shape(kind: str, boxes: Sequence[int], device, tile_shape):
     return autotune.cached_tile_shape(kind, max(boxes), device)
 
 
+def _layout(boxes: Sequence[int], n_pixels: int, n_voxels: int, device, volume_layout):
+    """Volume layout the batched extraction gathers from: ``volume_layout``
+    ('plain' or 'bricks') when given, else the autotuner's choice for the
+    largest box when it has one, else the single-volume policy (the bricked
+    copies from half a slice pixel per voxel)."""
+    from .torch_fourier_slice import _layout as lay
+
+    if volume_layout is not None:
+        if volume_layout not in ("plain", "bricks"):
+            raise ValueError(f"volume_layout must be 'plain' or 'bricks', got {volume_layout!r}")
+        return lay.BRICKS if volume_layout == "bricks" else lay.PLAIN
+    from . import autotune
+
+    tuned = autotune.cached_layout("extract", max(boxes), device)
+    if tuned is not None:
+        return tuned
+    return lay.BRICKS if n_pixels >= lay.MIN_PIXELS_PER_VOXEL * n_voxels else lay.PLAIN
+
+
 def _check_ctf(ctf, n, device):
     if ctf is None:
         return None
@@ -95,25 +114,36 @@ def extract_central_slices_rfft_3d_batched(
     x_tolerance: float = 1e-8,
     rot_tolerance: float | None = 1e-8,
     tile_shape: int | None = None,
+    volume_layout: str | None = None,
 ) -> list[torch.Tensor]:
     """Extract slices from every volume in one launch.
 
     ``volumes[i]`` is an fftshifted rfft volume (d, d, d//2+1) complex64,
     ``rotation_matrices[i]`` (n_i, 3, 3), ``image_shapes[i]`` defaults to
     (d, d, d), ``ctf[i]`` is None or (n_i, 8) CTF rows (see ``ctf_params``).
+    ``volume_layout`` ('plain' or 'bricks', default: autotuned or by the
+    pixels-per-voxel policy) selects whether the gathers read the volumes or
+    their bricked copies (packed here; the results are the same bit for bit).
     Returns the list of (n_i, h_i, w_i//2+1) complex64 slice stacks."""
+    from .torch_fourier_slice import _layout as lay
+
     if not volumes:
         return []
     dev = _lib.require_cuda(*volumes)
     ctf = list(ctf) if ctf is not None else [None] * len(volumes)
     shapes = list(image_shapes) if image_shapes is not None else [
         (v.shape[0], v.shape[0], v.shape[0]) for v in volumes]
+    Rs = [rotation_arg(R, dev)[0] for R in rotation_matrices]
+    n_pixels = sum(R.shape[0] * int(sh[-2]) * (int(sh[-1]) // 2 + 1) for R, sh in zip(Rs, shapes))
+    layout = _layout([v.shape[0] for v in volumes], n_pixels, sum(v.numel() for v in volumes), dev,
+                     volume_layout)
+    if layout == lay.BRICKS and not all(lay.bricks_fit(v) for v in volumes):
+        layout = lay.PLAIN
     outs, entries, keep = [], [], []
-    for vol, R, shape, c in zip(volumes, rotation_matrices, shapes, ctf):
+    for vol, Rm, shape, c in zip(volumes, Rs, shapes, ctf):
         if vol.ndim != 3 or vol.dtype != torch.complex64:
             raise ValueError("batched extraction takes complex64 (d, h, w//2+1) volumes")
         vol = _lib.dense(vol)
-        Rm, _ = rotation_arg(R, dev)
         n = Rm.shape[0]
         h, w = int(shape[-2]), int(shape[-1])
         out = torch.empty((n, h, w // 2 + 1), dtype=torch.complex64, device=dev)
@@ -121,9 +151,13 @@ def extract_central_slices_rfft_3d_batched(
         p = slice_params(n=n, image_shape=shape, volume=vol, rotation=Rm, fftfreq_max=fftfreq_max,
                          zyx_matrices=zyx_matrices, x_tolerance=x_tolerance,
                          rot_tolerance=rot_tolerance)
-        entries.append(_lib.BatchVolume(p, vol.data_ptr(), out.data_ptr(), None, Rm.data_ptr(),
+        src = vol
+        if layout == lay.BRICKS and n > 0:
+            src = lay.pack(vol, p, lay.BRICKS)
+            p = lay.with_layout(p, lay.BRICKS)
+        entries.append(_lib.BatchVolume(p, src.data_ptr(), out.data_ptr(), None, Rm.data_ptr(),
                                         cc.data_ptr() if cc is not None else None))
-        keep += [vol, Rm, cc]
+        keep += [vol, src, Rm, cc]
         outs.append(out)
     ts = _tile_shape("extract", [v.shape[0] for v in volumes], dev, tile_shape)
     for chunk in _batches(entries):

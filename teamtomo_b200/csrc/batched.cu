@@ -2,12 +2,16 @@
 // box sizes, each with its own set of rotations and an optional per-image
 // CTF, in ONE persistent launch.
 //
-// Work queue: the slices of all volumes form one global list; each block
-// takes the next slice from an atomic counter, finds its volume by binary
-// search over the per-volume slice offsets, loads the rotation (and computes
-// the slice's CTF constants) once, and walks the slice's pixel tiles.  Every
-// slice of a volume is equal work, so the queue balances uneven box sizes
-// and slice counts without any host-side scheduling.
+// Work queue over (volume, slice, row of tiles) items: the items of all
+// volumes form one global list; each block takes the next item from an atomic
+// counter, finds its volume by binary search over the per-volume item
+// offsets, loads the slice's rotation (and computes its CTF constants), and
+// walks the row of pixel tiles.  The items of a volume are equal work and
+// small (one row of tiles), so the queue balances uneven box sizes and slice
+// counts without any host-side scheduling and without a long tail.  The
+// extraction gathers from each volume's plain rfft or, when every volume of
+// the call is given as its bricked copy (volume_layout 2,
+// tt_pack_volume_bricks), from the bricked copies.
 //
 // The per-volume descriptors travel as a __grid_constant__ kernel parameter
 // (no host-to-device copy, so the launch captures into a CUDA graph as-is);
@@ -40,22 +44,9 @@ struct BatchVolumeDev {
 
 struct BatchParams {
     int nvol;
-    int64_t slice_offset[kMaxBatch + 1];
+    int64_t item_offset[kMaxBatch + 1];  // work items (slice, row of tiles) before each volume
     BatchVolumeDev v[kMaxBatch];
 };
-
-// Pixel of this thread in tile `tile` for TX-wide tiles of 256 pixels
-// (each warp covers TX x 32/TX pixels).
-template <int TX>
-__device__ __forceinline__ bool tile_pixel_t(const SliceGeom& g, int tile, int& iy, int& ix) {
-    constexpr int TY = 256 / TX, RPW = 32 / TX;
-    const int txt = (g.wr + TX - 1) / TX;
-    const int ty = tile / txt, tx = tile - ty * txt;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    ix = tx * TX + (lane % TX);
-    iy = ty * TY + warp * RPW + lane / TX;
-    return ix < g.wr && iy < g.img_h;
-}
 
 template <int TX>
 __host__ inline int tiles_t(int img_h, int wr) {
@@ -63,67 +54,87 @@ __host__ inline int tiles_t(int img_h, int wr) {
     return ((wr + TX - 1) / TX) * ((img_h + TY - 1) / TY);
 }
 
-template <int TX, bool INSERT>
+template <int TX, bool INSERT, typename VT>
 __global__ void __launch_bounds__(256)
 batched_slices_kernel(const __grid_constant__ BatchParams bp, unsigned long long* __restrict__ queue,
                       int64_t total, int phase, int nphase) {
+    constexpr int TY = 256 / TX, RPW = 32 / TX;
     __shared__ float m[9];
     __shared__ CtfConst cc;
     __shared__ int64_t cur;
     __shared__ int vsel;
-    for (;;) {
-        __syncthreads();  // m / cc / cur of the previous slice are no longer read
-        if (threadIdx.x == 0) {
-            const int64_t gs = (int64_t)atomicAdd(queue, 1ULL);
-            int lo = 0, hi = bp.nvol;  // slice_offset[lo] <= gs < slice_offset[lo + 1]
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (bp.slice_offset[mid] <= gs) lo = mid;
-                else hi = mid;
-            }
-            cur = gs;
-            vsel = lo;
+    const int lane = threadIdx.x & 31;
+    // volume of item gi: item_offset[lo] <= gi < item_offset[lo + 1]
+    auto volume_of = [&](int64_t gi) {
+        int lo = 0, hi = bp.nvol;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (bp.item_offset[mid] <= gi) lo = mid;
+            else hi = mid;
         }
-        __syncthreads();
-        const int64_t gs = cur;
-        if (gs >= total) return;
+        return lo;
+    };
+    if (threadIdx.x == 0) {
+        cur = (int64_t)atomicAdd(queue, 1ULL);
+        vsel = volume_of(cur);
+    }
+    for (;;) {
+        __syncthreads();  // this item's cur / vsel are visible; m / cc of the previous one are no longer read
+        const int64_t gi = cur;
+        if (gi >= total) return;
         const BatchVolumeDev& bv = bp.v[vsel];
-        const int64_t s = gs - bp.slice_offset[vsel];
+        const int txt = (bv.g.wr + TX - 1) / TX, tyt = (bv.g.img_h + TY - 1) / TY;
+        const int64_t local = gi - bp.item_offset[vsel];
+        const int64_t s = local / tyt;  // item = (slice, row of tiles)
+        const int ty = (int)(local - s * tyt);
         if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(bv.rot, bv.g.rot_f64, s, threadIdx.x, bv.g, !INSERT);
         if (threadIdx.x == 0 && bv.ctf) cc = make_ctf_const(bv.ctf[s]);
-        __syncthreads();
+        // the next item is taken now and published after this one's pixels, so
+        // the queue's round trip overlaps the work
+        unsigned long long next = 0;
+        if (threadIdx.x == 0) next = atomicAdd(queue, 1ULL);
+        __syncthreads();  // every thread has read cur / vsel and sees m / cc
         const CtfConst* ccp = bv.ctf ? &cc : nullptr;
-        for (int tile = 0; tile < bv.tiles; tile++) {
-            int iy, ix;
-            const bool has_pixel = tile_pixel_t<TX>(bv.g, tile, iy, ix);
-            if (INSERT) {
-                // z-phased filling of large accumulators (the same answer in every thread)
-                if (nphase > 1) {
-                    constexpr int TY = 256 / TX;
-                    const int txt = (bv.g.wr + TX - 1) / TX;
-                    const int ty = tile / txt, tx = tile - ty * txt;
-                    if (insert_tile_phase(bv.g, m, min(ty * TY + TY / 2, bv.g.img_h - 1),
-                                          min(tx * TX + TX / 2, bv.g.wr - 1), nphase) != phase)
-                        continue;
+        const int iy = ty * TY + (threadIdx.x >> 5) * RPW + lane / TX;
+        if constexpr (!INSERT) {
+            // extraction: the row part of the geometry formed once for the row of tiles
+            if (iy < bv.g.img_h) {
+                const SliceRow row = slice_row_geom(bv.g, m, iy);
+                float2* orow = bv.slices + (s * bv.g.img_h + slice_row(bv.g, iy)) * (int64_t)bv.g.wr;
+                const VT* vol = reinterpret_cast<const VT*>(bv.vol);
+                for (int tx = 0; tx < txt; tx++) {
+                    const int ix = tx * TX + (lane % TX);
+                    if (ix >= bv.g.wr) continue;
+                    float qx, c[3];
+                    bool cj = false;
+                    float2 r = make_float2(0.0f, 0.0f);
+                    if (extract_geometry_row(bv.g, m, row, ix, qx, cj, c)) {
+                        r = sample_trilinear(vol, bv.g, make_corners(bv.g, c));
+                        if (cj) r.y = -r.y;
+                        if (ccp) {
+                            const float cv = ctf_value(*ccp, row.qy, qx);
+                            r.x *= cv;
+                            r.y *= cv;
+                        }
+                    }
+                    __stcs(orow + ix, r);
                 }
+            }
+        } else {
+            for (int tx = 0; tx < txt; tx++) {
+                // z-phased filling of large accumulators (the same answer in every thread)
+                if (nphase > 1 && insert_tile_phase(bv.g, m, min(ty * TY + TY / 2, bv.g.img_h - 1),
+                                                    min(tx * TX + TX / 2, bv.g.wr - 1), nphase) != phase)
+                    continue;
+                const int ix = tx * TX + (lane % TX);
+                const bool has_pixel = ix < bv.g.wr && iy < bv.g.img_h;
                 // every lane takes part: lane pairs share a pixel's x-corners
                 insert_point_paired(bv.slices, m, bv.acc, bv.g, s, has_pixel, iy, ix, ccp);
-            } else {
-                if (!has_pixel) continue;
-                float qy, qx, c[3];
-                bool cj = false;
-                float2 r = make_float2(0.0f, 0.0f);
-                if (extract_geometry(bv.g, m, iy, ix, qy, qx, cj, c)) {
-                    r = sample_trilinear(bv.vol, bv.g, make_corners(bv.g, c));
-                    if (cj) r.y = -r.y;
-                    if (ccp) {
-                        const float cv = ctf_value(*ccp, qy, qx);
-                        r.x *= cv;
-                        r.y *= cv;
-                    }
-                }
-                __stcs(bv.slices + (s * bv.g.img_h + slice_row(bv.g, iy)) * (int64_t)bv.g.wr + ix, r);
             }
+        }
+        if (threadIdx.x == 0) {
+            cur = (int64_t)next;
+            vsel = volume_of((int64_t)next);
         }
     }
 }
@@ -135,12 +146,20 @@ static int tiles_for_shape(const SliceGeom& g) {
 
 int insert_phases(size_t acc_bytes);  // insert.cu
 
-template <int TX, bool INSERT>
-static int launch_batched(BatchParams& bp, unsigned long long* queue, int64_t total, cudaStream_t st) {
-    for (int v = 0; v < bp.nvol; v++) bp.v[v].tiles = tiles_for_shape<TX>(bp.v[v].g);
+template <int TX, bool INSERT, typename VT>
+static int launch_batched(BatchParams& bp, unsigned long long* queue, cudaStream_t st) {
+    constexpr int TY = 256 / TX;
+    bp.item_offset[0] = 0;
+    for (int v = 0; v < bp.nvol; v++) {
+        bp.v[v].tiles = tiles_for_shape<TX>(bp.v[v].g);
+        const int64_t rows = (bp.v[v].g.img_h + TY - 1) / TY;
+        bp.item_offset[v + 1] = bp.item_offset[v] + (int64_t)bp.v[v].g.n * rows;
+    }
+    const int64_t total = bp.item_offset[bp.nvol];
+    if (total == 0) return TT_OK;
     int dev = 0, sms = 148, occ = 1;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batched_slices_kernel<TX, INSERT>, 256, 0) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batched_slices_kernel<TX, INSERT, VT>, 256, 0) !=
             cudaSuccess ||
         occ < 1)
         occ = 1;
@@ -158,7 +177,7 @@ static int launch_batched(BatchParams& bp, unsigned long long* queue, int64_t to
             cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
             if (e != cudaSuccess) return fail(TT_ERR_CUDA, "batched: memset: %s", cudaGetErrorString(e));
         }
-        batched_slices_kernel<TX, INSERT><<<(unsigned)blocks, 256, 0, st>>>(bp, queue, total, ph, nphase);
+        batched_slices_kernel<TX, INSERT, VT><<<(unsigned)blocks, 256, 0, st>>>(bp, queue, total, ph, nphase);
         if (int e = check_launch("batched_slices_kernel")) return e;
     }
     return TT_OK;
@@ -177,10 +196,20 @@ static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
     bp.nvol = n_volumes;
-    bp.slice_offset[0] = 0;
+    int layout = -1;  // every volume of an extraction batch gathers from the same layout
+    int64_t slices = 0;
     for (int v = 0; v < n_volumes; v++) {
         const tt_batch_volume& x = volumes[v];
-        if (int e = validate_params(&x.params)) return e;
+        if (int e = validate_params(&x.params, !insert)) return e;
+        if (!insert && x.params.volume_layout == TT_VOLUME_XPAIRS)
+            return fail(TT_ERR_INVALID, "%s: volume %d: the batched extraction takes plain or bricked volumes", what,
+                        v);
+        if (!insert && x.params.n > 0) {
+            if (layout >= 0 && x.params.volume_layout != layout)
+                return fail(TT_ERR_INVALID, "%s: volume %d: all volumes of one call share one volume_layout", what,
+                            v);
+            layout = x.params.volume_layout;
+        }
         if (x.params.deterministic)
             return fail(TT_ERR_INVALID, "%s: volume %d: the batched launch has no deterministic mode", what, v);
         if (x.params.n > 0) {
@@ -201,22 +230,26 @@ static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_
         d.acc = (float4*)x.accumulator;
         d.rot = x.rotation_matrices;
         d.ctf = x.ctf;
-        bp.slice_offset[v + 1] = bp.slice_offset[v] + x.params.n;
+        slices += x.params.n;
     }
-    const int64_t total = bp.slice_offset[n_volumes];
-    if (total == 0) return TT_OK;
+    if (slices == 0) return TT_OK;
     cudaStream_t st = as_stream(stream);
     unsigned long long* queue = (unsigned long long*)workspace;
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail(TT_ERR_CUDA, "%s: memset: %s", what, cudaGetErrorString(e));
     if (insert) {
-        if (tile_shape == 0) return launch_batched<8, true>(bp, queue, total, st);
-        if (tile_shape == 1) return launch_batched<16, true>(bp, queue, total, st);
-        return launch_batched<32, true>(bp, queue, total, st);
+        if (tile_shape == 0) return launch_batched<8, true, float2>(bp, queue, st);
+        if (tile_shape == 1) return launch_batched<16, true, float2>(bp, queue, st);
+        return launch_batched<32, true, float2>(bp, queue, st);
     }
-    if (tile_shape == 0) return launch_batched<8, false>(bp, queue, total, st);
-    if (tile_shape == 1) return launch_batched<16, false>(bp, queue, total, st);
-    return launch_batched<32, false>(bp, queue, total, st);
+    if (layout == TT_VOLUME_BRICKS) {
+        if (tile_shape == 0) return launch_batched<8, false, VoxBrick2>(bp, queue, st);
+        if (tile_shape == 1) return launch_batched<16, false, VoxBrick2>(bp, queue, st);
+        return launch_batched<32, false, VoxBrick2>(bp, queue, st);
+    }
+    if (tile_shape == 0) return launch_batched<8, false, float2>(bp, queue, st);
+    if (tile_shape == 1) return launch_batched<16, false, float2>(bp, queue, st);
+    return launch_batched<32, false, float2>(bp, queue, st);
 }
 
 }  // namespace tt

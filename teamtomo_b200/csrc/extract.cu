@@ -179,8 +179,7 @@ __device__ __forceinline__ void mse_point(const VT* __restrict__ vol, const floa
 // rotation-gradient partials reduced once per row.  WANT_DR: the row's sums of
 // the 6 non-zero entries of d/dR_zyx (per thread over its pixels, warp totals
 // in float, then the eight warps in double, in a fixed order) go to
-// part[(s * tiles + tile) * 6 + k] of the row's first tile, zeros to the
-// row's other tiles.  FIXED:
+// part[(s * rows + row) * 6 + k], one slot per row of tiles.  FIXED:
 // the volume gradient goes to the
 // fixed-point words `fixed` at the scale set by *absmax and n.  Resident
 // blocks: 6 for the rotation gradient alone (39 registers), 5 with the volume
@@ -218,18 +217,15 @@ extract_bwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
             double v = 0.0;
 #pragma unroll
             for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][threadIdx.x];
-            // the row's total in the slot of its first tile, zero in the others
-            const int64_t b0 = (int64_t)s * tiles + (int64_t)ty * tx_tiles;
-            part[b0 * 6 + threadIdx.x] = (float)v;
-            for (int tx = 1; tx < tx_tiles; tx++) part[(b0 + tx) * 6 + threadIdx.x] = 0.0f;
+            part[((int64_t)s * rows + ty) * 6 + threadIdx.x] = (float)v;
         }
     }
 }
 
 // Fused extraction + mean squared error + backward: one block per (slice, row
 // of tiles).  The row's partials of the loss (double) go to
-// loss_part[s * tiles + tile] and, with WANT_DR, those of d/dR_zyx to
-// part[(s * tiles + tile) * 6 + k], for the row's first tile (zeros for the others).
+// loss_part[s * rows + row] and, with WANT_DR, those of d/dR_zyx to
+// part[(s * rows + row) * 6 + k]: one slot per row of tiles.
 template <bool WANT_DV, bool WANT_DR, typename VT>
 __global__ void __launch_bounds__(kExtractThreads, 5)
 slice_mse_kernel(const VT* __restrict__ vol, const void* __restrict__ rot, const float2* __restrict__ target,
@@ -263,15 +259,11 @@ slice_mse_kernel(const VT* __restrict__ vol, const void* __restrict__ rot, const
         double v = 0.0;
 #pragma unroll
         for (int w = 0; w < kExtractThreads / 32; w++) v += red[w][threadIdx.x];
-        // the row's totals in the slots of its first tile, zero in the others
-        const int64_t b0 = (int64_t)s * tiles + (int64_t)ty * tx_tiles;
-        if (threadIdx.x == 6) {
+        const int64_t b0 = (int64_t)s * rows + ty;
+        if (threadIdx.x == 6)
             loss_part[b0] = v;
-            for (int tx = 1; tx < tx_tiles; tx++) loss_part[b0 + tx] = 0.0;
-        } else if (WANT_DR) {
+        else if (WANT_DR)
             part[b0 * 6 + threadIdx.x] = (float)v;
-            for (int tx = 1; tx < tx_tiles; tx++) part[(b0 + tx) * 6 + threadIdx.x] = 0.0f;
-        }
     }
 }
 
@@ -295,7 +287,7 @@ __global__ void __launch_bounds__(1024) mse_loss_finish_kernel(const double* __r
 // caller-layout gradient: undo the xyz->zyx flip, zero the tolerance-zeroed
 // elements, cast to the rotation dtype.  One thread per (slice, element).
 __global__ void drot_finish_kernel(const float* __restrict__ part, const void* __restrict__ rot,
-                                   void* __restrict__ drot, SliceGeom g, int tiles) {
+                                   void* __restrict__ drot, SliceGeom g, int parts) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)g.n * 9) return;
     const int64_t s = idx / 9;
@@ -304,8 +296,8 @@ __global__ void drot_finish_kernel(const float* __restrict__ part, const void* _
     const int i = g.zyx ? a : 2 - a, j = g.zyx ? b : 2 - b;
     double v = 0.0;
     if (j != 0) {
-        const float* ps = part + (int64_t)s * tiles * 6 + i * 2 + (j - 1);
-        for (int k = 0; k < tiles; k++) v += (double)ps[(int64_t)k * 6];
+        const float* ps = part + (int64_t)s * parts * 6 + i * 2 + (j - 1);
+        for (int k = 0; k < parts; k++) v += (double)ps[(int64_t)k * 6];
     }
     float r = g.rot_f64 ? __double2float_rn(((const double*)rot)[idx]) : ((const float*)rot)[idx];
     if (g.has_rot_tol && fabsf(r) < g.rot_tol) v = 0.0;
@@ -368,12 +360,18 @@ __global__ void dv_fixed_add_kernel(const long long* __restrict__ fixed, float2*
     dvol[i] = o;
 }
 
-static size_t partial_bytes(int64_t n, int tiles) { return (size_t)(n * tiles * 6) * sizeof(float); }
+// Rotation-gradient partials: `parts` slots of 6 floats per slice (one per
+// row of tiles for the single-channel kernels, one per tile for the
+// multichannel ones).
+static size_t partial_bytes(int64_t n, int parts) { return (size_t)(n * parts * 6) * sizeof(float); }
 
-int launch_drot_finish(const float* part, const void* rot, void* drot, const SliceGeom& g, int tiles,
+// Rows of tiles per slice: the single-channel kernels' blocks and partial slots.
+static int tile_rows(int img_h) { return (img_h + kTileY - 1) / kTileY; }
+
+int launch_drot_finish(const float* part, const void* rot, void* drot, const SliceGeom& g, int parts,
                        cudaStream_t st) {
     const int64_t total = (int64_t)g.n * 9;
-    drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rot, drot, g, tiles);
+    drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rot, drot, g, parts);
     return check_launch("drot_finish_kernel");
 }
 
@@ -384,7 +382,7 @@ static size_t fixed_dv_bytes(const tt_slice_params* p) {
 }
 
 // Launches the backward and the rotation-gradient reduction; `part` holds
-// n * tiles * 6 floats when grad_rotation is set; `fixed` (deterministic
+// 6 floats per row of tiles when grad_rotation is set; `fixed` (deterministic
 // volume gradient) is the zeroed header + accumulator of fixed_dv_bytes.
 template <typename VT>
 static int launch_backward_t(const VT* v, const void* rot, const float2* gr, float2* dv, void* grad_rotation,
@@ -416,11 +414,8 @@ static int launch_backward_t(const VT* v, const void* rot, const float2* gr, flo
                                                                                   part, g, tiles);
     }
     if (int e = check_launch("extract_bwd_kernel")) return e;
-    if (grad_rotation) {
-        const int64_t total = (int64_t)g.n * 9;
-        drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rot, grad_rotation, g, tiles);
-        if (int e = check_launch("drot_finish_kernel")) return e;
-    }
+    if (grad_rotation)
+        if (int e = launch_drot_finish(part, rot, grad_rotation, g, tile_rows(g.img_h), st)) return e;
     return TT_OK;
 }
 
@@ -494,13 +489,14 @@ static int launch_mse(const VT* v, const void* rot, const float2* t, float2* dv,
 
 using namespace tt;
 
-static size_t mse_workspace_bytes(int64_t n, int tiles) {
-    return (size_t)(n * tiles) * sizeof(double) + partial_bytes(n, tiles);
+// Loss partials (double) and rotation-gradient partials, one slot per row of tiles.
+static size_t mse_workspace_bytes(int64_t n, int rows) {
+    return (size_t)(n * rows) * sizeof(double) + partial_bytes(n, rows);
 }
 
 extern "C" size_t tt_central_slice_mse_workspace_bytes(const tt_slice_params* p) {
     if (!p || p->n <= 0 || p->img_h < 1 || p->img_w < 1) return 0;
-    return mse_workspace_bytes(p->n, tiles_per_slice((int)p->img_h, (int)(p->img_w / 2 + 1)));
+    return mse_workspace_bytes(p->n, tile_rows((int)p->img_h));
 }
 
 extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotation_matrices, const void* targets,
@@ -515,9 +511,10 @@ extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotatio
         return fail(TT_ERR_INVALID, "central_slice_mse: NULL pointer argument");
     SliceGeom g = make_geom(*p);
     const int tiles = extract_tiles(g);
-    const int64_t blocks = (int64_t)g.n * tiles;
-    if (blocks > 0x7fffffffLL) return fail(TT_ERR_INVALID, "central_slice_mse: too many blocks");
-    const size_t need = mse_workspace_bytes(g.n, tiles);
+    const int rows = tile_rows(g.img_h);
+    const int64_t blocks = (int64_t)g.n * rows;  // one block (and one partial slot) per row of tiles
+    if ((int64_t)g.n * tiles > 0x7fffffffLL) return fail(TT_ERR_INVALID, "central_slice_mse: too many blocks");
+    const size_t need = mse_workspace_bytes(g.n, rows);
     if (!workspace || workspace_bytes < need)
         return fail(TT_ERR_WORKSPACE, "central_slice_mse: workspace of %zu bytes needed, got %zu", need,
                     workspace_bytes);
@@ -546,12 +543,7 @@ extern "C" int tt_central_slice_mse(const void* volume_rfft, const void* rotatio
     if (e) return e;
     mse_loss_finish_kernel<<<1, 1024, 0, st>>>(loss_part, blocks, 1.0 / m, loss);
     if (int e = check_launch("mse_loss_finish_kernel")) return e;
-    if (grad_rotation) {
-        const int64_t total = (int64_t)g.n * 9;
-        drot_finish_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(part, rotation_matrices, grad_rotation,
-                                                                            g, tiles);
-        if (int e = check_launch("drot_finish_kernel")) return e;
-    }
+    if (grad_rotation) return launch_drot_finish(part, rotation_matrices, grad_rotation, g, rows, st);
     return TT_OK;
 }
 
@@ -644,6 +636,9 @@ extern "C" int tt_slice_geometry(const void* rotation_matrices, int32_t mode, ui
 
 extern "C" size_t tt_extract_backward_workspace_bytes(const tt_slice_params* p) {
     if (!p || p->n <= 0 || p->img_h < 1 || p->img_w < 1) return 0;
+    // one slot of partials per tile: the multichannel backward (one block per
+    // tile) takes this workspace too; the single-channel kernels use one slot
+    // per row of tiles of it
     return fixed_dv_bytes(p) + partial_bytes(p->n, tiles_per_slice((int)p->img_h, (int)(p->img_w / 2 + 1)));
 }
 
@@ -660,7 +655,7 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward(
     if ((int64_t)g.n * tiles > 0x7fffffffLL) return fail(TT_ERR_INVALID, "extract backward: too many blocks");
     const size_t fixed = grad_volume ? fixed_dv_bytes(p) : 0;
     if (grad_rotation || fixed) {
-        const size_t need = fixed + (grad_rotation ? partial_bytes(g.n, tiles) : 0);
+        const size_t need = fixed + (grad_rotation ? partial_bytes(g.n, tile_rows(g.img_h)) : 0);
         if (!workspace || workspace_bytes < need)
             return fail(TT_ERR_WORKSPACE, "extract backward: workspace of %zu bytes needed, got %zu", need,
                         workspace_bytes);
@@ -743,10 +738,10 @@ extern "C" int tt_extract_central_slices_rfft_3d_backward_noalloc(const void* vo
     const void* v = volume_rfft;
     const float2* gr = (const float2*)grad_slices;
     float2* dv = (float2*)grad_volume;
-    // the scratch holds n * tiles * 6 partial sums of the rotation gradient
+    // the scratch holds 6 partial sums of the rotation gradient per row of tiles
     if (!grad_rotation)  // the volume gradient alone needs no scratch
         return launch_backward(v, rotation_matrices, gr, dv, nullptr, nullptr, g, st);
-    const size_t need = partial_bytes(g.n, tiles);
+    const size_t need = partial_bytes(g.n, tile_rows(g.img_h));
     if (need > (size_t)TT_NOALLOC_SCRATCH_BYTES)
         return fail(TT_ERR_INVALID,
                     "noalloc backward: %lld slices of %lld x %lld need %zu bytes of scratch, more than the "

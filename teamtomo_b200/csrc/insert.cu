@@ -16,6 +16,12 @@
 // same instruction (insert_point_paired): the two voxels usually share an L2
 // sector, so a warp's reductions touch fewer sectors (-15 % time at 256^3).
 //
+// The one-shot entry point (tt_insert_central_slices_rfft_3d) accumulates
+// large float volumes into a 2 x 2 x 2-bricked accumulator instead
+// (accumulator_slot: the eight corners of an even-aligned cell share one
+// 128-byte line; a cell touches 3.4 lines on average instead of 4.5), split
+// by insert_finalize_bricked_kernel.
+//
 // Finalize stage: the reference also inserts conj(data)*w at ((d-z)%d, (h-y)%h, 0)
 // for every corner that lands on the x=0 plane except the DC voxel.  Summed
 // over all points that equals, per plane voxel v with partner m(v),
@@ -35,7 +41,7 @@ namespace tt {
 // One block per (slice, row of tiles): the block loads the rotation once and
 // walks the row, skipping the tiles of other z-phases (a few instructions
 // each, so extra phases cost almost nothing).
-template <typename R>
+template <typename R, bool BRICKED = false>
 __global__ void __launch_bounds__(kTileThreads)
 insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void* __restrict__ rot,
                          typename Acc<R>::T* __restrict__ acc, SliceGeom g, int phase, int nphase) {
@@ -54,7 +60,7 @@ insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void*
         int iy, ix;
         const bool has_pixel = tile_pixel(g, ty * tx_tiles + tx, iy, ix);
         if constexpr (std::is_same<R, float>::value)
-            insert_point_paired(img, m, acc, g, s, has_pixel, iy, ix);  // every lane takes part
+            insert_point_paired<BRICKED>(img, m, acc, g, s, has_pixel, iy, ix);  // every lane takes part
         else if (has_pixel)
             insert_point<R>(img, m, acc, g, s, iy, ix);
     }
@@ -90,6 +96,35 @@ __global__ void insert_finalize_kernel(const typename Acc<R>::T* __restrict__ ac
     o.y = im;
     vol[idx] = o;
     if (ch == 0 && wts) wts[r] = wt;
+}
+
+// Bricked float accumulator (accumulator_slot) -> (volume, weights) with the
+// Friedel completion of the x=0 plane.  One block per (z, y) pair of brick
+// rows: it reads that brick row's contiguous slots (coalesced float4 loads)
+// and writes the four voxel rows it covers (runs of two x per brick).
+__global__ void insert_finalize_bricked_kernel(const float4* __restrict__ acc, float2* __restrict__ vol,
+                                               float* __restrict__ wts, SliceGeom g) {
+    const int bh = (g.H + 1) >> 1, bw = (g.W + 1) >> 1;
+    const int bz = blockIdx.x / bh, by = blockIdx.x - bz * bh;
+    const float4* row = acc + (int64_t)blockIdx.x * bw * 8;
+    for (int t = threadIdx.x; t < bw * 8; t += blockDim.x) {
+        const int z = 2 * bz + ((t >> 2) & 1), y = 2 * by + ((t >> 1) & 1), x = 2 * (t >> 3) + (t & 1);
+        if (z >= g.D || y >= g.H || x >= g.W) continue;
+        const float4 a = row[t];
+        float re = a.x, im = a.y, wt = a.z;
+        if (x == 0) {
+            const int zm = (g.D - z) % g.D, ym = (g.H - y) % g.H;
+            if (!(zm == g.D / 2 && ym == g.H / 2)) {
+                const float4 b = acc[accumulator_slot(g, zm, ym, 0)];
+                re += b.x;
+                im -= b.y;
+                wt += b.z;
+            }
+        }
+        const int64_t o = ((int64_t)z * g.H + y) * g.W + x;
+        vol[o] = make_float2(re, im);
+        wts[o] = wt;
+    }
 }
 
 // Friedel completion of the x=0 plane of already split volumes, in place
@@ -150,40 +185,54 @@ __global__ void mirror_x0_kernel(typename Acc<R>::C* __restrict__ vol, R* __rest
 //   dL/dacc[v] = G[v] + conj(G[m v])  on the x = 0 plane, v not DC
 // and each kept source pixel gathers sum_k w_k dL/dacc[corner k] with the
 // splat's own float32 weights, conjugated where the point was redirected.
-// One thread per slice pixel; every pixel is written (zero when dropped).
-// float: eight resident blocks (32 registers, no spills) for the gathers.
+// One thread per slice pixel, one block per row of tiles (the row part of the
+// geometry formed once per thread); every pixel is written (zero when
+// dropped).  float: eight resident blocks (32 registers) for the gathers.
 template <typename R>
 __global__ void __launch_bounds__(kTileThreads, sizeof(R) == 4 ? 8 : 1)
 insert_bwd_kernel(const typename Acc<R>::C* __restrict__ gvol, const void* __restrict__ rot,
                   typename Acc<R>::C* __restrict__ gimg, SliceGeom g, int tiles) {
     __shared__ float m[9];
-    const int64_t s = blockIdx.x / tiles;
-    const int tile = blockIdx.x - (int)(s * tiles);
+    // one block per (slice, row of tiles); this thread's slice row is fixed
+    const int tx_tiles = tiles_x_of(g.wr);
+    const int rows = tiles / tx_tiles;
+    const int64_t s = blockIdx.x / rows;
+    const int ty = blockIdx.x - (int)(s * rows);
     if (threadIdx.x < 9) m[threadIdx.x] = prep_rotation_elem(rot, g.rot_f64, s, threadIdx.x, g, false);
     __syncthreads();
-    int iy, ix;
-    if (!tile_pixel(g, tile, iy, ix)) return;
-    typename Acc<R>::C out;
-    out.x = 0;
-    out.y = 0;
-    const float qy = shifted_freq(iy, g.img_h, g.inv_h);
-    const float qx = __fmul_rn((float)ix, g.inv_w);
-    bool cj;
-    InsertCell k;
-    if (insert_pixel_kept(g, qy, qx) && insert_cell(g, m, qy, qx, cj, k)) {
+    const int lane = threadIdx.x & 31;
+    const int iy = ty * kTileY + (threadIdx.x >> 5) * 4 + (lane >> 3);
+    if (iy >= g.img_h) return;
+    const SliceRow row = slice_row_geom(g, m, iy);
+    typename Acc<R>::C* orow = gimg + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr;
+    for (int tx = 0; tx < tx_tiles; tx++) {
+        const int ix = tx * kTileX + (lane & 7);
+        if (ix >= g.wr) continue;
+        typename Acc<R>::C out;
+        out.x = 0;
+        out.y = 0;
+        const float qx = __fmul_rn((float)ix, g.inv_w);
+        bool cj;
+        float c[3];
+        const bool kept = (!g.has_fmax || __fsqrt_rn(__fadd_rn(row.qy2, __fmul_rn(qx, qx))) <= g.fmax) &&
+                          !(qx == 0.0f && row.qy < 0.0f);
+        if (kept && insert_coords_row(g, m, row, qx, cj, c)) {
+            InsertCell k;
+            cell_at(c, k);
 #pragma unroll
-        for (int corner = 0; corner < 8; corner++) {
-            const float w = insert_corner_weight(k, corner);
-            if (w == 0.0f) continue;
-            int z, y, x;
-            insert_corner_zyx(k, corner, z, y, x);
-            const typename Acc<R>::C gv = completed_grad<R>(gvol, g, z, y, x);
-            out.x += (R)w * gv.x;
-            out.y += (R)w * gv.y;
+            for (int corner = 0; corner < 8; corner++) {
+                const float w = insert_corner_weight(k, corner);
+                if (w == 0.0f) continue;
+                int z, y, x;
+                insert_corner_zyx(k, corner, z, y, x);
+                const typename Acc<R>::C gv = completed_grad<R>(gvol, g, z, y, x);
+                out.x += (R)w * gv.x;
+                out.y += (R)w * gv.y;
+            }
+            if (cj) out.y = -out.y;
         }
-        if (cj) out.y = -out.y;
+        __stcs(orow + ix, out);
     }
-    __stcs(gimg + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix, out);
 }
 
 int insert_deterministic(const void* image_rfft, int32_t complex128, const void* rot, void* volume, void* weights,
@@ -210,6 +259,22 @@ int insert_phases(size_t acc_bytes) {
     }
     const int k = (int)ceil((double)acc_bytes / (1.1 * (double)l2));
     return k < 1 ? 1 : (k > 16 ? 16 : k);
+}
+
+// Bytes of the 2 x 2 x 2-bricked float accumulator of p's volume.
+size_t bricked_accumulator_bytes(const tt_slice_params* p) {
+    return (size_t)(((p->vol_d + 1) / 2) * ((p->vol_h + 1) / 2) * ((p->vol_w + 1) / 2)) * 8 * sizeof(float4);
+}
+
+// The one-shot float insertion accumulates into the bricked layout from this
+// accumulator size up.  Measured on a B200: 3.86 vs 3.93 ms at 256^3 x 4096
+// slices, 3.21 vs 3.31 ms at 320^3 x 2048, equal at 128^3, and 0.130 vs
+// 0.102 ms at 64^3 x 1000 (where the brick-row finalize's small blocks cost
+// more than the splat saves).
+constexpr size_t kBrickedAccumulatorMinBytes = 64u << 20;
+
+bool insert_bricked(const tt_slice_params* p) {
+    return !p->volume_unshifted && bricked_accumulator_bytes(p) >= kBrickedAccumulatorMinBytes;
 }
 
 int launch_insert_accumulate(const void* image_rfft, int32_t complex128, const void* rot, void* acc,
@@ -281,6 +346,7 @@ extern "C" size_t tt_insert_accumulator_bytes(int32_t complex128, int64_t channe
 extern "C" size_t tt_insert_workspace_bytes(int32_t complex128, const tt_slice_params* p) {
     if (!p) return 0;
     if (p->deterministic) return kFixedHeaderBytes + tt_insert_fixed_accumulator_bytes(1, p->vol_d, p->vol_h, p->vol_w);
+    if (!complex128 && insert_bricked(p)) return bricked_accumulator_bytes(p);  // dims padded to even
     return tt_insert_accumulator_bytes(complex128, 1, p->vol_d, p->vol_h, p->vol_w);
 }
 
@@ -319,6 +385,24 @@ extern "C" int tt_insert_central_slices_rfft_3d(const void* image_rfft, int32_t 
         return insert_deterministic(image_rfft, complex128, rotation_matrices, volume_rfft, weights, workspace, p, st);
     cudaError_t e = cudaMemsetAsync(workspace, 0, need, st);
     if (e != cudaSuccess) return fail(TT_ERR_CUDA, "insert: memset: %s", cudaGetErrorString(e));
+    if (!complex128 && insert_bricked(p)) {
+        // float: the 2 x 2 x 2-bricked accumulator (fewer 128-byte lines per splatted cell)
+        SliceGeom g = make_geom(*p);
+        if (p->n > 0) {
+            const int64_t items = (int64_t)g.n * ((g.img_h + kTileY - 1) / kTileY);
+            if (items > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert: too many blocks");
+            const int nphase = insert_phases(bricked_accumulator_bytes(p));
+            for (int ph = 0; ph < nphase; ph++) {
+                insert_accumulate_kernel<float, true><<<(unsigned)items, kTileThreads, 0, st>>>(
+                    (const float2*)image_rfft, rotation_matrices, (float4*)workspace, g, ph, nphase);
+                if (int r = check_launch("insert_accumulate_kernel")) return r;
+            }
+        }
+        const unsigned rows = (unsigned)(((g.D + 1) / 2) * ((g.H + 1) / 2));
+        insert_finalize_bricked_kernel<<<rows, 256, 0, st>>>((const float4*)workspace, (float2*)volume_rfft,
+                                                             (float*)weights, g);
+        return check_launch("insert_finalize_bricked_kernel");
+    }
     if (p->n > 0)
         if (int r = launch_insert_accumulate(image_rfft, complex128, rotation_matrices, workspace, p, st)) return r;
     return launch_insert_finalize(workspace, complex128, 1, p->vol_d, p->vol_h, p->vol_w, volume_rfft, weights, st);
@@ -333,8 +417,8 @@ extern "C" int tt_insert_central_slices_rfft_3d_backward(const void* grad_volume
         return fail(TT_ERR_INVALID, "insert backward: NULL pointer argument");
     SliceGeom g = make_geom(*p);
     const int tiles = tiles_per_slice(g.img_h, g.wr);
-    const int64_t items = (int64_t)g.n * tiles;
-    if (items > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert backward: too many blocks");
+    if ((int64_t)g.n * tiles > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert backward: too many blocks");
+    const int64_t items = (int64_t)g.n * (tiles / tiles_x_of(g.wr));  // one block per row of tiles
     cudaStream_t st = as_stream(stream);
     if (complex128)
         insert_bwd_kernel<double><<<(unsigned)items, kTileThreads, 0, st>>>((const double2*)grad_volume,

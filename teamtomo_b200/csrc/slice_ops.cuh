@@ -346,6 +346,23 @@ __device__ __forceinline__ bool insert_coords(const SliceGeom& g, const float* m
     return inside_volume(g, c);
 }
 
+// insert_coords with the row part of the geometry precomputed (slice_row_geom):
+// the same operations and roundings.
+__device__ __forceinline__ bool insert_coords_row(const SliceGeom& g, const float* m, const SliceRow& row, float qx,
+                                                  bool& cj, float c[3]) {
+    float p[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++) p[i] = __fadd_rn(row.my[i], __fmul_rn(m[i * 3 + 2], qx));
+    cj = p[2] < 0.0f;
+    if (cj) {
+        p[0] = -p[0];
+        p[1] = -p[1];
+        p[2] = -p[2];
+    }
+    to_dft_coords(g, p, c);
+    return inside_volume(g, c);
+}
+
 // Floor / ceil cell of inside array coordinates c.
 __device__ __forceinline__ void cell_at(const float c[3], InsertCell& k) {
     const float z0 = floorf(c[0]), y0 = floorf(c[1]), x0 = floorf(c[2]);
@@ -437,6 +454,15 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
     }
 }
 
+// Slot of voxel (z, y, x) (fftshifted) in a 2 x 2 x 2-bricked accumulator:
+// bricks of 8 float4 slots (one 128-byte line) in (z, y, x) brick order, x
+// fastest inside a brick; dims padded to even.
+__device__ __forceinline__ int64_t accumulator_slot(const SliceGeom& g, int z, int y, int x) {
+    const int64_t bh = (g.H + 1) >> 1, bw = (g.W + 1) >> 1;
+    return ((((int64_t)(z >> 1) * bh + (y >> 1)) * bw + (x >> 1)) << 3) + ((z & 1) << 2) + ((y & 1) << 1) +
+           (x & 1);
+}
+
 // Float splat of one source pixel with x-paired lanes: lanes 2j and 2j+1
 // reduce the x-low and the x-high corner of the same pixel in the same
 // instruction (adjacent voxels, usually one 32-byte L2 sector), serving pixels
@@ -446,6 +472,12 @@ __device__ __forceinline__ void insert_point_to(const typename Acc<R>::C* __rest
 // ((fz * fy) * fx), CTF weighting and values as insert_point.  Must be called
 // by all 32 lanes of the warp (has_pixel false where the tile overhangs the
 // slice).
+//
+// BRICKED: acc is the 2 x 2 x 2-bricked accumulator (accumulator_slot): the
+// eight corners of a cell whose origin is even on all three axes share one
+// 128-byte line, and a cell touches (1.5)^3 lines on average instead of the
+// 4.5 of four x-rows.
+template <bool BRICKED = false>
 __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ img, const float* m,
                                                     float4* __restrict__ acc, const SliceGeom& g, int64_t s,
                                                     bool has_pixel, int iy, int ix, const CtfConst* ctf = nullptr) {
@@ -493,8 +525,11 @@ __device__ __forceinline__ void insert_point_paired(const float2* __restrict__ i
         for (int zy = 0; zy < 4; zy++) {
             const int bz = zy >> 1, by = zy & 1;
             const float w = ((bz ? k.tz : 1.0f - k.tz) * (by ? k.ty : 1.0f - k.ty)) * fx;
-            if (w != 0.0f)
-                acc_add(acc + vox_index(g, bz ? k.iz1 : k.iz0, by ? k.iy1 : k.iy0, x), sre * w, sim * w, w * sws);
+            if (w != 0.0f) {
+                const int z = bz ? k.iz1 : k.iz0, y = by ? k.iy1 : k.iy0;
+                const int64_t slot = BRICKED ? accumulator_slot(g, z, y, x) : vox_index(g, z, y, x);
+                acc_add(acc + slot, sre * w, sim * w, w * sws);
+            }
         }
     }
 }

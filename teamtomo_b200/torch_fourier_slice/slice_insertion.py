@@ -162,10 +162,34 @@ def _splat(chans, R, volume_shape, fftfreq_max, zyx_matrices, deterministic, c12
             insert_fixed_accumulate(img, R, volume_shape, acc[ch], absmax, max(n, 1), fftfreq_max, zyx_matrices,
                                     images_unshifted=unshifted)
         return insert_fixed_finalize(acc, c128, absmax, n)
+    if len(chans) == 1 and not c128:
+        return _insert_one_shot(chans[0], R, volume_shape, fftfreq_max, zyx_matrices, unshifted)
     acc = new_accumulator(volume_shape, c128, dev, channels=len(chans))
     for ch, img in enumerate(chans):
         insert_accumulate(img, R, volume_shape, acc[ch], fftfreq_max, zyx_matrices, images_unshifted=unshifted)
     return insert_finalize(acc, c128)
+
+
+def _insert_one_shot(image_rfft, R, volume_shape, fftfreq_max, zyx_matrices, unshifted):
+    """Float insertion of one (n, h, w//2+1) stack through the one-shot entry
+    point, whose workspace holds the bricked accumulator."""
+    dev = image_rfft.device
+    if not (image_rfft.is_contiguous() and R.is_contiguous()):
+        raise ValueError("insertion needs C-contiguous slices and rotations")
+    params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=None, rotation=R,
+                          fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices, slices_unshifted=unshifted,
+                          vol_dims=rfft_shape(volume_shape))
+    d, h, w = rfft_shape(volume_shape)
+    volume = torch.empty((1, d, h, w), dtype=torch.complex64, device=dev)
+    weights = torch.empty((d, h, w), dtype=torch.float32, device=dev)
+    L = _lib.load()
+    nbytes = int(L.tt_insert_workspace_bytes(0, params))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    _lib.check(L.tt_insert_central_slices_rfft_3d(_lib.ptr(image_rfft), 0, _lib.ptr(R), _lib.ptr(volume),
+                                                  _lib.ptr(weights), _lib.ptr(ws), nbytes, params,
+                                                  _lib.stream_of(dev)),
+               "insert_central_slices_rfft_3d")
+    return volume, weights
 
 
 def insert_backward(grad_volume, R, volume_shape, fftfreq_max=None, zyx_matrices=False,

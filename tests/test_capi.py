@@ -173,6 +173,15 @@ def test_batched_validation_and_layout():
     bad = (_lib.BatchVolume * 1)(_lib.BatchVolume(_params(vol_w=8), None, fake, fake, fake, None))
     assert L.tt_insert_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
     assert L.tt_extract_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+    # layouts: the extraction takes plain or bricked volumes, one layout per call; the insertion plain only
+    xp = (_lib.BatchVolume * 1)(_lib.BatchVolume(_params(volume_layout=1), fake, fake, fake, fake, None))
+    assert L.tt_extract_central_slices_rfft_3d_batched(xp, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+    assert b"plain or bricked" in L.tt_last_error()
+    mixed = (_lib.BatchVolume * 2)(_lib.BatchVolume(_params(volume_layout=2), fake, fake, fake, fake, None),
+                                   _lib.BatchVolume(_params(), fake, fake, fake, fake, None))
+    assert L.tt_extract_central_slices_rfft_3d_batched(mixed, 2, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+    assert b"one volume_layout" in L.tt_last_error()
+    assert L.tt_insert_central_slices_rfft_3d_batched(mixed, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
 
 
 @pytest.mark.fake_pointers
@@ -256,7 +265,7 @@ def test_workspace_query():
 
     L = _lib.load()
     p = _params(n=4096, img_d=256, img_h=256, img_w=256, vol_d=256, vol_h=256, vol_w=129)
-    tiles = ((129 + 7) // 8) * ((256 + 31) // 32)  # 8 x 32 pixel tiles
+    tiles = ((129 + 7) // 8) * ((256 + 31) // 32)  # 8 x 32 pixel tiles: one slot of 6 partial sums each
     assert L.tt_extract_backward_workspace_bytes(ctypes.byref(p)) == 4096 * tiles * 6 * 4
     assert L.tt_insert_accumulator_bytes(0, 1, 256, 256, 129) == 256 * 256 * 129 * 16
     assert L.tt_insert_accumulator_bytes(1, 2, 4, 4, 3) == 2 * 4 * 4 * 3 * 32
@@ -342,8 +351,8 @@ def test_fused_mse_validation():
     fake = ctypes.c_void_p(16)
     p = _params()
     need = L.tt_central_slice_mse_workspace_bytes(ctypes.byref(p))
-    tiles = ((9 + 7) // 8) * ((16 + 31) // 32)
-    assert need == 4 * tiles * 8 + 4 * tiles * 6 * 4
+    rows = (16 + 31) // 32  # loss (double) and rotation partials per row of tiles
+    assert need == 4 * rows * 8 + 4 * rows * 6 * 4
     assert L.tt_central_slice_mse(fake, fake, fake, fake, None, None, fake, 8, ctypes.byref(p),
                                   None) == _lib.TT_ERR_WORKSPACE
     assert L.tt_central_slice_mse(fake, fake, fake, None, None, None, fake, need, ctypes.byref(p),

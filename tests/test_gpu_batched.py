@@ -156,10 +156,26 @@ def test_autotuner_caches_the_fastest_shape(tmp_path, monkeypatch):
     monkeypatch.setenv("TT_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
     monkeypatch.setattr(autotune, "_mem", None)
     times = autotune.tune("extract", 48, n_slices=32, repeats=2)
-    assert set(times) == {0, 1, 2} and all(t > 0 for t in times.values())
-    best = min(times, key=times.get)
-    assert autotune.cached_tile_shape("extract", 48, torch.device("cuda")) == best
+    # every tile shape with both volume layouts
+    assert set(times) == {(t, lay) for t in (0, 1, 2) for lay in ("plain", "bricks")}
+    assert all(t > 0 for t in times.values())
+    best_ts, best_lay = min(times, key=times.get)
+    dev = torch.device("cuda")
+    assert autotune.cached_tile_shape("extract", 48, dev) == best_ts
+    assert autotune.cached_layout("extract", 48, dev) == (2 if best_lay == "bricks" else 0)
     assert (tmp_path / "tune.json").exists()
     monkeypatch.setattr(autotune, "_mem", None)  # reload from disk
-    assert autotune.cached_tile_shape("extract", 48, torch.device("cuda")) == best
-    assert autotune.cached_tile_shape("insert", 48, torch.device("cuda")) == autotune.DEFAULT_TILE_SHAPE
+    assert autotune.cached_tile_shape("extract", 48, dev) == best_ts
+    assert autotune.cached_tile_shape("insert", 48, dev) == autotune.DEFAULT_TILE_SHAPE
+    assert autotune.cached_layout("insert", 48, dev) is None
+
+
+def test_batched_extraction_from_bricked_copies_is_bitwise_plain():
+    """The bricked copies give the same slices bit for bit, CTF included."""
+    boxes, vols, rots, ctfs = _uneven_batch(4)
+    plain = B().extract_central_slices_rfft_3d_batched(vols, rots, ctf=ctfs, volume_layout="plain")
+    bricks = B().extract_central_slices_rfft_3d_batched(vols, rots, ctf=ctfs, volume_layout="bricks")
+    for a, b in zip(plain, bricks):
+        assert torch.equal(a, b)
+    with pytest.raises(ValueError):
+        B().extract_central_slices_rfft_3d_batched(vols, rots, volume_layout="xpairs")

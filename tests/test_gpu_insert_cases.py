@@ -1,6 +1,7 @@
 """Insertion cases beyond the golden vectors: the one-shot C entry point
-(tt_insert_central_slices_rfft_3d, its own workspace and finalize) against
-the Python API's accumulate + finalize form and the oracle, on odd boxes,
+(tt_insert_central_slices_rfft_3d, its own workspace and finalize; for
+accumulators of 64 MB and more a 2 x 2 x 2-bricked accumulator) against the
+accumulate + finalize form (plain accumulator) and the oracle, on odd boxes,
 fftfreq_max, zyx matrices, axis-aligned and 180-degree-apart rotations, many
 slices of a small box, and several calls into one accumulator.
 
@@ -72,6 +73,8 @@ def _two_stage(imgs, n, rots, fftfreq_max=None, zyx_matrices=False):
     (32, 1, {}), (32, 7, {}), (48, 200, {}), (64, 300, {}), (63, 120, {}),  # odd box
     (65, 90, dict(fftfreq_max=0.3)), (64, 150, dict(zyx_matrices=True)),
     (96, 64, dict(fftfreq_max=0.45)), (128, 256, {}),
+    # accumulators of 64 MB and more: the one-shot splat uses the bricked layout
+    (201, 60, {}), (256, 30, dict(zyx_matrices=True)),
 ])
 def test_one_shot_matches_two_stage_and_oracle(oracle, n, nrot, kw):
     imgs = _images(n, nrot, seed=n + nrot)
