@@ -1089,13 +1089,13 @@ def main():
                 tt.distributed.all_reduce_sum(w)
             # the results go out on their own stream: the device-to-host copies
             # of this step overlap the host-to-device copies of the next one
-            d2h.wait_stream(stream)
-            with torch.cuda.stream(d2h):
+            out_stream.wait_stream(stream)
+            with torch.cuda.stream(out_stream):
                 for src, dst in ((Vd.grad, h_dV), (vol, h_vol), (w, h_w), (loss, h_loss)):
-                    src.record_stream(d2h)
+                    src.record_stream(out_stream)
                     dst.copy_(src, non_blocking=True)
 
-        d2h = torch.cuda.Stream(device=dev)
+        out_stream = torch.cuda.Stream(device=dev)
         e2e_steps = max(3, min(args.steps, 10))
         e2e_step()
         torch.cuda.synchronize(dev)
@@ -1105,7 +1105,7 @@ def main():
         s2.record(stream)
         for _ in range(e2e_steps):
             e2e_step()
-        stream.wait_stream(d2h)  # the last step's results are on the host before the clock stops
+        stream.wait_stream(out_stream)  # the last step's results are on the host before the clock stops
         e2.record(stream)
         torch.cuda.synchronize(dev)
         el2 = s2.elapsed_time(e2)
