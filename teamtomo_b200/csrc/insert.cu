@@ -19,8 +19,9 @@
 // The one-shot entry point (tt_insert_central_slices_rfft_3d) accumulates
 // large float volumes into a 2 x 2 x 2-bricked accumulator instead
 // (accumulator_slot: the eight corners of an even-aligned cell share one
-// 128-byte line; a cell touches 3.4 lines on average instead of 4.5), split
-// by insert_finalize_bricked_kernel.
+// 128-byte line; a cell touches 3.4 lines on average instead of 4.5), with
+// the eight corners of a pixel reduced by eight lanes in one instruction
+// (insert_point_octet), split by insert_finalize_bricked_kernel.
 //
 // Finalize stage: the reference also inserts conj(data)*w at ((d-z)%d, (h-y)%h, 0)
 // for every corner that lands on the x=0 plane except the DC voxel.  Summed
@@ -59,8 +60,10 @@ insert_accumulate_kernel(const typename Acc<R>::C* __restrict__ img, const void*
             continue;
         int iy, ix;
         const bool has_pixel = tile_pixel(g, ty * tx_tiles + tx, iy, ix);
-        if constexpr (std::is_same<R, float>::value)
-            insert_point_paired<BRICKED>(img, m, acc, g, s, has_pixel, iy, ix);  // every lane takes part
+        if constexpr (std::is_same<R, float>::value && BRICKED)
+            insert_point_octet(img, m, acc, g, s, has_pixel, iy, ix);  // every lane takes part
+        else if constexpr (std::is_same<R, float>::value)
+            insert_point_paired(img, m, acc, g, s, has_pixel, iy, ix);  // every lane takes part
         else if (has_pixel)
             insert_point<R>(img, m, acc, g, s, iy, ix);
     }
