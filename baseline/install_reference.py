@@ -18,7 +18,7 @@ import os
 import shutil
 import sys
 
-PACKAGES = ("torch-fourier-slice", "torch-image-interpolation", "torch-grid-utils")
+PACKAGES = ("torch-fourier-slice", "torch-image-interpolation", "torch-grid-utils", "torch-ctf")
 
 
 def main() -> int:

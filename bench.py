@@ -188,6 +188,74 @@ def reference_modules():
     return ref_extract, ref_insert
 
 
+def reference_ctf():
+    """calculate_ctf_2d of the reference's torch-ctf from baseline/_ref, or None."""
+    if not os.path.isdir(os.path.join(REF_DIR, "torch_ctf")):
+        return None
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    from torch_ctf import calculate_ctf_2d
+
+    return calculate_ctf_2d
+
+
+def reference_ctf_images(calc, rows, box):
+    """(n, box, box//2+1) CTF images of the reference's calculate_ctf_2d
+    (rfft, fftshifted) for (n, 8) rows of batched.ctf_params."""
+    c = rows.float()
+    return calc(defocus=c[:, 0], astigmatism=c[:, 1], astigmatism_angle=c[:, 2], voltage=c[:, 3],
+                spherical_aberration=c[:, 4], amplitude_contrast=c[:, 5], phase_shift=c[:, 6],
+                pixel_size=c[:, 7], image_shape=(box, box), rfft=True, fftshift=True)
+
+
+def reference_ctf_insert(mods, calc, images, R, rows, box):
+    """CTF-weighted insertion in the reference's own code: the CTF images,
+    then one insertion of images x CTF (the volume) and one of CTF^2 (whose
+    real part is the weights); the rotations go in as a copy (the reference
+    zeroes near-zero elements of its argument in place)."""
+    import torch
+
+    _, ref_insert = mods
+    shape = (box, box, box)
+    with torch.no_grad():
+        ctf = reference_ctf_images(calc, rows, box)
+        v, _ = ref_insert(images * ctf, shape, R.clone())
+        w, _ = ref_insert((ctf * ctf).to(images.dtype), shape, R.clone())
+    return v, w.real
+
+
+def reference_ctf_extract_insert(mods, calc, vol, R, rows, box):
+    """One volume of the batched step in the reference's own code: CTF
+    images, the CTF-weighted extraction, then the CTF-weighted insertion of
+    those slices."""
+    import torch
+
+    ref_extract, _ = mods
+    with torch.no_grad():
+        ctf = reference_ctf_images(calc, rows, box)
+        S = ref_extract(vol, (box, box, box), R.clone()) * ctf
+    return reference_ctf_insert(mods, calc, S, R, rows, box)
+
+
+def reference_extract_fwd_bwd(mods, V, R, T, box):
+    """Extraction, MSE against T and the autograd backward for d/drotation in
+    the reference's own code (d/dvolume left out: its autograd expands the
+    volume per sample point)."""
+    ref_extract, _ = mods
+    Rg = R.double().clone().requires_grad_(True)
+    S = ref_extract(V, (box, box, box), Rg)
+    (S - T).abs().square().mean().backward()
+
+
+def _host_seconds(fn, warm=None):
+    """Wall time of fn() on the host (one untimed call of warm() first)."""
+    if warm is not None:
+        warm()
+    t0 = time.perf_counter()
+    fn()
+    return time.perf_counter() - t0
+
+
 def cpu_workload(box, sample, mods, seed=ROT_SEED):
     """The GPU arm's workload on the host: the same seeded blob volumes, the
     first ``sample`` of its 4096 rotations, targets = central slices of the
@@ -485,6 +553,7 @@ def batched_workload(args):
     tr = load_traffic()
     re_, ri_ = tr.get("batched_extract_per_algorithmic_byte"), tr.get("batched_insert_per_algorithmic_byte")
     traffic = int(re_ * algo_e + ri_ * algo_i) if re_ and ri_ else None
+    ref_gpu, ref_cpu = batched_reference_legs(args, dev, vols, rots, ctfs, boxes, counts)
     line = {
         "metric": "slices/s CTF-weighted extract+insert, 32 uneven volumes, one launch per stage",
         "value": total / (ms / 1e3), "unit": "slices/s", "n_gpus": 1, "steps": args.steps,
@@ -501,10 +570,93 @@ def batched_workload(args):
         "autotune_ms": {k: {(f"{s[0]}/{s[1]}" if s[1] else str(s[0])): round(t, 4) for s, t in v.items()}
                         for k, v in tuned.items()},
         "clocks": clk, "gpu_launches": args.steps * (3 + nvol),
+        "torch_gpu_reference": ref_gpu, "cpu_baseline": ref_cpu,
     }
     del outs
     print(json.dumps(line))
     return 0
+
+
+def batched_reference_legs(args, dev, vols, rots, ctfs, boxes, counts, gpu_sample=256, cpu_sample=4):
+    """The batched step in the reference's own code (per volume: CTF images,
+    CTF-weighted extraction, CTF-weighted insertion as two insertions), timed
+    on the first ``gpu_sample`` slices of every volume on this GPU and the
+    first ``cpu_sample`` on the host cores; each volume's time is scaled
+    linearly to its slice count and the rate is the step's slices over the
+    sum.  Returns (torch_gpu_reference, cpu_baseline), None where skipped."""
+    import torch
+
+    mods, calc = reference_modules(), reference_ctf()
+    if mods is None or calc is None:
+        why = {"unavailable": "baseline/_ref missing (run baseline/install_reference.py)"}
+        return why, why
+    total = sum(counts)
+    gpu = cpu = None
+    if not args.no_torch_gpu:
+        est = 0.0
+        for v, r, c, b, n in zip(vols, rots, ctfs, boxes, counts):
+            k = min(n, gpu_sample)
+            fn = lambda: reference_ctf_extract_insert(mods, calc, v, r[:k], c[:k], b)  # noqa: E731
+            est += _time_device(fn, 1, 1, dev) / 1e3 * n / k
+        gpu = {"value": total / est, "unit": "slices/s",
+               "sample": f"first {gpu_sample} slices of each volume (all of smaller ones), each volume's time "
+                         "scaled linearly to its slice count (extrapolated)",
+               "code": "reference torch_fourier_slice + torch_ctf, unmodified, CUDA tensors: calculate_ctf_2d, "
+                       "extract x CTF, insert(slices x CTF) + insert(CTF^2) for the weights"}
+    if not args.no_cpu_baseline:
+        est = 0.0
+        for v, r, c, b, n in zip(vols, rots, ctfs, boxes, counts):
+            k = min(n, cpu_sample)
+            vc, rc, cc = v.cpu(), r[:k].cpu(), c[:k].cpu()
+            est += _host_seconds(lambda: reference_ctf_extract_insert(mods, calc, vc, rc, cc, b),
+                                 warm=lambda: reference_ctf_extract_insert(mods, calc, vc, rc[:1], cc[:1], b)) * n / k
+        cpu = {"value": total / est, "unit": "slices/s", "cores": torch.get_num_threads(), "kind": "reference",
+               "host_cpus": os.cpu_count(),
+               "sample": f"first {cpu_sample} slices of each volume on the host cores, each volume's time scaled "
+                         "linearly to its slice count (extrapolated); the reference's torch code as in "
+                         "torch_gpu_reference"}
+    return gpu, cpu
+
+
+def fullscale_reference_legs(args, dev, images, V, n, gpu=(256, 256), cpu=(16, 8)):
+    """The full-scale workload in the reference's own code on a prefix:
+    the CTF-weighted insertion (CTF images, insert(images x CTF),
+    insert(CTF^2) for the weights) of the first images, and the extraction
+    with MSE and autograd d/drotation (d/dvolume left out) of the first
+    orientations, on this GPU (``gpu`` = images, orientations) and on the
+    host cores (``cpu``); rates per image / orientation, extrapolated
+    linearly to the workload.  Returns (torch_gpu_reference, cpu_baseline)."""
+    import torch
+
+    mods, calc = reference_modules(), reference_ctf()
+    if mods is None or calc is None:
+        why = {"unavailable": "baseline/_ref missing (run baseline/install_reference.py)"}
+        return why, why
+    R, ctf, S = images(0, max(gpu))
+    out_gpu = out_cpu = None
+    if not args.no_torch_gpu:
+        ni, ne = gpu
+        ti = _time_device(lambda: reference_ctf_insert(mods, calc, S[:ni], R[:ni], ctf[:ni], n), 1, 1, dev)
+        te = _time_device(lambda: reference_extract_fwd_bwd(mods, V, R[:ne], S[:ne], n), 1, 1, dev)
+        out_gpu = {"value": ni / (ti / 1e3), "unit": "images/s",
+                   "extract_fwd_bwd": {"value": ne / (te / 1e3), "unit": "slices/s",
+                                       "excluded": "d/dvolume (the reference's autograd expands the volume per "
+                                                   "sample point)"},
+                   "sample": f"first {ni} images / {ne} orientations, extrapolated linearly",
+                   "code": "reference torch_fourier_slice + torch_ctf, unmodified, CUDA tensors"}
+    if not args.no_cpu_baseline:
+        ni, ne = cpu
+        Vc, Rc, Sc, Cc = V.cpu(), R[:max(cpu)].cpu(), S[:max(cpu)].cpu(), ctf[:max(cpu)].cpu()
+        ti = _host_seconds(lambda: reference_ctf_insert(mods, calc, Sc[:ni], Rc[:ni], Cc[:ni], n),
+                           warm=lambda: reference_ctf_insert(mods, calc, Sc[:1], Rc[:1], Cc[:1], n))
+        te = _host_seconds(lambda: reference_extract_fwd_bwd(mods, Vc, Rc[:ne], Sc[:ne], n),
+                           warm=lambda: reference_extract_fwd_bwd(mods, Vc, Rc[:1], Sc[:1], n))
+        out_cpu = {"value": ni / ti, "unit": "images/s", "cores": torch.get_num_threads(), "kind": "reference",
+                   "host_cpus": os.cpu_count(),
+                   "extract_fwd_bwd": {"value": ne / te, "unit": "slices/s"},
+                   "sample": f"first {ni} images / {ne} orientations on the host cores, extrapolated linearly; "
+                             "the reference's torch code as in torch_gpu_reference (d/dvolume left out)"}
+    return out_gpu, out_cpu
 
 
 def _ref_module():
@@ -562,10 +714,17 @@ def config_workload(args):
         ms = _time_device(lambda: tt.project_3d_to_2d(vol, R), args.steps, args.warmup, dev)
         clk = clocks.stop()
         ref_ms = (_time_device(lambda: ref.project_3d_to_2d(vol, R), 5, 2, dev) if ref else None)
+        cpu = None
+        if ref is not None and not args.no_cpu_baseline:
+            vc, Rc = vol.cpu(), R.cpu()
+            t = _host_seconds(lambda: ref.project_3d_to_2d(vc, Rc), warm=lambda: ref.project_3d_to_2d(vc, Rc[:2]))
+            cpu = {"value": k / t, "unit": "slices/s", "cores": torch.get_num_threads(), "kind": "reference",
+                   "host_cpus": os.cpu_count(), "sample": f"the whole workload ({k} rotations), reference "
+                   "project_3d_to_2d (baseline/_ref, unmodified) on the host cores"}
         out.update({"metric": "slices/s project_3d_to_2d 64^3 pad 2.0", "value": k / (ms / 1e3), "unit": "slices/s",
                     "ms_per_step": ms, "config": {"workload": "project 64^3 x 100 rotations, pad 2.0"},
                     "torch_gpu_reference": None if ref is None else {"value": k / (ref_ms / 1e3), "ms": ref_ms},
-                    "clocks": clk, "gpu_launches": 4 * args.steps})
+                    "cpu_baseline": cpu, "clocks": clk, "gpu_launches": 4 * args.steps})
     elif args.workload == "backproject":
         n, k = 128, 10_000
         vol = blob_volume_torch(n, 1002, dev)
@@ -590,11 +749,25 @@ def config_workload(args):
             for pf in (1.0, 2.0):
                 rms = _time_device(lambda: ref.backproject_2d_to_3d(imgs[:m], R[:m], pad_factor=pf), 2, 1, dev)
                 refres[f"pad{pf:g}"] = {"value": m / (rms / 1e3), "sample": m}
+        cpu = None
+        if ref is not None and not args.no_cpu_baseline:
+            m = 100  # prefix of the images on the host cores, extrapolated linearly
+            ic, Rc = imgs[:m].cpu(), R[:m].cpu()
+            cpu = {"unit": "images/s", "cores": torch.get_num_threads(), "kind": "reference",
+                   "host_cpus": os.cpu_count(),
+                   "sample": f"first {m} of the {k} images on the host cores, extrapolated linearly; reference "
+                             "backproject_2d_to_3d (baseline/_ref, unmodified); value at pad 1.0"}
+            for pf in (1.0, 2.0):
+                t = _host_seconds(lambda: ref.backproject_2d_to_3d(ic, Rc, pad_factor=pf),
+                                  warm=lambda: ref.backproject_2d_to_3d(ic[:2], Rc[:2], pad_factor=pf))
+                cpu[f"pad{pf:g}"] = m / t
+            cpu["value"] = cpu["pad1"]
         out.update({"metric": "images/s backproject_2d_to_3d 10,000 x 128^2", "value": res["pad1"]["value"],
                     "unit": "images/s", "ms_per_step": res["pad1"]["ms_per_step"],
                     "config": {"workload": "backproject 10,000 x 128^2 (SNR 0.1); value at pad 1.0 "
                                "(128x128x65 volume), pad 2.0 beside it"},
-                    "pads": res, "torch_gpu_reference": refres, "clocks": clk, "gpu_launches": 5 * args.steps})
+                    "pads": res, "torch_gpu_reference": refres, "cpu_baseline": cpu, "clocks": clk,
+                    "gpu_launches": 5 * args.steps})
     else:
         n, n_img, n_ext, chunk = 320, 200_000, 100_000, 10_000
         vol_real = blob_volume_torch(n, 1005, dev)
@@ -641,6 +814,7 @@ def config_workload(args):
             torch.cuda.synchronize(dev)
             ext_ms += a.elapsed_time(b)
         clk = clocks.stop()
+        ref_gpu, ref_cpu = fullscale_reference_legs(args, dev, images, Vfit.detach(), n)
         out.update({"metric": "images/s CTF-weighted insertion, 320^3, 200,000 images; then slices/s extract "
                               "fwd+bwd, 100,000 orientations",
                     "value": n_img / (ins_ms / 1e3), "unit": "images/s", "ms_per_step": ins_ms + ext_ms,
@@ -650,7 +824,7 @@ def config_workload(args):
                     "config": {"workload": "full scale: 320^3 complex64 rfft volume (320x320x161), "
                                f"images generated on the GPU in chunks of {chunk} (not timed)",
                                "images": n_img, "orientations": n_ext},
-                    "torch_gpu_reference": None, "clocks": clk,
+                    "torch_gpu_reference": ref_gpu, "cpu_baseline": ref_cpu, "clocks": clk,
                     # insertion: splat, finalize, sum; fused MSE: loss kernel, loss and rotation finish
                     # (+ the pack of the volume copy the gathers read)
                     "gpu_launches": n_img // chunk * 3
