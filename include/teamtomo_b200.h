@@ -257,6 +257,25 @@ int tt_insert_accumulate(const void *image_rfft, int32_t complex128, const void 
 int tt_insert_finalize(const void *accumulator, int32_t complex128, int64_t channels, int64_t d,
                        int64_t h, int64_t w_rfft, void *volume_rfft, void *weights, void *stream);
 
+/* Accumulator layout for p's volume in the batched float insertion:
+ * TT_VOLUME_BRICKS from 64 MB of accumulator up while it fits one z-phase
+ * (about 1.1 x the L2; fftshifted volumes), else TT_VOLUME_PLAIN (the
+ * one-shot tt_insert_central_slices_rfft_3d bricks every accumulator from
+ * 64 MB up, whatever its phases).  A bricked accumulator holds 2 x 2 x 2 voxel bricks of 8
+ * (re, im, w, pad) float32 slots (one 128-byte line) in (z, y, x) brick
+ * order, x fastest inside a brick, dims rounded up to even
+ * (tt_insert_bricked_accumulator_bytes); the splat reduces the eight
+ * corners of a pixel in one instruction.  The batched insertion takes one
+ * per volume (params.volume_layout = TT_VOLUME_BRICKS), finished by
+ * tt_insert_finalize_bricked.  No counterpart in the reference (its
+ * index_put_ accumulates into the output volume directly). */
+int32_t tt_insert_accumulator_layout(const tt_slice_params *p);
+size_t tt_insert_bricked_accumulator_bytes(int64_t d, int64_t h, int64_t w_rfft);
+/* Bricked accumulator -> volume (d, h, w_rfft) complex64 and weights (may be
+ * NULL) with the Friedel completion of the x=0 plane, as tt_insert_finalize. */
+int tt_insert_finalize_bricked(const void *accumulator, int64_t d, int64_t h, int64_t w_rfft,
+                               void *volume_rfft, void *weights, void *stream);
+
 /* Friedel completion of the x=0 plane, equal to the reference's per-corner
  * mirror insertion (_insert_central_slices_rfft_3d.py:350-404):
  * out[v] = acc[v] + conj(acc[m(v)]) unless m(v) is the DC voxel, with
@@ -387,7 +406,9 @@ typedef struct tt_batch_volume {
     tt_slice_params params;          /* geometry of this volume's slices (params.n = its slice count) */
     const void *volume_rfft;         /* extraction: complex64 source volume */
     void *slices;                    /* extraction: complex64 output (n, h, w/2+1); insertion: input */
-    void *accumulator;               /* insertion: (re, im, w, pad) float32 slots, zeroed by the caller */
+    void *accumulator;               /* insertion: (re, im, w, pad) float32 slots, zeroed by the caller;
+                                        bricked when params.volume_layout = TT_VOLUME_BRICKS
+                                        (tt_insert_accumulator_layout) */
     const void *rotation_matrices;   /* (n, 3, 3) float32 or float64 */
     const tt_ctf_params *ctf;        /* device array of n CTFs, or NULL for none.  Extraction
                                         multiplies each slice by its CTF; insertion weights the
@@ -399,7 +420,8 @@ int tt_extract_central_slices_rfft_3d_batched(const tt_batch_volume *volumes, in
                                               int32_t tile_shape, void *workspace,
                                               size_t workspace_bytes, void *stream);
 /* Accumulates into each volume's accumulator; finish each volume with
- * tt_insert_finalize (Friedel completion, volume + weights). */
+ * tt_insert_finalize, or tt_insert_finalize_bricked for a bricked one
+ * (Friedel completion, volume + weights). */
 int tt_insert_central_slices_rfft_3d_batched(const tt_batch_volume *volumes, int32_t n_volumes,
                                              int32_t tile_shape, void *workspace,
                                              size_t workspace_bytes, void *stream);

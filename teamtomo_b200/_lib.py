@@ -81,6 +81,9 @@ SIGNATURES = {
     "tt_insert_central_slices_rfft_3d_backward": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_accumulate": ([_vp, _i32, _vp, _vp, ctypes.POINTER(SliceParams), _vp], _i32),
     "tt_insert_finalize": ([_vp, _i32, _i64, _i64, _i64, _i64, _vp, _vp, _vp], _i32),
+    "tt_insert_accumulator_layout": ([ctypes.POINTER(SliceParams)], _i32),
+    "tt_insert_bricked_accumulator_bytes": ([_i64, _i64, _i64], _sz),
+    "tt_insert_finalize_bricked": ([_vp, _i64, _i64, _i64, _vp, _vp, _vp], _i32),
     "tt_friedel_mirror_x0": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp], _i32),
     "tt_insert_workspace_bytes": ([_i32, ctypes.POINTER(SliceParams)], _sz),
     "tt_fixed_absmax": ([_vp, _i32, _i64, _vp, _vp], _i32),

@@ -27,6 +27,7 @@ import torch
 
 from . import _lib
 from .torch_fourier_slice._params import rfft_shape, rotation_arg, slice_params
+from .torch_fourier_slice._layout import BRICKS as _BRICKS
 from .torch_fourier_slice.slice_insertion import insert_finalize, new_accumulator
 
 CTF_FIELDS = ("defocus_um", "astigmatism_um", "astigmatism_angle_deg", "voltage_kv",
@@ -188,6 +189,7 @@ def insert_central_slices_rfft_3d_batched(
     shapes = list(volume_shapes) if volume_shapes is not None else [
         (im.shape[-2], im.shape[-2], im.shape[-2]) for im in images]
     accs, entries, keep = [], [], []
+    L = _lib.load()
     for img, R, shape, c in zip(images, rotation_matrices, shapes, ctf):
         if img.dtype != torch.complex64:
             raise ValueError("batched insertion takes complex64 slices")
@@ -199,22 +201,37 @@ def insert_central_slices_rfft_3d_batched(
         if math.prod(img.shape[:-2]) != n:
             raise ValueError(f"{n} rotation matrices for {math.prod(img.shape[:-2])} slices")
         img = _lib.dense(img.reshape(n, *img.shape[-2:]))
-        acc = new_accumulator(shape, False, dev)
         cc = _check_ctf(c, n, dev)
         p = slice_params(n=n, image_shape=shape, volume=None, rotation=Rm, fftfreq_max=fftfreq_max,
                          zyx_matrices=zyx_matrices, vol_dims=rfft_shape(shape))
+        # large accumulators are 2 x 2 x 2-bricked (the library's policy, as the one-shot insertion)
+        p.volume_layout = int(L.tt_insert_accumulator_layout(ctypes.byref(p)))
+        if p.volume_layout == _BRICKS:
+            d, h, w = rfft_shape(shape)
+            acc = torch.zeros(int(L.tt_insert_bricked_accumulator_bytes(d, h, w)) // 4, dtype=torch.float32,
+                              device=dev)
+        else:
+            acc = new_accumulator(shape, False, dev)
         entries.append(_lib.BatchVolume(p, None, img.data_ptr(), acc.data_ptr(), Rm.data_ptr(),
                                         cc.data_ptr() if cc is not None else None))
         keep += [img, Rm, cc]
-        accs.append(acc)
+        accs.append((acc, p.volume_layout, rfft_shape(shape)))
     ts = _tile_shape("insert", [s[-2] for s in shapes], dev, tile_shape)
     for chunk in _batches(entries):
         _run("tt_insert_central_slices_rfft_3d_batched", chunk, ts, dev,
              "insert_central_slices_rfft_3d_batched")
     out = []
-    for acc in accs:
-        v, w = insert_finalize(acc, False)
-        out.append((v[0], w))
+    for acc, layout, (d, h, w) in accs:
+        if layout == _BRICKS:
+            vol = torch.empty((d, h, w), dtype=torch.complex64, device=dev)
+            wts = torch.empty((d, h, w), dtype=torch.float32, device=dev)
+            _lib.check(L.tt_insert_finalize_bricked(_lib.ptr(acc), d, h, w, _lib.ptr(vol), _lib.ptr(wts),
+                                                    _lib.stream_of(dev)),
+                       "insert_central_slices_rfft_3d_batched finalize")
+            out.append((vol, wts))
+        else:
+            v, wt = insert_finalize(acc, False)
+            out.append((v[0], wt))
     return out
 
 

@@ -128,8 +128,11 @@ batched_slices_kernel(const __grid_constant__ BatchParams bp, unsigned long long
                     continue;
                 const int ix = tx * TX + (lane % TX);
                 const bool has_pixel = ix < bv.g.wr && iy < bv.g.img_h;
-                // every lane takes part: lane pairs share a pixel's x-corners
-                insert_point_paired(bv.slices, m, bv.acc, bv.g, s, has_pixel, iy, ix, ccp);
+                // every lane takes part: lane octets (bricked accumulator) or lane pairs share a pixel
+                if (bv.g.vol_layout == TT_VOLUME_BRICKS)
+                    insert_point_octet(bv.slices, m, bv.acc, bv.g, s, has_pixel, iy, ix, ccp);
+                else
+                    insert_point_paired(bv.slices, m, bv.acc, bv.g, s, has_pixel, iy, ix, ccp);
             }
         }
         if (threadIdx.x == 0) {
@@ -144,10 +147,11 @@ static int tiles_for_shape(const SliceGeom& g) {
     return tiles_t<TX>(g.img_h, g.wr);
 }
 
-int insert_phases(size_t acc_bytes);  // insert.cu
+int insert_phases(size_t acc_bytes);                     // insert.cu
+size_t bricked_accumulator_bytes(const tt_slice_params* p);  // insert.cu
 
 template <int TX, bool INSERT, typename VT>
-static int launch_batched(BatchParams& bp, unsigned long long* queue, cudaStream_t st) {
+static int launch_batched(BatchParams& bp, const size_t* acc_bytes, unsigned long long* queue, cudaStream_t st) {
     constexpr int TY = 256 / TX;
     bp.item_offset[0] = 0;
     for (int v = 0; v < bp.nvol; v++) {
@@ -169,7 +173,7 @@ static int launch_batched(BatchParams& bp, unsigned long long* queue, cudaStream
     int nphase = 1;
     if (INSERT)
         for (int v = 0; v < bp.nvol; v++) {
-            const int k = insert_phases((size_t)((int64_t)bp.v[v].g.D * bp.v[v].g.H * bp.v[v].g.W) * sizeof(float4));
+            const int k = insert_phases(acc_bytes[v]);
             nphase = k > nphase ? k : nphase;
         }
     for (int ph = 0; ph < nphase; ph++) {
@@ -193,6 +197,7 @@ static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_
     if (!workspace || workspace_bytes < sizeof(unsigned long long))
         return fail(TT_ERR_WORKSPACE, "%s: workspace of %zu bytes needed", what, sizeof(unsigned long long));
     static BatchParams bp;  // large; filled under the lock below
+    static size_t acc_bytes[kMaxBatch];
     static std::mutex mu;
     std::lock_guard<std::mutex> lock(mu);
     bp.nvol = n_volumes;
@@ -200,7 +205,7 @@ static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_
     int64_t slices = 0;
     for (int v = 0; v < n_volumes; v++) {
         const tt_batch_volume& x = volumes[v];
-        if (int e = validate_params(&x.params, !insert)) return e;
+        if (int e = validate_params(&x.params, true)) return e;
         if (!insert && x.params.volume_layout == TT_VOLUME_XPAIRS)
             return fail(TT_ERR_INVALID, "%s: volume %d: the batched extraction takes plain or bricked volumes", what,
                         v);
@@ -216,6 +221,10 @@ static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_
             if (!x.rotation_matrices || !x.slices) return fail(TT_ERR_INVALID, "%s: volume %d: NULL pointer", what, v);
             if (insert) {
                 if (!x.accumulator) return fail(TT_ERR_INVALID, "%s: volume %d: NULL accumulator", what, v);
+                if (x.params.volume_layout != TT_VOLUME_PLAIN &&
+                    (x.params.volume_layout != TT_VOLUME_BRICKS || x.params.volume_unshifted))
+                    return fail(TT_ERR_INVALID,
+                                "%s: volume %d: the accumulator is plain or (fftshifted volumes) bricked", what, v);
                 if (x.params.vol_d != x.params.img_d || x.params.vol_h != x.params.img_h ||
                     x.params.vol_w != x.params.img_w / 2 + 1)
                     return fail(TT_ERR_INVALID, "%s: volume %d: dims are not the rfft of volume_shape", what, v);
@@ -230,6 +239,9 @@ static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_
         d.acc = (float4*)x.accumulator;
         d.rot = x.rotation_matrices;
         d.ctf = x.ctf;
+        acc_bytes[v] = x.params.volume_layout == TT_VOLUME_BRICKS
+                           ? bricked_accumulator_bytes(&x.params)
+                           : (size_t)(x.params.vol_d * x.params.vol_h * x.params.vol_w) * sizeof(float4);
         slices += x.params.n;
     }
     if (slices == 0) return TT_OK;
@@ -238,18 +250,18 @@ static int run_batched(const tt_batch_volume* volumes, int32_t n_volumes, int32_
     cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st);
     if (e != cudaSuccess) return fail(TT_ERR_CUDA, "%s: memset: %s", what, cudaGetErrorString(e));
     if (insert) {
-        if (tile_shape == 0) return launch_batched<8, true, float2>(bp, queue, st);
-        if (tile_shape == 1) return launch_batched<16, true, float2>(bp, queue, st);
-        return launch_batched<32, true, float2>(bp, queue, st);
+        if (tile_shape == 0) return launch_batched<8, true, float2>(bp, acc_bytes, queue, st);
+        if (tile_shape == 1) return launch_batched<16, true, float2>(bp, acc_bytes, queue, st);
+        return launch_batched<32, true, float2>(bp, acc_bytes, queue, st);
     }
     if (layout == TT_VOLUME_BRICKS) {
-        if (tile_shape == 0) return launch_batched<8, false, VoxBrick2>(bp, queue, st);
-        if (tile_shape == 1) return launch_batched<16, false, VoxBrick2>(bp, queue, st);
-        return launch_batched<32, false, VoxBrick2>(bp, queue, st);
+        if (tile_shape == 0) return launch_batched<8, false, VoxBrick2>(bp, acc_bytes, queue, st);
+        if (tile_shape == 1) return launch_batched<16, false, VoxBrick2>(bp, acc_bytes, queue, st);
+        return launch_batched<32, false, VoxBrick2>(bp, acc_bytes, queue, st);
     }
-    if (tile_shape == 0) return launch_batched<8, false, float2>(bp, queue, st);
-    if (tile_shape == 1) return launch_batched<16, false, float2>(bp, queue, st);
-    return launch_batched<32, false, float2>(bp, queue, st);
+    if (tile_shape == 0) return launch_batched<8, false, float2>(bp, acc_bytes, queue, st);
+    if (tile_shape == 1) return launch_batched<16, false, float2>(bp, acc_bytes, queue, st);
+    return launch_batched<32, false, float2>(bp, acc_bytes, queue, st);
 }
 
 }  // namespace tt

@@ -126,7 +126,7 @@ __global__ void insert_finalize_bricked_kernel(const float4* __restrict__ acc, f
         }
         const int64_t o = ((int64_t)z * g.H + y) * g.W + x;
         vol[o] = make_float2(re, im);
-        wts[o] = wt;
+        if (wts) wts[o] = wt;
     }
 }
 
@@ -363,6 +363,36 @@ extern "C" int tt_insert_accumulate(const void* image_rfft, int32_t complex128, 
     if (!image_rfft || !rotation_matrices || !accumulator)
         return fail(TT_ERR_INVALID, "insert_accumulate: NULL pointer argument");
     return launch_insert_accumulate(image_rfft, complex128, rotation_matrices, accumulator, p, as_stream(stream));
+}
+
+// The batched insertion's policy: bricked from 64 MB of accumulator while the
+// accumulator fits one z-phase.  Measured on a B200 (batched launch, CTF,
+// best tile shape): 256^3 x 4096 3.77 vs 3.84 ms, 200^3 2.38 vs 2.37 ms (below
+// 64 MB), 320^3 x 10000 (two z-phases) 16.1 vs 15.0 ms.
+extern "C" int32_t tt_insert_accumulator_layout(const tt_slice_params* p) {
+    if (!p || p->deterministic || !insert_bricked(p)) return TT_VOLUME_PLAIN;
+    return insert_phases(bricked_accumulator_bytes(p)) == 1 ? TT_VOLUME_BRICKS : TT_VOLUME_PLAIN;
+}
+
+extern "C" size_t tt_insert_bricked_accumulator_bytes(int64_t d, int64_t h, int64_t w_rfft) {
+    if (d < 1 || h < 1 || w_rfft < 1) return 0;
+    return (size_t)(((d + 1) / 2) * ((h + 1) / 2) * ((w_rfft + 1) / 2)) * 8 * sizeof(float4);
+}
+
+extern "C" int tt_insert_finalize_bricked(const void* accumulator, int64_t d, int64_t h, int64_t w_rfft,
+                                          void* volume_rfft, void* weights, void* stream) {
+    if (!accumulator || !volume_rfft) return fail(TT_ERR_INVALID, "insert_finalize_bricked: NULL pointer argument");
+    if (d < 1 || h < 1 || w_rfft < 1 || d > 0x7fffffff || h > 0x7fffffff || w_rfft > 0x7fffffff)
+        return fail(TT_ERR_INVALID, "insert_finalize_bricked: bad dims");
+    const int64_t rows = ((d + 1) / 2) * ((h + 1) / 2);
+    if (rows > 0x7fffffffLL) return fail(TT_ERR_INVALID, "insert_finalize_bricked: too many brick rows");
+    SliceGeom g{};  // the finalize reads only the volume dims
+    g.D = (int)d;
+    g.H = (int)h;
+    g.W = (int)w_rfft;
+    insert_finalize_bricked_kernel<<<(unsigned)rows, 256, 0, as_stream(stream)>>>(
+        (const float4*)accumulator, (float2*)volume_rfft, (float*)weights, g);
+    return check_launch("insert_finalize_bricked_kernel");
 }
 
 extern "C" int tt_insert_finalize(const void* accumulator, int32_t complex128, int64_t channels, int64_t d, int64_t h,

@@ -173,15 +173,47 @@ def test_batched_validation_and_layout():
     bad = (_lib.BatchVolume * 1)(_lib.BatchVolume(_params(vol_w=8), None, fake, fake, fake, None))
     assert L.tt_insert_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
     assert L.tt_extract_central_slices_rfft_3d_batched(bad, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
-    # layouts: the extraction takes plain or bricked volumes, one layout per call; the insertion plain only
+    # layouts: the extraction takes plain or bricked volumes, one layout per call; the insertion plain
+    # or bricked accumulators (fftshifted volumes), mixed in one call
     xp = (_lib.BatchVolume * 1)(_lib.BatchVolume(_params(volume_layout=1), fake, fake, fake, fake, None))
     assert L.tt_extract_central_slices_rfft_3d_batched(xp, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
     assert b"plain or bricked" in L.tt_last_error()
+    assert L.tt_insert_central_slices_rfft_3d_batched(xp, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+    assert b"bricked" in L.tt_last_error()
+    unshifted = (_lib.BatchVolume * 1)(_lib.BatchVolume(_params(volume_layout=2, volume_unshifted=1), fake, fake,
+                                                        fake, fake, None))
+    assert L.tt_insert_central_slices_rfft_3d_batched(unshifted, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
     mixed = (_lib.BatchVolume * 2)(_lib.BatchVolume(_params(volume_layout=2), fake, fake, fake, fake, None),
                                    _lib.BatchVolume(_params(), fake, fake, fake, fake, None))
     assert L.tt_extract_central_slices_rfft_3d_batched(mixed, 2, 0, fake, 256, None) == _lib.TT_ERR_INVALID
     assert b"one volume_layout" in L.tt_last_error()
-    assert L.tt_insert_central_slices_rfft_3d_batched(mixed, 1, 0, fake, 256, None) == _lib.TT_ERR_INVALID
+    # accepted: with no CUDA device visible it fails on the first CUDA call, not in validation
+    assert L.tt_insert_central_slices_rfft_3d_batched(mixed, 2, 0, fake, 256, None) not in (_lib.TT_OK,
+                                                                                          _lib.TT_ERR_INVALID)
+    assert b"memset" in L.tt_last_error()
+
+
+def test_bricked_insert_accumulator_policy():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    # plain below 64 MB of bricked accumulator, bricked from there up (fftshifted, float) while the
+    # accumulator fits one z-phase of the L2 (a B200's 126 MB: 256^3 does, 320^3 does not; with no
+    # device to ask, one phase is assumed)
+    import torch
+
+    phased = 0 if torch.cuda.is_available() else 2
+    for n, want in ((64, 0), (128, 0), (200, 0), (216, 2), (256, 2), (320, phased)):
+        p = _params(img_d=n, img_h=n, img_w=n, vol_d=n, vol_h=n, vol_w=n // 2 + 1)
+        assert L.tt_insert_accumulator_layout(ctypes.byref(p)) == want, n
+        assert L.tt_insert_bricked_accumulator_bytes(n, n, n // 2 + 1) == (
+            ((n + 1) // 2) * ((n + 1) // 2) * ((n // 2 + 2) // 2) * 8 * 16)
+        p.volume_unshifted = 1
+        assert L.tt_insert_accumulator_layout(ctypes.byref(p)) == 0
+        p.volume_unshifted, p.deterministic = 0, 1
+        assert L.tt_insert_accumulator_layout(ctypes.byref(p)) == 0
+    assert L.tt_insert_bricked_accumulator_bytes(0, 4, 4) == 0
+    assert L.tt_insert_finalize_bricked(None, 4, 4, 3, None, None, None) == _lib.TT_ERR_INVALID
 
 
 @pytest.mark.fake_pointers

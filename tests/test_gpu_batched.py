@@ -3,6 +3,8 @@ persistent launch), its CUDA-graph plan and the tile-shape autotuner."""
 
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -106,6 +108,41 @@ def test_batched_insert_with_ctf(oracle):
         ctf = np.stack([oracle.ctf_2d(*cc[j], image_shape=(n, n)) for j in range(len(cc))])
         rv, _ = oracle.insert((im.cpu().numpy() * ctf).astype(np.complex64), (n, n, n), R.cpu().numpy())
         rw, _ = oracle.insert((ctf * ctf).astype(np.complex64), (n, n, n), R.cpu().numpy())
+        assert rel_l2(vol.cpu().numpy(), rv) < 1e-4, n
+        assert rel_l2(w.cpu().numpy(), rw.real) < 1e-4, n
+
+
+def test_batched_insert_bricked_accumulators(oracle):
+    """Volumes with 64 MB of accumulator and more go to bricked accumulators
+    (lane-octet splat, bricked finalize), the small ones stay plain, in one
+    launch: each against the one-shot single-volume insertion (also bricked
+    from that size) and, with a CTF, against the oracle's insertions of
+    ctf * image and ctf^2."""
+    from teamtomo_b200 import _lib
+    from teamtomo_b200.torch_fourier_slice._params import rfft_shape, slice_params
+
+    L = _lib.load()
+    boxes, counts = [216, 48, 230], [40, 30, 25]
+    vols = [cuda(rfft_volume_np(blob_volume(b, seed=b, n_blobs=8))) for b in boxes]
+    rots = [cuda(rotations(k, seed=b + k)).float() for b, k in zip(boxes, counts)]
+    layouts = [L.tt_insert_accumulator_layout(ctypes.byref(slice_params(
+        n=k, image_shape=(b, b, b), volume=None, rotation=R, vol_dims=rfft_shape((b, b, b)))))
+        for b, k, R in zip(boxes, counts, rots)]
+    assert layouts == [2, 0, 2]
+    imgs = [tt().extract_central_slices_rfft_3d(v, (n, n, n), R) for n, v, R in zip(boxes, vols, rots)]
+    for n, im, R, (vol, w) in zip(boxes, imgs, rots, B().insert_central_slices_rfft_3d_batched(imgs, rots)):
+        v1, w1 = tt().insert_central_slices_rfft_3d(im, (n, n, n), R)
+        assert rel_l2(vol.cpu().numpy(), v1.cpu().numpy()) < 1e-6, n
+        assert rel_l2(w.cpu().numpy(), w1.cpu().numpy()) < 1e-6, n
+        assert torch.equal(w != 0, w1 != 0), n
+    ctfs = [B().ctf_params(np.linspace(0.8, 2.5, k), n=k, device="cuda") for k in counts]
+    outs = B().insert_central_slices_rfft_3d_batched(imgs, rots, ctf=ctfs)
+    for n, im, R, c, (vol, w) in zip(boxes, imgs, rots, ctfs, outs):
+        cc = c.cpu().numpy()
+        ctf = np.stack([oracle.ctf_2d(*cc[j], image_shape=(n, n)) for j in range(len(cc))])
+        rv, _ = oracle.insert((im.cpu().numpy() * ctf).astype(np.complex64), (n, n, n), R.cpu().numpy(),
+                              nthreads=8)
+        rw, _ = oracle.insert((ctf * ctf).astype(np.complex64), (n, n, n), R.cpu().numpy(), nthreads=8)
         assert rel_l2(vol.cpu().numpy(), rv) < 1e-4, n
         assert rel_l2(w.cpu().numpy(), rw.real) < 1e-4, n
 
