@@ -147,6 +147,34 @@ def test_batched_insert_bricked_accumulators(oracle):
         assert rel_l2(w.cpu().numpy(), rw.real) < 1e-4, n
 
 
+def test_bricked_finalize_without_weights():
+    """tt_insert_finalize_bricked with weights NULL writes the same volume."""
+    from teamtomo_b200 import _lib
+    from teamtomo_b200.torch_fourier_slice._params import rfft_shape, slice_params
+
+    L = _lib.load()
+    n, k = 216, 12
+    shape = (n, n, n)
+    d, h, w = rfft_shape(shape)
+    R = cuda(rotations(k, seed=5)).float()
+    img = tt().extract_central_slices_rfft_3d(cuda(rfft_volume_np(blob_volume(n, seed=3, n_blobs=6))), shape, R)
+    p = slice_params(n=k, image_shape=shape, volume=None, rotation=R, vol_dims=(d, h, w))
+    p.volume_layout = 2
+    acc = torch.zeros(int(L.tt_insert_bricked_accumulator_bytes(d, h, w)) // 4, dtype=torch.float32, device="cuda")
+    ws = torch.empty(int(L.tt_batch_workspace_bytes()), dtype=torch.uint8, device="cuda")
+    arr = (_lib.BatchVolume * 1)(_lib.BatchVolume(p, None, img.data_ptr(), acc.data_ptr(), R.data_ptr(), None))
+    st = _lib.stream_of(torch.device("cuda"))
+    assert L.tt_insert_central_slices_rfft_3d_batched(arr, 1, 0, _lib.ptr(ws), ws.numel(), st) == 0
+    v1 = torch.empty((d, h, w), dtype=torch.complex64, device="cuda")
+    v2 = torch.empty_like(v1)
+    wt = torch.empty((d, h, w), dtype=torch.float32, device="cuda")
+    assert L.tt_insert_finalize_bricked(_lib.ptr(acc), d, h, w, _lib.ptr(v1), _lib.ptr(wt), st) == 0
+    assert L.tt_insert_finalize_bricked(_lib.ptr(acc), d, h, w, _lib.ptr(v2), None, st) == 0
+    assert torch.equal(v1, v2)
+    v0, w0 = tt().insert_central_slices_rfft_3d(img, shape, R)
+    assert rel_l2(v1.cpu().numpy(), v0.cpu().numpy()) < 1e-6 and rel_l2(wt.cpu().numpy(), w0.cpu().numpy()) < 1e-6
+
+
 def test_batched_chunks_beyond_one_launch():
     """More volumes than one launch carries (96) are split into launches."""
     vols = [cuda(rfft_volume_np(blob_volume(8, seed=s, n_blobs=2))) for s in range(100)]
