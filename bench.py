@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--torch-gpu-sample", type=int, default=512, help="slices timed on the reference's torch path")
     ap.add_argument("--e2e-chunk", type=int, default=256, help="slices per streamed chunk in the e2e leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-probe", action="store_true", help="skip the L2 reduction-rate probe")
     ap.add_argument("--cpu-sample", type=int, default=1024, help="slices of the oracle-port CPU sample")
     ap.add_argument("--ref-cpu-sample", type=int, default=32,
                     help="slices of the reference-torch-on-CPU sample (cpu_baseline)")
@@ -452,6 +453,52 @@ def torch_gpu_reference(dev, n, V0, R0, T, sample, chunk=128):
             "sample": f"{sample} of the 4096 slices, chunks of {chunk}, volume without grad",
             "excluded": "d/dvolume (the reference's autograd expands the volume per sample)",
             "code": "reference torch_fourier_slice, unmodified, CUDA tensors"}
+
+
+def l2_reduction_ceiling(dev, n, R, insert_ms, reps=3):
+    """The insertion's trilinear-corner reductions per second beside the L2's
+    float4 reduction rate (tt_probe_l2_reductions) for the same number of
+    reductions: eight lanes per 128-byte line on random lines of a buffer of
+    the insertion accumulator's size and of one that fits the L2 (32 MB), and
+    two lanes per line (the x-paired rows' pattern) on the accumulator-sized
+    buffer.  The corner count is exact: every kept source pixel whose point
+    lies inside the volume adds its corners of non-zero weight (an axis whose
+    coordinate is an integer has one).  Outside the timed region."""
+    import ctypes
+
+    import torch
+
+    from teamtomo_b200 import _lib
+    from teamtomo_b200.torch_fourier_slice import slice_extraction as se
+    from teamtomo_b200.torch_fourier_slice._params import rfft_shape, slice_params
+
+    L = _lib.load()
+    shape = (n, n, n)
+    dims = rfft_shape(shape)
+    count = 0
+    for i in range(0, R.shape[0], 256):
+        flags, c = se.central_slice_geometry(R[i:i + 256], shape, dims, mode="insert")
+        ok = ((flags & 1) != 0) & ((flags & 4) != 0)
+        corners = (1 + (c != torch.floor(c)).to(torch.int64)).prod(dim=-1)
+        count += int((corners * ok).sum().item())
+        del flags, c
+    p = slice_params(n=R.shape[0], image_shape=shape, volume=None, rotation=R, vol_dims=dims)
+    acc_bytes = int(L.tt_insert_workspace_bytes(0, ctypes.byref(p)))
+    st = _lib.stream_of(dev)
+    out = {"insert_corner_reductions": count,
+           "insert_g_per_s": round(count / (insert_ms / 1e3) / 1e9, 1), "probe_g_per_s": {}}
+    for label, nbytes, lanes in ((f"8 lanes/line, {acc_bytes >> 20} MiB", acc_bytes, 8),
+                                 ("8 lanes/line, 32 MiB", 32 << 20, 8),
+                                 (f"2 lanes/line, {acc_bytes >> 20} MiB", acc_bytes, 2)):
+        buf = torch.zeros(nbytes // 4, dtype=torch.float32, device=dev)
+        run = lambda: _lib.check(L.tt_probe_l2_reductions(_lib.ptr(buf), nbytes, count, lanes, 1234, st),  # noqa
+                                 "probe_l2_reductions")
+        ms = _time_device(run, reps, 1, dev)
+        out["probe_g_per_s"][label] = round(count / (ms / 1e3) / 1e9, 1)
+        del buf
+    first = next(iter(out["probe_g_per_s"].values()))
+    out["insert_over_probe_8_lanes_same_size"] = round(out["insert_g_per_s"] / first, 3)
+    return out
 
 
 def load_peaks():
@@ -1305,6 +1352,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_baseline(n, args.ref_cpu_sample, args.cpu_sample)
 
+    reductions = None
+    if rank == 0 and world == 1 and not det and not args.no_probe:
+        reductions = l2_reduction_ceiling(dev, n, R0, kernels["insert"]["ms"])
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -1316,7 +1367,7 @@ def main():
                                                       if world > 1 else ""),
                        "deterministic": det},
             "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "fused_mse": fused, "torch_gpu_reference": torch_gpu,
+            "fused_mse": fused, "torch_gpu_reference": torch_gpu, "l2_reductions": reductions,
             # extract (+ the pack of the bricked volume copy it gathers from), backward,
             # rotation-gradient finish, insert splat, insert finalize (+ absmax
             # pre-passes and the fixed-point add-back when deterministic)

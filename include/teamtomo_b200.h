@@ -426,6 +426,17 @@ int tt_insert_central_slices_rfft_3d_batched(const tt_batch_volume *volumes, int
                                              int32_t tile_shape, void *workspace,
                                              size_t workspace_bytes, void *stream);
 
+/* ---- measurement probe ------------------------------------------------
+ * `reductions` float4 additions into `buffer` (`bytes`: a positive multiple
+ * of 128, 128-byte aligned) in groups of `lanes_per_line` (1, 2, 4 or 8)
+ * lanes of a warp on adjacent 16-byte slots of one 128-byte line, each
+ * group's line drawn by a hash of its index and `seed`: the L2's float4
+ * reduction rate for a scatter over a buffer of that size, the ceiling the
+ * insertion splat is measured against.  The buffer's contents are
+ * incremented (no other meaning).  No counterpart in the reference. */
+int tt_probe_l2_reductions(void *buffer, size_t bytes, int64_t reductions, int32_t lanes_per_line,
+                           uint64_t seed, void *stream);
+
 /* ---- generic 3D interpolation (torch_image_interpolation) -------------
  * dtype codes: 0 float32, 1 float64, 2 complex64, 3 complex128.  Images are
  * (channels, d, h, w) of that dtype. */

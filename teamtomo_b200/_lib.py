@@ -84,6 +84,7 @@ SIGNATURES = {
     "tt_insert_accumulator_layout": ([ctypes.POINTER(SliceParams)], _i32),
     "tt_insert_bricked_accumulator_bytes": ([_i64, _i64, _i64], _sz),
     "tt_insert_finalize_bricked": ([_vp, _i64, _i64, _i64, _vp, _vp, _vp], _i32),
+    "tt_probe_l2_reductions": ([_vp, _sz, _i64, _i32, ctypes.c_uint64, _vp], _i32),
     "tt_friedel_mirror_x0": ([_vp, _vp, _i32, _i64, _i64, _i64, _i64, _vp], _i32),
     "tt_insert_workspace_bytes": ([_i32, ctypes.POINTER(SliceParams)], _sz),
     "tt_fixed_absmax": ([_vp, _i32, _i64, _vp, _vp], _i32),

@@ -193,6 +193,20 @@ def test_batched_validation_and_layout():
     assert b"memset" in L.tt_last_error()
 
 
+@pytest.mark.fake_pointers
+def test_probe_validation():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    fake = ctypes.c_void_p(1 << 20)
+    assert L.tt_probe_l2_reductions(None, 1 << 20, 8, 8, 0, None) == _lib.TT_ERR_INVALID
+    assert L.tt_probe_l2_reductions(ctypes.c_void_p((1 << 20) + 16), 1 << 20, 8, 8, 0, None) == _lib.TT_ERR_INVALID
+    assert L.tt_probe_l2_reductions(fake, 1000, 8, 8, 0, None) == _lib.TT_ERR_INVALID
+    assert L.tt_probe_l2_reductions(fake, 1 << 20, 8, 3, 0, None) == _lib.TT_ERR_INVALID
+    assert L.tt_probe_l2_reductions(fake, 1 << 20, -1, 8, 0, None) == _lib.TT_ERR_INVALID
+    assert L.tt_probe_l2_reductions(fake, 1 << 20, 4, 8, 0, None) == _lib.TT_OK  # fewer than one group
+
+
 def test_bricked_insert_accumulator_policy():
     from teamtomo_b200 import _lib
 

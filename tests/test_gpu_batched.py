@@ -244,3 +244,18 @@ def test_batched_extraction_from_bricked_copies_is_bitwise_plain():
         assert torch.equal(a, b)
     with pytest.raises(ValueError):
         B().extract_central_slices_rfft_3d_batched(vols, rots, volume_layout="xpairs")
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8])
+def test_l2_reduction_probe_adds_every_reduction(lanes):
+    """The probe's reductions all land in the buffer: the x components sum to
+    the count (whole groups), the fourth components stay zero."""
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    nbytes, count = 1 << 20, (1 << 18) + 5
+    buf = torch.zeros(nbytes // 4, dtype=torch.float32, device="cuda")
+    assert L.tt_probe_l2_reductions(_lib.ptr(buf), nbytes, count, lanes, 7, _lib.stream_of(buf.device)) == 0
+    q = buf.view(-1, 4).double()
+    assert q[:, 0].sum().item() == (count // lanes) * lanes
+    assert torch.equal(q[:, 0], q[:, 1]) and torch.equal(q[:, 0], q[:, 2]) and q[:, 3].abs().sum().item() == 0
