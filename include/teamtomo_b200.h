@@ -428,7 +428,7 @@ int tt_insert_central_slices_rfft_3d_batched(const tt_batch_volume *volumes, int
 
 /* ---- measurement probe ------------------------------------------------
  * `reductions` float4 additions into `buffer` (`bytes`: a positive multiple
- * of 128, 128-byte aligned) in groups of `lanes_per_line` (1, 2, 4 or 8)
+ * of 128 below 512 GiB, 128-byte aligned) in groups of `lanes_per_line` (1, 2, 4 or 8)
  * lanes of a warp on adjacent 16-byte slots of one 128-byte line, each
  * group's line drawn by a hash of its index and `seed`: the L2's float4
  * reduction rate for a scatter over a buffer of that size, the ceiling the

@@ -36,7 +36,10 @@ __global__ void __launch_bounds__(256) l2_reduction_probe_kernel(float4* __restr
     for (long long w = warp; w * per_warp < groups; w += warps) {
         const long long gi = w * per_warp + lane / lanes;
         if (gi < groups) {
-            const unsigned long long line = probe_mix((unsigned long long)gi ^ seed) % lines;
+            // multiply-shift range reduction of the hash's high word (no 64-bit division:
+            // the probe must not be bound by its own index arithmetic)
+            const unsigned long long h = probe_mix((unsigned long long)gi ^ seed) >> 32;
+            const unsigned long long line = (h * lines) >> 32;
             atomicAdd(buf + line * 8 + (lane % lanes), make_float4(1.0f, 1.0f, 1.0f, 0.0f));
         }
     }
@@ -51,8 +54,8 @@ extern "C" int tt_probe_l2_reductions(void* buffer, size_t bytes, int64_t reduct
     if (!buffer) return fail(TT_ERR_INVALID, "probe_l2_reductions: NULL buffer");
     if ((reinterpret_cast<uintptr_t>(buffer) & 127) != 0)
         return fail(TT_ERR_INVALID, "probe_l2_reductions: the buffer must be 128-byte aligned");
-    if (bytes < 128 || bytes % 128 != 0)
-        return fail(TT_ERR_INVALID, "probe_l2_reductions: bytes must be a positive multiple of 128");
+    if (bytes < 128 || bytes % 128 != 0 || bytes / 128 > 0xffffffffULL)
+        return fail(TT_ERR_INVALID, "probe_l2_reductions: bytes must be a positive multiple of 128 below 512 GiB");
     if (lanes_per_line != 1 && lanes_per_line != 2 && lanes_per_line != 4 && lanes_per_line != 8)
         return fail(TT_ERR_INVALID, "probe_l2_reductions: lanes_per_line must be 1, 2, 4 or 8");
     if (reductions < 0) return fail(TT_ERR_INVALID, "probe_l2_reductions: negative count");
