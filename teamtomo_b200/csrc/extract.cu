@@ -96,17 +96,20 @@ __device__ __forceinline__ void bwd_point(const VT* __restrict__ vol, const floa
         gv = __ldcs(grad + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr + ix);
         if (cj) gv.y = -gv.y;  // G' = conj(G) where the sample was conjugated
     }
+    // the rotation gradient first: its corner values are dead before the
+    // scatter's shuffles and reductions, which then run without spills
+    // (256^3 x 4096: 3.21 vs 3.52 ms with the scatter first)
+    if (WANT_DR && valid) {
+        float2 v[2][2][2];
+        load_corners(vol, g, k, v);
+        drot_terms(v, k, gv, cj, g, qy, qx, acc);
+    }
     if (WANT_DV) {
         if (FIXED) {
             scatter_dv_fixed_paired(dv.fixed, dv.scale, g, si, gv, valid);
         } else {
             scatter_dv_paired(dv.dvol, g, si, gv, valid);
         }
-    }
-    if (WANT_DR && valid) {
-        float2 v[2][2][2];
-        load_corners(vol, g, k, v);
-        drot_terms(v, k, gv, cj, g, qy, qx, acc);
     }
 }
 
