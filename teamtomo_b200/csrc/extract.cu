@@ -229,8 +229,10 @@ extract_bwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
 // of tiles).  The row's partials of the loss (double) go to
 // loss_part[s * rows + row] and, with WANT_DR, those of d/dR_zyx to
 // part[(s * rows + row) * 6 + k]: one slot per row of tiles.
+// Five resident blocks (48 registers); four for the rotation gradient alone,
+// which spills at 48 (256^3 x 4096: 1.95 vs 2.19 ms at five).
 template <bool WANT_DV, bool WANT_DR, typename VT>
-__global__ void __launch_bounds__(kExtractThreads, 5)
+__global__ void __launch_bounds__(kExtractThreads, (WANT_DR && !WANT_DV) ? 4 : 5)
 slice_mse_kernel(const VT* __restrict__ vol, const void* __restrict__ rot, const float2* __restrict__ target,
                  float2* __restrict__ dvol, float* __restrict__ part, double* __restrict__ loss_part, float scale,
                  SliceGeom g, int tiles) {
