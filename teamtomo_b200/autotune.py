@@ -77,10 +77,11 @@ def tune(kind: str, box: int, n_slices: int = 512, device=None, repeats: int = 5
     from . import batched
 
     dev = torch.device(device or "cuda")
-    if kind == "extract":
-        # the bricked layout packs each volume once per call: time it where the
-        # pack is amortised as in use (four slice pixels per voxel or more)
-        n_slices = max(n_slices, 4 * box)
+    # time the kernels where the per-call work (the bricked layout's pack, the
+    # insertion's accumulator zeroing and finalize) is amortised as in use:
+    # four slice pixels per voxel or more (with 256 slices of a 256^3 box the
+    # insertion's fixed costs hid a 3 % difference between tile shapes)
+    n_slices = max(n_slices, 4 * box)
     g = torch.Generator(device=dev).manual_seed(box)
     shape3 = (box, box, box // 2 + 1)
     R = torch.linalg.qr(torch.randn((n_slices, 3, 3), device=dev, generator=g))[0].contiguous()

@@ -55,8 +55,9 @@ __host__ inline int tiles_t(int img_h, int wr) {
 }
 
 // The extraction instantiations keep six blocks resident (40 registers, no
-// spills; left free the compiler takes 55 and four blocks): 389K CTF slices
-// of 32 volumes in 63.8 vs 72.8 ms.  The insertion's take five (48).
+// spills): 389K CTF slices of 32 volumes in 63.9 / 71.7 ms (8 x 32 / 16 x 16
+// tiles) against 65.8 / 74.7 ms at five (47 registers) and 72.8 / 83.1 ms at
+// four.  The insertion's keep five (44 registers; equal times).
 template <int TX, bool INSERT, typename VT>
 __global__ void __launch_bounds__(256, INSERT ? 5 : 6)
 batched_slices_kernel(const __grid_constant__ BatchParams bp, unsigned long long* __restrict__ queue,
