@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <type_traits>
 
 #include "capi_util.cuh"
 #include "fixed_point.cuh"
@@ -41,8 +42,11 @@ __device__ __forceinline__ void load_rotation(float* sm, const void* rot, int64_
 // One block per (slice, row of tiles), eight resident blocks (32 registers):
 // the gathers are latency-bound at six (64 % warps active); full occupancy
 // takes 8.5 % off the launch, the row loop another 1 %.
-template <typename VT>
-__global__ void __launch_bounds__(kExtractThreads, 8)
+// From the bricked copy the row of tiles is unrolled by four at six resident
+// blocks (40 registers), so one thread's gathers of neighbouring tiles
+// overlap: 256^3 x 4096 1.30 vs 1.32-1.35 ms, 128^3 0.386 vs 0.394 ms.
+template <typename VT, int UNR = std::is_same<VT, VoxBrick2>::value ? 4 : 1>
+__global__ void __launch_bounds__(kExtractThreads, UNR > 1 ? 6 : 8)
 extract_fwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
                    float2* __restrict__ out, SliceGeom g, int tiles) {
     __shared__ float m[9];
@@ -58,6 +62,7 @@ extract_fwd_kernel(const VT* __restrict__ vol, const void* __restrict__ rot,
     if (iy >= g.img_h) return;
     const SliceRow row = slice_row_geom(g, m, iy);
     float2* orow = out + (s * g.img_h + slice_row(g, iy)) * (int64_t)g.wr;
+#pragma unroll UNR
     for (int tx = 0; tx < tx_tiles; tx++) {
         const int ix = tx * kTileX + (lane & 7);
         if (ix >= g.wr) continue;
