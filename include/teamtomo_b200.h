@@ -236,6 +236,10 @@ int tt_insert_central_slices_rfft_3d(const void *image_rfft, int32_t complex128,
  * gathered; conjugated where the point was redirected; zero for dropped
  * pixels) and of the Friedel completion of the x=0 plane.  The weights output
  * does not depend on the slices, so its gradient contributes nothing.
+ * complex64 with p->volume_layout = TT_VOLUME_BRICKS: grad_volume is the
+ * bricked copy of an fftshifted gradient volume (tt_pack_volume_bricks); the
+ * gathers then read fewer lines (256^3 x 4096: 1.23 vs 1.76 ms), results
+ * bit-identical.
  * Replaces the autograd graph of insert_central_slices_rfft_3d w.r.t. image_rfft
  * (index_put_ backward of _insert_central_slices_rfft_3d.py:213-406). */
 int tt_insert_central_slices_rfft_3d_backward(const void *grad_volume, int32_t complex128,

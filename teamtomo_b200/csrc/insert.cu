@@ -191,8 +191,8 @@ __global__ void mirror_x0_kernel(typename Acc<R>::C* __restrict__ vol, R* __rest
 // One thread per slice pixel, one block per row of tiles (the row part of the
 // geometry formed once per thread); every pixel is written (zero when
 // dropped).  float: eight resident blocks (32 registers) for the gathers.
-template <typename R>
-__global__ void __launch_bounds__(kTileThreads, sizeof(R) == 4 ? 8 : 1)
+template <typename R, bool BRICKED = false>
+__global__ void __launch_bounds__(kTileThreads, sizeof(R) == 4 ? (BRICKED ? 6 : 8) : 1)
 insert_bwd_kernel(const typename Acc<R>::C* __restrict__ gvol, const void* __restrict__ rot,
                   typename Acc<R>::C* __restrict__ gimg, SliceGeom g, int tiles) {
     __shared__ float m[9];
@@ -222,15 +222,52 @@ insert_bwd_kernel(const typename Acc<R>::C* __restrict__ gvol, const void* __res
         if (kept && insert_coords_row(g, m, row, qx, cj, c)) {
             InsertCell k;
             cell_at(c, k);
+            if constexpr (BRICKED) {
+                // the x-rows of the cell from the bricked copy (corner addressed
+                // once, neighbours by parity steps); corners of zero weight are
+                // not read; same corner order, weights and sums as below
+                Corners kk{};
+                kk.z0 = k.iz0;
+                kk.y0 = k.iy0;
+                kk.x0 = k.ix0;
+                const XRows<VoxBrick2> xr(reinterpret_cast<const VoxBrick2*>(gvol), g, kk);
+                const bool hx = k.tx != 0.0f;
 #pragma unroll
-            for (int corner = 0; corner < 8; corner++) {
-                const float w = insert_corner_weight(k, corner);
-                if (w == 0.0f) continue;
-                int z, y, x;
-                insert_corner_zyx(k, corner, z, y, x);
-                const typename Acc<R>::C gv = completed_grad<R>(gvol, g, z, y, x);
-                out.x += (R)w * gv.x;
-                out.y += (R)w * gv.y;
+                for (int bz = 0; bz < 2; bz++) {
+                    if (bz && k.tz == 0.0f) continue;
+#pragma unroll
+                    for (int by = 0; by < 2; by++) {
+                        if (by && k.ty == 0.0f) continue;
+                        float2 v0, v1;
+                        xr.load(g, bz, by, true, hx, v0, v1);
+                        const int z = bz ? k.iz1 : k.iz0, y = by ? k.iy1 : k.iy0;
+                        if (k.ix0 == 0 && !(z == g.D / 2 && y == g.H / 2)) {
+                            const float2 b = gvol[accumulator_slot(g, (g.D - z) % g.D, (g.H - y) % g.H, 0)];
+                            v0.x += b.x;
+                            v0.y -= b.y;
+                        }
+                        const float fzy = (bz ? k.tz : 1.0f - k.tz) * (by ? k.ty : 1.0f - k.ty);
+                        const float w0 = fzy * (1.0f - k.tx);
+                        out.x += w0 * v0.x;
+                        out.y += w0 * v0.y;
+                        if (hx) {
+                            const float w1 = fzy * k.tx;
+                            out.x += w1 * v1.x;
+                            out.y += w1 * v1.y;
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int corner = 0; corner < 8; corner++) {
+                    const float w = insert_corner_weight(k, corner);
+                    if (w == 0.0f) continue;
+                    int z, y, x;
+                    insert_corner_zyx(k, corner, z, y, x);
+                    const typename Acc<R>::C gv = completed_grad<R>(gvol, g, z, y, x);
+                    out.x += (R)w * gv.x;
+                    out.y += (R)w * gv.y;
+                }
             }
             if (cj) out.y = -out.y;
         }
@@ -444,7 +481,17 @@ extern "C" int tt_insert_central_slices_rfft_3d(const void* image_rfft, int32_t 
 extern "C" int tt_insert_central_slices_rfft_3d_backward(const void* grad_volume, int32_t complex128,
                                                          const void* rotation_matrices, void* grad_image,
                                                          const tt_slice_params* p, void* stream) {
-    if (int e = check_insert_params(p)) return e;
+    if (!p) return fail(TT_ERR_INVALID, "insert backward: NULL params");
+    // grad_volume plain, or (complex64, fftshifted) its bricked copy (tt_pack_volume_bricks)
+    const bool bricked = p->volume_layout == TT_VOLUME_BRICKS;
+    if (bricked && (complex128 || p->volume_unshifted))
+        return fail(TT_ERR_INVALID, "insert backward: a bricked gradient volume is complex64 and fftshifted");
+    if (p->volume_layout == TT_VOLUME_XPAIRS)
+        return fail(TT_ERR_INVALID, "insert backward: the gradient volume is plain or bricked");
+    if (int e = validate_params(p, true)) return e;
+    if (p->vol_d != p->img_d || p->vol_h != p->img_h || p->vol_w != p->img_w / 2 + 1)
+        return fail(TT_ERR_INVALID, "insert: volume dims (%lld, %lld, %lld) are not the rfft of volume_shape",
+                    (long long)p->vol_d, (long long)p->vol_h, (long long)p->vol_w);
     if (p->n == 0) return TT_OK;
     if (!grad_volume || !rotation_matrices || !grad_image)
         return fail(TT_ERR_INVALID, "insert backward: NULL pointer argument");
@@ -457,6 +504,9 @@ extern "C" int tt_insert_central_slices_rfft_3d_backward(const void* grad_volume
         insert_bwd_kernel<double><<<(unsigned)items, kTileThreads, 0, st>>>((const double2*)grad_volume,
                                                                            rotation_matrices, (double2*)grad_image,
                                                                            g, tiles);
+    else if (bricked)
+        insert_bwd_kernel<float, true><<<(unsigned)items, kTileThreads, 0, st>>>(
+            (const float2*)grad_volume, rotation_matrices, (float2*)grad_image, g, tiles);
     else
         insert_bwd_kernel<float><<<(unsigned)items, kTileThreads, 0, st>>>((const float2*)grad_volume,
                                                                           rotation_matrices, (float2*)grad_image, g,

@@ -25,6 +25,7 @@ import math
 import torch
 
 from .. import _lib
+from . import _layout
 from ._params import resolve_deterministic, rfft_shape, rotation_arg, slice_params
 
 
@@ -205,8 +206,16 @@ def insert_backward(grad_volume, R, volume_shape, fftfreq_max=None, zyx_matrices
     params = slice_params(n=R.shape[0], image_shape=volume_shape, volume=None, rotation=R,
                           fftfreq_max=fftfreq_max, zyx_matrices=zyx_matrices,
                           slices_unshifted=images_unshifted, vol_dims=(d, h, w))
+    # from half a slice pixel per voxel the gathers read a bricked copy of the
+    # gradient volume (the extraction's layout policy; bit-identical results)
+    src = grad_volume
+    if not c128 and grad_volume.ndim == 3:
+        layout = _layout.choose(R.shape[0] * h * w, grad_volume)
+        if layout == _layout.BRICKS:
+            params = _layout.with_layout(params, layout)
+            src = _layout.pack(grad_volume, params, layout)
     L = _lib.load()
-    _lib.check(L.tt_insert_central_slices_rfft_3d_backward(_lib.ptr(grad_volume), int(c128), _lib.ptr(R),
+    _lib.check(L.tt_insert_central_slices_rfft_3d_backward(_lib.ptr(src), int(c128), _lib.ptr(R),
                                                            _lib.ptr(out), params, _lib.stream_of(dev)),
                "insert_central_slices_rfft_3d backward")
     return out

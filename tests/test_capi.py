@@ -194,6 +194,25 @@ def test_batched_validation_and_layout():
 
 
 @pytest.mark.fake_pointers
+def test_insert_backward_gradient_layouts():
+    from teamtomo_b200 import _lib
+
+    L = _lib.load()
+    fake = ctypes.c_void_p(16)
+    # the gradient volume is plain or, complex64 and fftshifted, its bricked copy; never x-paired
+    for kw, c128 in ((dict(volume_layout=1), 0), (dict(volume_layout=2), 1),
+                     (dict(volume_layout=2, volume_unshifted=1), 0), (dict(volume_layout=3), 0)):
+        p = _params(**kw)
+        assert L.tt_insert_central_slices_rfft_3d_backward(fake, c128, fake, fake, ctypes.byref(p),
+                                                           None) == _lib.TT_ERR_INVALID, kw
+    p = _params(volume_layout=2, vol_w=8)
+    assert L.tt_insert_central_slices_rfft_3d_backward(fake, 0, fake, fake, ctypes.byref(p),
+                                                       None) == _lib.TT_ERR_INVALID
+    p = _params(volume_layout=2, n=0)
+    assert L.tt_insert_central_slices_rfft_3d_backward(fake, 0, fake, fake, ctypes.byref(p), None) == _lib.TT_OK
+
+
+@pytest.mark.fake_pointers
 def test_probe_validation():
     from teamtomo_b200 import _lib
 

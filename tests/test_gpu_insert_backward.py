@@ -60,6 +60,30 @@ def test_matches_oracle(oracle, n, k, kw):
     assert np.array_equal(got == 0, ref == 0)
 
 
+@pytest.mark.parametrize("n,k,kw", [(64, 200, {}), (33, 90, {}), (48, 150, dict(fftfreq_max=0.3)),
+                                    (40, 120, dict(zyx_matrices=True))])
+def test_bricked_gradient_copy_is_bitwise_plain(oracle, monkeypatch, n, k, kw):
+    """From half a slice pixel per voxel the backward gathers from a bricked
+    copy of the gradient volume: the same values and sums as from the plain
+    volume, bit for bit (odd box included: the copy is padded to even dims)."""
+    rng = np.random.default_rng(n * k)
+    shape = (k, n, n // 2 + 1)
+    imgs = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+    gvol = (rng.standard_normal((n, n, n // 2 + 1)) + 1j * rng.standard_normal((n, n, n // 2 + 1))).astype(
+        np.complex64)
+    rot = rotations(k, seed=n + 1)
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "plain")
+    plain = _grad(imgs, rot, gvol, n, **kw)
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "bricks")
+    bricked = _grad(imgs, rot, gvol, n, **kw)
+    monkeypatch.setenv("TT_VOLUME_LAYOUT", "auto")
+    auto = _grad(imgs, rot, gvol, n, **kw)
+    assert np.array_equal(plain, bricked) and np.array_equal(plain, auto)
+    ref = oracle.insert_grad_images(gvol, (n, n, n), rot, **kw)
+    assert rel_l2(bricked, ref) < 1e-6
+    assert np.array_equal(bricked == 0, ref == 0)
+
+
 @pytest.mark.parametrize("n", [128, 65])
 def test_adjoint_identity(n):
     """Re<G, insert(X)> = Re<insert_bwd(G), X>, in complex128."""
