@@ -202,11 +202,15 @@ def reference_ctf():
 
 def reference_ctf_images(calc, rows, box):
     """(n, box, box//2+1) CTF images of the reference's calculate_ctf_2d
-    (rfft, fftshifted) for (n, 8) rows of batched.ctf_params."""
-    c = rows.float()
-    return calc(defocus=c[:, 0], astigmatism=c[:, 1], astigmatism_angle=c[:, 2], voltage=c[:, 3],
-                spherical_aberration=c[:, 4], amplitude_contrast=c[:, 5], phase_shift=c[:, 6],
-                pixel_size=c[:, 7], image_shape=(box, box), rfft=True, fftshift=True)
+    (rfft, fftshifted) for (n, 8) rows of batched.ctf_params.  Each argument
+    goes in as its own copy: calculate_ctf_2d subtracts the astigmatism from
+    its defocus argument in place, which on views of one rows tensor also
+    corrupts the other columns it reads."""
+    c = rows.detach().float()
+    col = lambda i: c[:, i].clone()  # noqa: E731
+    return calc(defocus=col(0), astigmatism=col(1), astigmatism_angle=col(2), voltage=col(3),
+                spherical_aberration=col(4), amplitude_contrast=col(5), phase_shift=col(6),
+                pixel_size=col(7), image_shape=(box, box), rfft=True, fftshift=True)
 
 
 def reference_ctf_insert(mods, calc, images, R, rows, box):
