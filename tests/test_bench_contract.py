@@ -76,3 +76,23 @@ def test_reference_ctf_insert_weights_are_ctf_squared_insertions(oracle):
     rw, _ = oracle.insert((ctf * ctf).astype(np.complex64), (n, n, n), R)
     # float32 CTF (reference) against float64 (oracle): the GPU CTF tests use the same 1e-4
     assert rel_l2(v.numpy(), rv) < 1e-4 and rel_l2(w.numpy(), rw.real) < 1e-4
+
+
+def test_reference_arm_prints_its_line():
+    """--impl reference runs the reference's own torch code on the host cores
+    (here on a 32^3 box) and prints the contract's JSON line."""
+    import json
+    import subprocess
+
+    if not os.path.isdir(os.path.join(ROOT, "baseline", "_ref", "torch_fourier_slice")):
+        pytest.skip("baseline/_ref missing (run baseline/install_reference.py)")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--box", "32", "--steps", "1",
+                        "--warmup", "1"], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "slices/s"
+    assert line["higher_is_better"] is True and line["n_gpus"] == 1
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"] == {"value": line["value"], "unit": "slices/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
